@@ -1,0 +1,15 @@
+"""arma_b200: B200 implementation of the ARMA wavy-surface hot path.
+
+The product is the shared library ``libarma_b200.so`` (sm_100a CUDA kernels
+behind the C ABI declared in ``include/arma_b200.h``).  This package is a thin
+ctypes binding over that ABI for Python callers and tests; it never falls back
+to a CPU implementation -- if the library is missing, importing
+:mod:`arma_b200.capi` raises.
+"""
+from .capi import (  # noqa: F401
+    ArmaError, Context, MtParams, Surface, lib, library_path,
+    FP64, FP32C, ACF_STANDING, ACF_PROPAGATING,
+    NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL, NIT_BISECTION, NIT_LUT,
+    acf_eval, ar_fit, ar_fit_analytic, mt19937_params, mt_file_count,
+    mt_file_read, mt_file_write,
+)

@@ -1,0 +1,310 @@
+"""ctypes binding of the arma_b200 C ABI (``include/arma_b200.h``).
+
+Device buffers are passed as raw pointers (``int``), e.g.
+``torch.Tensor.data_ptr()``; host arrays are numpy arrays.  Every call checks
+the returned status and raises :class:`ArmaError` carrying the library's
+message, mirroring the reference's exceptions (``std::runtime_error``,
+``std::invalid_argument``, ``PRNG_error``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+library_path = os.path.join(_HERE, "libarma_b200.so")
+
+FP64, FP32C = 0, 1
+ACF_STANDING, ACF_PROPAGATING = 0, 1
+FIT_BUNCH_KAUFMAN, FIT_CHOLESKY = 0, 1
+NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL = 0, 1
+NIT_BISECTION, NIT_LUT = 0, 1
+
+ERRORS = {
+    -1: "ARMA_EINVAL", -2: "ARMA_ECUDA", -3: "ARMA_ENOMEM", -4: "ARMA_ETIMEDOUT",
+    -5: "ARMA_EIO", -6: "ARMA_EPRNG", -7: "ARMA_ENUMERIC", -8: "ARMA_ENOTSUP",
+}
+
+EXPORTS = (
+    "arma_version", "arma_last_error", "arma_ctx_create", "arma_ctx_destroy",
+    "arma_ctx_set_stream", "arma_ctx_synchronize", "arma_ctx_launch_count",
+    "arma_ctx_set_profiling", "arma_ctx_profile", "arma_ctx_profile_reset",
+    "arma_mt_file_count", "arma_mt_file_read", "arma_mt_file_write",
+    "arma_mt19937_params", "arma_mt_genrand", "arma_acf_eval", "arma_ar_fit",
+    "arma_ar_fit_analytic", "arma_white_noise", "arma_ar_filter",
+    "arma_variance_renorm", "arma_nit_apply", "arma_velocity_linear",
+    "arma_batch_generate", "arma_batch_generate_host",
+)
+
+
+class ArmaError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class MtParams(C.Structure):
+    """dcmt parameter set (``arma_mt_params``)."""
+
+    _fields_ = [
+        ("aaa", C.c_uint32), ("mm", C.c_int32), ("nn", C.c_int32),
+        ("rr", C.c_int32), ("ww", C.c_int32), ("wmask", C.c_uint32),
+        ("umask", C.c_uint32), ("lmask", C.c_uint32), ("shift0", C.c_int32),
+        ("shift1", C.c_int32), ("shiftB", C.c_int32), ("shiftC", C.c_int32),
+        ("maskB", C.c_uint32), ("maskC", C.c_uint32), ("i", C.c_int32),
+    ]
+
+    def as_tuple(self):
+        return tuple(getattr(self, f) for f, _ in self._fields_)
+
+
+class Surface(C.Structure):
+    """One surface of a batch (``arma_surface``)."""
+
+    _fields_ = [
+        ("shape", C.c_int * 3), ("order", C.c_int * 3),
+        ("phi", C.POINTER(C.c_double)), ("var_wn", C.c_double),
+        ("acf0", C.c_double), ("mt", MtParams), ("seed", C.c_uint32),
+        ("d_zeta", C.c_void_p), ("scale", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load the product library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(library_path):
+            raise ImportError(
+                f"{library_path} is missing: build it with `make -C arma_b200` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(library_path)
+        i, d, sz, vp = C.c_int, C.c_double, C.c_size_t, C.c_void_p
+        ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+        mp = C.POINTER(MtParams)
+        sigs = {
+            "arma_version": (i, []),
+            "arma_last_error": (i, [C.c_char_p, sz]),
+            "arma_ctx_create": (i, [i, C.POINTER(vp)]),
+            "arma_ctx_destroy": (i, [vp]),
+            "arma_ctx_set_stream": (i, [vp, vp]),
+            "arma_ctx_synchronize": (i, [vp]),
+            "arma_ctx_launch_count": (i, [vp, C.POINTER(C.c_uint64)]),
+            "arma_ctx_set_profiling": (i, [vp, i]),
+            "arma_ctx_profile": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_uint64)]),
+            "arma_ctx_profile_reset": (i, [vp]),
+            "arma_mt_file_count": (i, [C.c_char_p, ip]),
+            "arma_mt_file_read": (i, [C.c_char_p, i, mp]),
+            "arma_mt_file_write": (i, [C.c_char_p, mp, i]),
+            "arma_mt19937_params": (i, [mp]),
+            "arma_mt_genrand": (i, [vp, mp, C.c_uint32, C.c_uint64, sz, vp]),
+            "arma_acf_eval": (i, [i, d, d, dp, dp, dp, ip, dp]),
+            "arma_ar_fit": (i, [dp, ip, ip, i, dp, dp]),
+            "arma_ar_fit_analytic": (i, [i, d, d, dp, dp, dp, ip, dp, dp]),
+            "arma_white_noise": (i, [vp, mp, C.c_uint32, d, sz, i, vp]),
+            "arma_ar_filter": (i, [vp, dp, ip, ip, i, vp]),
+            "arma_variance_renorm": (i, [vp, vp, ip, i, d, dp]),
+            "arma_nit_apply": (i, [vp, i, dp, d, i, dp, d, i, i, d, sz, i, vp]),
+            "arma_velocity_linear": (i, [vp, vp, ip, i, dp, d, dp, i, ip, i, vp]),
+            "arma_batch_generate": (i, [vp, C.POINTER(Surface), i, i]),
+            "arma_batch_generate_host": (i, [vp, C.POINTER(Surface), i, i]),
+        }
+        for name, (res, args) in sigs.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        buf = C.create_string_buffer(1024)
+        lib().arma_last_error(buf, len(buf))
+        raise ArmaError(rc, buf.value.decode(errors="replace"))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i3(v):
+    return (C.c_int * 3)(*[int(x) for x in v])
+
+
+def _d(v):
+    a = np.ascontiguousarray(v, dtype=np.float64)
+    return a, _dp(a)
+
+
+# ------------------------------------------------------------------ host fit
+def acf_eval(kind, shape, amplitude, velocity, alpha, beta, delta=(1.0, 1.0, 1.0)):
+    out = np.empty(tuple(shape), np.float64)
+    a, ap = _d(alpha)
+    b, bp = _d(beta)
+    dl, dlp = _d(delta)
+    _check(lib().arma_acf_eval(kind, amplitude, velocity, ap, bp, dlp, _i3(shape), _dp(out)))
+    return out
+
+
+def ar_fit(acf, order, method=FIT_CHOLESKY):
+    acf = np.ascontiguousarray(acf, np.float64)
+    phi = np.empty(tuple(order), np.float64)
+    var = C.c_double()
+    _check(lib().arma_ar_fit(_dp(acf), _i3(acf.shape), _i3(order), method, _dp(phi), C.byref(var)))
+    return phi, var.value
+
+
+def ar_fit_analytic(kind, order, amplitude, velocity, alpha, beta, delta=(1.0, 1.0, 1.0)):
+    phi = np.empty(tuple(order), np.float64)
+    var = C.c_double()
+    a, ap = _d(alpha)
+    b, bp = _d(beta)
+    dl, dlp = _d(delta)
+    _check(lib().arma_ar_fit_analytic(kind, amplitude, velocity, ap, bp, dlp, _i3(order),
+                                      _dp(phi), C.byref(var)))
+    return phi, var.value
+
+
+def mt19937_params() -> MtParams:
+    p = MtParams()
+    _check(lib().arma_mt19937_params(C.byref(p)))
+    return p
+
+
+def mt_file_count(path: str) -> int:
+    n = C.c_int()
+    _check(lib().arma_mt_file_count(path.encode(), C.byref(n)))
+    return n.value
+
+
+def mt_file_read(path: str, index: int) -> MtParams:
+    p = MtParams()
+    _check(lib().arma_mt_file_read(path.encode(), index, C.byref(p)))
+    return p
+
+
+def mt_file_write(path: str, sets) -> None:
+    arr = (MtParams * len(sets))(*sets)
+    _check(lib().arma_mt_file_write(path.encode(), arr, len(sets)))
+
+
+# ------------------------------------------------------------------ device
+class Context:
+    """An ``arma_ctx`` bound to one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().arma_ctx_create(device, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().arma_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib().arma_ctx_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        _check(lib().arma_ctx_synchronize(self._h))
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        _check(lib().arma_ctx_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def set_profiling(self, on: bool = True):
+        _check(lib().arma_ctx_set_profiling(self._h, 1 if on else 0))
+
+    def profile(self, name: str):
+        """(milliseconds, launches) accumulated for one kernel class."""
+        ms = C.c_double()
+        n = C.c_uint64()
+        _check(lib().arma_ctx_profile(self._h, name.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def profile_reset(self):
+        _check(lib().arma_ctx_profile_reset(self._h))
+
+    def mt_genrand(self, params: MtParams, seed: int, n: int, d_out: int, offset: int = 0):
+        _check(lib().arma_mt_genrand(self._h, C.byref(params), seed, offset, n, C.c_void_p(d_out)))
+
+    def white_noise(self, params: MtParams, seed: int, stddev: float, n: int, precision: int,
+                    d_out: int):
+        _check(lib().arma_white_noise(self._h, C.byref(params), seed, stddev, n, precision,
+                                      C.c_void_p(d_out)))
+
+    def ar_filter(self, phi, shape, precision: int, d_zeta: int):
+        phi = np.ascontiguousarray(phi, np.float64)
+        _check(lib().arma_ar_filter(self._h, _dp(phi), _i3(phi.shape), _i3(shape), precision,
+                                    C.c_void_p(d_zeta)))
+
+    def variance_renorm(self, d_zeta: int, shape, precision: int, acf0: float) -> float:
+        s = C.c_double()
+        _check(lib().arma_variance_renorm(self._h, C.c_void_p(d_zeta), _i3(shape), precision,
+                                          acf0, C.byref(s)))
+        return s.value
+
+    def nit_apply(self, dist: int, params, stdev: float, method: int, n: int, precision: int,
+                  d_zeta: int, interval=(0.0, 1.0), eps=1e-6, max_iter=100, lut_nodes=1024,
+                  lut_range=5.0):
+        p, pp = _d(list(params) + [0.0] * (3 - len(params)))
+        iv, ivp = _d(interval)
+        _check(lib().arma_nit_apply(self._h, dist, pp, stdev, method, ivp, eps, max_iter,
+                                    lut_nodes, lut_range, n, precision, C.c_void_p(d_zeta)))
+
+    def velocity_linear(self, d_zeta: int, shape, precision: int, delta, depth: float,
+                        z_levels, t_idx, d_out: int):
+        dl, dlp = _d(delta)
+        zs, zsp = _d(z_levels)
+        ti = np.ascontiguousarray(t_idx, np.int32)
+        _check(lib().arma_velocity_linear(self._h, C.c_void_p(d_zeta), _i3(shape), precision,
+                                          dlp, depth, zsp, len(zs),
+                                          ti.ctypes.data_as(C.POINTER(C.c_int)), len(ti),
+                                          C.c_void_p(d_out)))
+
+    def batch_generate(self, surfaces, precision: int, host: bool = False):
+        arr = (Surface * len(surfaces))(*surfaces)
+        fn = lib().arma_batch_generate_host if host else lib().arma_batch_generate
+        _check(fn(self._h, arr, len(surfaces), precision))
+        for k, s in enumerate(surfaces):
+            s.scale = arr[k].scale
+        return [arr[k].scale for k in range(len(surfaces))]
+
+
+def make_surface(shape, phi, var_wn, acf0, mt: MtParams, seed: int, buf_ptr: int) -> Surface:
+    """Build an ``arma_surface``; keeps a reference to phi on the struct."""
+    phi = np.ascontiguousarray(phi, np.float64)
+    s = Surface()
+    s.shape = (C.c_int * 3)(*shape)
+    s.order = (C.c_int * 3)(*phi.shape)
+    s.phi = _dp(phi)
+    s._phi_ref = phi  # keep alive
+    s.var_wn = var_wn
+    s.acf0 = acf0
+    s.mt = mt
+    s.seed = seed
+    s.d_zeta = buf_ptr
+    s.scale = 0.0
+    return s

@@ -1,0 +1,368 @@
+// FP32 compensated AR filter: a persistent tile wavefront over a batch of
+// independent surfaces.
+//
+// The filter (reference src/generator/ar_model_surf.cc:5-36) is
+//     zeta(t,x,y) = eps(t,x,y) + sum_{(k,i,j) != 0} phi(k,i,j) zeta(t-k,x-i,y-j)
+// with zeta = 0 outside the array.  Because phi(0,i,j) != 0, every point
+// depends on earlier points of its own time slice as well as on the previous
+// pt-1 slices.  The work is split into spatial tiles of TX x TY points; one
+// CTA owns one tile of one surface for all t and walks the slices in order.
+// For slice t it
+//   1. accumulates the terms on slices t-1 .. t-pt+1 (90% of the work for a
+//      10^3 model) from a shared-memory ring that holds those slices for the
+//      tile plus its west/north halo,
+//   2. waits for the three neighbour tiles (x-1, y-1, both) to publish slice t
+//      (a per-tile counter in global memory; bounded spin),
+//   3. loads slice t of the halo and adds the current-slice terms that reach
+//      into it (the in-tile part of the current slice is held at zero),
+//   4. solves the remaining in-tile recursion zeta = S + A0 zeta exactly as a
+//      quarter-plane convolution zeta = H * S, where H is the impulse response
+//      of 1 / (1 - A0(z1,z2)) on the tile (precomputed in FP64),
+//   5. stores the slice to the ring and to global memory and publishes it.
+// Sums are plain FP32 FMAs over one (k,i) row of taps, combined across rows
+// with Kahan compensation.  Tiles are handed out through a global ticket
+// counter in dependency order, so a CTA only ever waits on tiles that are
+// already owned by running CTAs.
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+
+namespace armab {
+namespace {
+
+constexpr int TX = 16;            // tile rows (x)
+constexpr int TY = 32;            // tile columns (y)
+constexpr int R = 8;              // outputs per thread along y
+constexpr int STRIPS = TY / R;    // threads per tile row
+constexpr int NTHREADS = TX * STRIPS;
+constexpr int LH = 12;            // left (y) halo columns held in the ring
+constexpr int W = LH + TY;        // ring row width (floats)
+constexpr int SPAD = TY + 8;      // zero padding left of each S row
+constexpr int SW = SPAD + TY + 4; // S row width (padded against bank conflicts)
+constexpr int MAXO = 13;          // max order per axis supported (py <= LH+1)
+constexpr long long kSpinLimit = 1ll << 24;
+
+struct Task {
+	int nt, nx, ny, pt, px, py;
+	int tiles_x, tiles_y;
+	int ticket_base;
+	float* zeta;
+	const float* phi;
+	const float* h;
+	int* flags;
+};
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+	const float y = v - c;
+	const float t = s + y;
+	c = (t - s) - y;
+	s = t;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+	int v;
+	asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+
+__device__ __forceinline__ void st_release(int* p, int v) {
+	asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Wait until *flag >= need.  Gives up after kSpinLimit polls (or when another
+// CTA already gave up) and reports DEV_TIMEOUT; returns false then.
+__device__ bool wait_flag(const int* flag, int need, int* err) {
+	for (long long it = 0; it < kSpinLimit; ++it) {
+		if (ld_acquire(flag) >= need) return true;
+		if ((it & 63) == 63 && *((volatile int*)err) != DEV_OK) return false;
+		__nanosleep(128);
+	}
+	atomicExch(err, DEV_TIMEOUT);
+	return false;
+}
+
+template <int PY>
+__device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) {
+	const int tid = threadIdx.x;
+	const int xl = tid / STRIPS;            // tile-local row
+	const int yl0 = (tid % STRIPS) * R;     // tile-local first column
+	const int pt = tk.pt, px = tk.px;
+	const int hx = px - 1;
+	const int rows = TX + hx;
+	const int slot_sz = rows * W;
+	constexpr int PYP = (PY + 3) & ~3;      // padded tap row
+	const int x0 = bx * TX, y0 = by * TY;
+	const long long sst = (long long)tk.nx * tk.ny;
+
+	float* ring = smem;                                  // pt slots
+	float* sphi = ring + pt * slot_sz;                   // pt*px*PYP
+	float* sh = sphi + pt * px * PYP;                    // TX*TY
+	float* ss = sh + TX * TY;                            // TX*SW
+
+	// stage coefficients (rows padded with zeros), H, zero the ring and S pads
+	for (int q = tid; q < pt * px * PYP; q += NTHREADS) {
+		const int j = q % PYP, ki = q / PYP;
+		sphi[q] = j < PY ? tk.phi[ki * PY + j] : 0.0f;
+	}
+	for (int q = tid; q < TX * TY; q += NTHREADS) sh[q] = tk.h[q];
+	for (int q = tid; q < pt * slot_sz; q += NTHREADS) ring[q] = 0.0f;
+	for (int q = tid; q < TX * SW; q += NTHREADS) ss[q] = 0.0f;
+	__syncthreads();
+
+	const int gx = x0 + xl;
+	const int* fW = (bx > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by : nullptr;
+	const int* fN = (by > 0) ? tk.flags + bx * tk.tiles_y + by - 1 : nullptr;
+	const int* fNW = (bx > 0 && by > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by - 1 : nullptr;
+
+	for (int t = 0; t < tk.nt; ++t) {
+		float* cur = ring + (t % pt) * slot_sz;
+		float* zt = tk.zeta + t * sst;
+		// noise of this thread's strip (own tile: written by an earlier kernel)
+		float s[R], c[R];
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+			const int gy = y0 + yl0 + r;
+			s[r] = (gx < tk.nx && gy < tk.ny) ? zt[(long long)gx * tk.ny + gy] : 0.0f;
+			c[r] = 0.0f;
+		}
+		// clear the current slot (halo is refilled below; in-tile stays 0 until
+		// the slice is solved)
+		for (int q = tid; q < slot_sz; q += NTHREADS) cur[q] = 0.0f;
+
+		auto accumulate_rows = [&](const float* slot, int k) {
+			const float* prow = sphi + (k * px) * PYP;
+			for (int i = 0; i < px; ++i) {
+				const float* zr = slot + (xl + hx - i) * W + yl0;
+				float win[R + LH];
+#pragma unroll
+				for (int q = 0; q < (R + LH) / 4; ++q) {
+					const float4 v = reinterpret_cast<const float4*>(zr)[q];
+					win[4 * q] = v.x;
+					win[4 * q + 1] = v.y;
+					win[4 * q + 2] = v.z;
+					win[4 * q + 3] = v.w;
+				}
+				float ph[PYP];
+#pragma unroll
+				for (int q = 0; q < PYP / 4; ++q) {
+					const float4 v = reinterpret_cast<const float4*>(prow + i * PYP)[q];
+					ph[4 * q] = v.x;
+					ph[4 * q + 1] = v.y;
+					ph[4 * q + 2] = v.z;
+					ph[4 * q + 3] = v.w;
+				}
+#pragma unroll
+				for (int r = 0; r < R; ++r) {
+					float p = 0.0f;
+#pragma unroll
+					for (int j = 0; j < PY; ++j) p = fmaf(ph[j], win[LH + r - j], p);
+					kahan_add(s[r], c[r], p);
+				}
+			}
+		};
+
+		// 1. previous slices
+		for (int k = 1; k < pt && k <= t; ++k) accumulate_rows(ring + ((t - k) % pt) * slot_sz, k);
+		__syncthreads();  // slot cleared by all threads
+
+		// 2. neighbours' slice t
+		__shared__ int s_ok;
+		if (tid == 0) {
+			bool ok = true;
+			if (fW) ok = ok && wait_flag(fW, t + 1, err);
+			if (ok && fN) ok = ok && wait_flag(fN, t + 1, err);
+			if (ok && fNW) ok = ok && wait_flag(fNW, t + 1, err);
+			s_ok = ok ? 1 : 0;
+		}
+		__syncthreads();
+		if (!s_ok) return;
+
+		// 3. halo of slice t: rows above the tile (all columns) and the left
+		//    columns of the tile rows
+		for (int q = tid; q < rows * W; q += NTHREADS) {
+			const int rr = q / W, cc = q % W;
+			if (rr >= hx && cc >= LH) continue;  // in-tile: stays zero
+			const int x = x0 - hx + rr, y = y0 - LH + cc;
+			if (x < 0 || y < 0 || x >= tk.nx || y >= tk.ny) continue;
+			cur[q] = __ldcg(zt + (long long)x * tk.ny + y);
+		}
+		__syncthreads();
+		accumulate_rows(cur, 0);
+
+		// 4. S = noise + all terms outside the unknown in-tile part
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+			const int gy = y0 + yl0 + r;
+			const bool valid = gx < tk.nx && gy < tk.ny;
+			ss[xl * SW + SPAD + yl0 + r] = valid ? (s[r] - c[r]) : 0.0f;
+		}
+		__syncthreads();
+
+		//    zeta = H * S over the quarter plane of the tile
+		float a[R], ac[R];
+#pragma unroll
+		for (int r = 0; r < R; ++r) { a[r] = 0.0f; ac[r] = 0.0f; }
+		for (int dx = 0; dx <= xl; ++dx) {
+			const float* srow = ss + (xl - dx) * SW + SPAD;
+			const float* hrow = sh + dx * TY;
+			float p[R];
+#pragma unroll
+			for (int r = 0; r < R; ++r) p[r] = 0.0f;
+			for (int dy0 = 0; dy0 <= yl0; dy0 += R) {
+				// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
+				float w[2 * R];
+				const float4* sp = reinterpret_cast<const float4*>(srow + yl0 - dy0 - R);
+#pragma unroll
+				for (int q = 0; q < 2 * R / 4; ++q) {
+					const float4 v = sp[q];
+					w[4 * q] = v.x;
+					w[4 * q + 1] = v.y;
+					w[4 * q + 2] = v.z;
+					w[4 * q + 3] = v.w;
+				}
+				float hv[R];
+				const float4* hp = reinterpret_cast<const float4*>(hrow + dy0);
+#pragma unroll
+				for (int q = 0; q < R / 4; ++q) {
+					const float4 v = hp[q];
+					hv[4 * q] = v.x;
+					hv[4 * q + 1] = v.y;
+					hv[4 * q + 2] = v.z;
+					hv[4 * q + 3] = v.w;
+				}
+#pragma unroll
+				for (int dd = 0; dd < R; ++dd)
+#pragma unroll
+					for (int r = 0; r < R; ++r) p[r] = fmaf(hv[dd], w[R + r - dd], p[r]);
+			}
+#pragma unroll
+			for (int r = 0; r < R; ++r) kahan_add(a[r], ac[r], p[r]);
+		}
+
+		// 5. store the solved slice and publish it
+		float* own = cur + hx * W + LH;
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+			const float v = a[r] - ac[r];
+			own[xl * W + yl0 + r] = v;
+			const int gy = y0 + yl0 + r;
+			if (gx < tk.nx && gy < tk.ny) zt[(long long)gx * tk.ny + gy] = v;
+		}
+		__syncthreads();
+		if (tid == 0) {
+			__threadfence();
+			st_release(tk.flags + bx * tk.tiles_y + by, t + 1);
+		}
+	}
+}
+
+template <int PY>
+__global__ void __launch_bounds__(NTHREADS)
+ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
+             int* __restrict__ ticket_counter, int* __restrict__ err) {
+	extern __shared__ __align__(16) float smem[];
+	__shared__ int s_ticket;
+	for (;;) {
+		if (threadIdx.x == 0) s_ticket = atomicAdd(ticket_counter, 1);
+		__syncthreads();
+		const int ticket = s_ticket;
+		__syncthreads();
+		if (ticket >= total_tickets) return;
+		if (*((volatile int*)err) != DEV_OK) return;
+		// locate the surface owning this ticket
+		int lo = 0, hi = ntasks - 1;
+		while (lo < hi) {
+			const int mid = (lo + hi + 1) / 2;
+			if (tasks[mid].ticket_base <= ticket) lo = mid; else hi = mid - 1;
+		}
+		const Task tk = tasks[lo];
+		const int local = ticket - tk.ticket_base;
+		run_tile<PY>(tk, local / tk.tiles_y, local % tk.tiles_y, smem, err);
+		__syncthreads();
+	}
+}
+
+size_t smem_bytes(int pt, int px, int py) {
+	const int rows = TX + px - 1;
+	const int pyp = (py + 3) & ~3;
+	return sizeof(float) * (size_t(pt) * rows * W + size_t(pt) * px * pyp + TX * TY + TX * SW);
+}
+
+template <int PY>
+void launch_group(Ctx* c, const std::vector<Task>& tasks, int total, int pt_max, int px_max) {
+	Task* d_tasks = static_cast<Task*>(scratch_take(c, sizeof(Task) * tasks.size()));
+	int* d_ticket = static_cast<int*>(scratch_take(c, sizeof(int)));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d_tasks, tasks.data(), sizeof(Task) * tasks.size(),
+	                              cudaMemcpyHostToDevice, c->stream));
+	ARMA_CUDA_TRY(cudaMemsetAsync(d_ticket, 0, sizeof(int), c->stream));
+	const size_t smem = smem_bytes(pt_max, px_max, PY);
+	ARMA_CUDA_TRY(cudaFuncSetAttribute(ar32c_kernel<PY>,
+	                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+	int per_sm = 0;
+	ARMA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ar32c_kernel<PY>,
+	                                                            NTHREADS, smem));
+	ARMA_REQUIRE(per_sm > 0, ARMA_EINVAL, "AR tile does not fit in shared memory");
+	const int grid = std::min(total, per_sm * c->num_sms);
+	ProfScope prof_(c, "ar32c");
+	ar32c_kernel<PY><<<grid, NTHREADS, smem, c->stream>>>(d_tasks, int(tasks.size()), total,
+	                                                     d_ticket, c->d_err);
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 1;
+}
+
+}  // namespace
+
+int ar32c_tile_x() { return TX; }
+int ar32c_tile_y() { return TY; }
+
+void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int ty, int) {
+	ARMA_REQUIRE(tx == TX && ty == TY, ARMA_EINVAL, "unsupported AR tile shape");
+	// group by py (compile-time tap count); order each group by work, largest first
+	std::vector<std::vector<int>> groups(MAXO + 1);
+	for (size_t k = 0; k < surfaces.size(); ++k) {
+		const Ar32Surface& s = surfaces[k];
+		ARMA_REQUIRE(s.px <= TX + 1 && s.py <= MAXO && s.pt >= 1 && s.px >= 1 && s.py >= 1,
+		             ARMA_ENOTSUP, "AR order not supported by the FP32 tile kernel");
+		groups[s.py].push_back(int(k));
+	}
+	for (int py = 1; py <= MAXO; ++py) {
+		auto& g = groups[py];
+		if (g.empty()) continue;
+		std::sort(g.begin(), g.end(), [&](int a, int b) {
+			const Ar32Surface &A = surfaces[a], &B = surfaces[b];
+			return double(A.nt) * A.nx * A.ny * A.pt * A.px > double(B.nt) * B.nx * B.ny * B.pt * B.px;
+		});
+		std::vector<Task> tasks;
+		int total = 0, pt_max = 1, px_max = 1;
+		size_t nflags = 0;
+		for (int k : g) nflags += size_t(surfaces[k].tiles_x) * surfaces[k].tiles_y;
+		int* flags = static_cast<int*>(scratch_take(c, sizeof(int) * nflags));
+		ARMA_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int) * nflags, c->stream));
+		size_t foff = 0;
+		for (int k : g) {
+			const Ar32Surface& s = surfaces[k];
+			Task t;
+			t.nt = s.nt; t.nx = s.nx; t.ny = s.ny;
+			t.pt = s.pt; t.px = s.px; t.py = s.py;
+			t.tiles_x = s.tiles_x; t.tiles_y = s.tiles_y;
+			t.ticket_base = total;
+			t.zeta = s.zeta; t.phi = s.phi; t.h = s.h;
+			t.flags = flags + foff;
+			foff += size_t(s.tiles_x) * s.tiles_y;
+			total += s.tiles_x * s.tiles_y;
+			pt_max = std::max(pt_max, s.pt);
+			px_max = std::max(px_max, s.px);
+			tasks.push_back(t);
+		}
+		switch (py) {
+#define ARMA_PY_CASE(N) case N: launch_group<N>(c, tasks, total, pt_max, px_max); break;
+			ARMA_PY_CASE(1) ARMA_PY_CASE(2) ARMA_PY_CASE(3) ARMA_PY_CASE(4) ARMA_PY_CASE(5)
+			ARMA_PY_CASE(6) ARMA_PY_CASE(7) ARMA_PY_CASE(8) ARMA_PY_CASE(9) ARMA_PY_CASE(10)
+			ARMA_PY_CASE(11) ARMA_PY_CASE(12) ARMA_PY_CASE(13)
+#undef ARMA_PY_CASE
+		}
+	}
+}
+
+}  // namespace armab

@@ -1,0 +1,687 @@
+// C ABI: argument checking, error mapping, context and scratch management,
+// and the orchestration of the device kernels.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "distributions.h"
+#include "internal.h"
+
+struct arma_ctx {
+	armab::Ctx c;
+	std::vector<std::pair<char*, size_t>> chunks;  // scratch chunks
+	size_t used = 0;                                // bytes used in the last chunk
+	size_t high_water = 0;                          // total bytes taken in one call
+	size_t taken = 0;
+};
+
+namespace armab {
+
+namespace {
+thread_local std::string g_last_error;
+
+arma_ctx* outer(Ctx* c) {
+	return reinterpret_cast<arma_ctx*>(reinterpret_cast<char*>(c) - offsetof(arma_ctx, c));
+}
+
+template <class F>
+int guard(F&& f) {
+	try {
+		f();
+		return ARMA_OK;
+	} catch (const Error& e) {
+		g_last_error = e.msg;
+		return e.code;
+	} catch (const std::bad_alloc&) {
+		g_last_error = "host allocation failed";
+		return ARMA_ENOMEM;
+	} catch (const std::exception& e) {
+		g_last_error = e.what();
+		return ARMA_EINVAL;
+	}
+}
+
+void require_shape(const int s[3], const char* name) {
+	ARMA_REQUIRE(s && s[0] > 0 && s[1] > 0 && s[2] > 0, ARMA_EINVAL,
+	             std::string("Bad \"") + name + "\": dimensions must be positive");
+}
+
+size_t elem_size(int precision) {
+	ARMA_REQUIRE(precision == ARMA_FP64 || precision == ARMA_FP32C, ARMA_EINVAL,
+	             "bad precision");
+	return precision == ARMA_FP64 ? sizeof(double) : sizeof(float);
+}
+
+// Host-side copy of sgenrand-independent validation of a parameter set.
+void require_mt(const arma_mt_params* p) {
+	ARMA_REQUIRE(p, ARMA_EINVAL, "null MT parameter set");
+	ARMA_REQUIRE(p->ww == 32 && p->nn > 1 && p->mm > 0 && p->mm < p->nn && p->rr >= 0 &&
+	                 p->rr < 32,
+	             ARMA_EINVAL, "bad MT parameter set");
+}
+
+uint64_t noise_attempts(size_t n, double margin) {
+	const double pairs = std::ceil(n / 2.0);
+	return uint64_t((pairs * (4.0 / dist::kPi) + 8.0 * std::sqrt(pairs) + 256.0) * margin);
+}
+
+void white_noise(Ctx* c, const arma_mt_params& p, uint32_t seed, double stddev, size_t n,
+                 int precision, void* d_out) {
+	ARMA_REQUIRE(stddev >= 0.0 && std::isfinite(stddev), ARMA_EINVAL,
+	             "variance is less than zero");
+	if (n == 0) return;
+	double margin = 1.0;
+	for (int round = 0; round < 8; ++round) {
+		const uint64_t n_att = noise_attempts(n, margin);
+		uint32_t* words = static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * 4 * n_att));
+		launch_mt_generate(c, p, seed, 0, 4 * n_att, words);
+		if (launch_white_noise(c, words, 4 * n_att, stddev, n, precision, d_out)) return;
+		margin *= 1.5;
+	}
+	throw Error{ARMA_ECUDA, "white noise: rejection sampling did not converge"};
+}
+
+// White noise for many surfaces: all MT streams in one launch (one CTA per
+// stream), the polar transforms enqueued back to back, one host check.
+void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
+                       const std::vector<void*>& dz) {
+	std::vector<MtJob> jobs(n);
+	std::vector<uint64_t> att(n);
+	for (int k = 0; k < n; ++k) {
+		ARMA_REQUIRE(s[k].var_wn >= 0.0 && std::isfinite(s[k].var_wn), ARMA_EINVAL,
+		             "variance is less than zero");
+		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
+		att[k] = noise_attempts(np, 1.0);
+		jobs[k] = MtJob{s[k].mt, s[k].seed, 0, 4 * att[k],
+		                static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * 4 * att[k]))};
+	}
+	long long* d_pairs = static_cast<long long*>(scratch_take(c, sizeof(long long) * n));
+	launch_mt_generate_batch(c, jobs);
+	for (int k = 0; k < n; ++k) {
+		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
+		enqueue_white_noise(c, jobs[k].out, 4 * att[k], std::sqrt(s[k].var_wn), np, precision,
+		                    dz[k], d_pairs + k);
+	}
+	std::vector<long long> pairs(n);
+	ARMA_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(long long) * n,
+	                              cudaMemcpyDeviceToHost, c->stream));
+	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+	for (int k = 0; k < n; ++k) {
+		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
+		if (uint64_t(pairs[k]) * 2 < np)  // rare: not enough accepted attempts
+			white_noise(c, s[k].mt, s[k].seed, std::sqrt(s[k].var_wn), np, precision, dz[k]);
+	}
+}
+
+}  // namespace
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+const std::string& last_error() { return g_last_error; }
+
+void scratch_begin(Ctx* c, size_t) {
+	arma_ctx* o = outer(c);
+	if (o->chunks.size() > 1 || (o->chunks.size() == 1 && o->chunks[0].second < o->high_water)) {
+		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+		for (auto& ch : o->chunks) cudaFree(ch.first);
+		o->chunks.clear();
+		char* p = nullptr;
+		if (cudaMalloc(&p, o->high_water) != cudaSuccess)
+			throw Error{ARMA_ENOMEM, "device scratch allocation failed"};
+		o->chunks.emplace_back(p, o->high_water);
+	}
+	o->used = 0;
+	o->taken = 0;
+}
+
+void* scratch_take(Ctx* c, size_t bytes) {
+	arma_ctx* o = outer(c);
+	bytes = (bytes + 255) & ~size_t(255);
+	if (o->chunks.empty() || o->used + bytes > o->chunks.back().second) {
+		const size_t sz = std::max(bytes, size_t(64) << 20);
+		char* p = nullptr;
+		if (cudaMalloc(&p, sz) != cudaSuccess)
+			throw Error{ARMA_ENOMEM, "device scratch allocation failed"};
+		o->chunks.emplace_back(p, sz);
+		o->used = 0;
+	}
+	void* r = o->chunks.back().first + o->used;
+	o->used += bytes;
+	o->taken += bytes;
+	o->high_water = std::max(o->high_water, o->taken);
+	return r;
+}
+
+ProfScope::ProfScope(Ctx* c, const char* name) : c_(c) {
+	if (!c->profiling) return;
+	Ctx::Pending p;
+	p.name = name;
+	ARMA_CUDA_TRY(cudaEventCreate(&p.start));
+	ARMA_CUDA_TRY(cudaEventCreate(&p.stop));
+	ARMA_CUDA_TRY(cudaEventRecord(p.start, c->stream));
+	c->pending.push_back(p);
+	idx_ = int(c->pending.size()) - 1;
+}
+
+ProfScope::~ProfScope() {
+	if (idx_ >= 0) cudaEventRecord(c_->pending[idx_].stop, c_->stream);
+}
+
+void resolve_profile(Ctx* c) {
+	if (c->pending.empty()) return;
+	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+	for (auto& p : c->pending) {
+		float ms = 0.0f;
+		ARMA_CUDA_TRY(cudaEventElapsedTime(&ms, p.start, p.stop));
+		c->prof_ms[p.name] += ms;
+		c->prof_count[p.name] += 1;
+		cudaEventDestroy(p.start);
+		cudaEventDestroy(p.stop);
+	}
+	c->pending.clear();
+}
+
+void check_device_error(Ctx* c) {
+	int h = 0;
+	ARMA_CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (h == DEV_TIMEOUT) {
+		ARMA_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+		throw Error{ARMA_ETIMEDOUT, "a bounded device wait gave up (tile dependency not met)"};
+	}
+	if (h != DEV_OK) {
+		ARMA_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+		throw Error{ARMA_ECUDA, "device-side check failed"};
+	}
+}
+
+}  // namespace armab
+
+using namespace armab;
+
+extern "C" {
+
+int arma_version(void) { return ARMA_B200_VERSION; }
+
+int arma_last_error(char* buf, size_t len) {
+	if (!buf || len == 0) return ARMA_EINVAL;
+	std::snprintf(buf, len, "%s", g_last_error.c_str());
+	return ARMA_OK;
+}
+
+int arma_ctx_create(int device, arma_ctx** out) {
+	return guard([&] {
+		ARMA_REQUIRE(out, ARMA_EINVAL, "null output pointer");
+		int ndev = 0;
+		ARMA_CUDA_TRY(cudaGetDeviceCount(&ndev));
+		ARMA_REQUIRE(device >= 0 && device < ndev, ARMA_EINVAL, "bad device index");
+		ARMA_CUDA_TRY(cudaSetDevice(device));
+		std::unique_ptr<arma_ctx> ctx(new arma_ctx());
+		ctx->c.device = device;
+		ARMA_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+		ctx->c.own_stream = true;
+		ARMA_CUDA_TRY(cudaMalloc(&ctx->c.d_err, sizeof(int)));
+		ARMA_CUDA_TRY(cudaMemset(ctx->c.d_err, 0, sizeof(int)));
+		ARMA_CUDA_TRY(cudaDeviceGetAttribute(&ctx->c.num_sms, cudaDevAttrMultiProcessorCount, device));
+		*out = ctx.release();
+	});
+}
+
+int arma_ctx_destroy(arma_ctx* ctx) {
+	return guard([&] {
+		if (!ctx) return;
+		cudaSetDevice(ctx->c.device);
+		cudaStreamSynchronize(ctx->c.stream);
+		for (auto& p : ctx->c.pending) {
+			cudaEventDestroy(p.start);
+			cudaEventDestroy(p.stop);
+		}
+		for (auto& kv : ctx->c.graphs) cudaGraphExecDestroy(kv.second);
+		for (auto& ch : ctx->chunks) cudaFree(ch.first);
+		cudaFree(ctx->c.d_err);
+		if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
+		delete ctx;
+	});
+}
+
+int arma_ctx_set_stream(arma_ctx* ctx, void* stream) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
+		if (ctx->c.own_stream) {
+			ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+			ARMA_CUDA_TRY(cudaStreamDestroy(ctx->c.stream));
+		}
+		ctx->c.stream = static_cast<cudaStream_t>(stream);
+		ctx->c.own_stream = false;
+	});
+}
+
+int arma_ctx_synchronize(arma_ctx* ctx) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+	});
+}
+
+int arma_ctx_launch_count(arma_ctx* ctx, uint64_t* count) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && count, ARMA_EINVAL, "null argument");
+		*count = ctx->c.launches;
+	});
+}
+
+int arma_ctx_set_profiling(arma_ctx* ctx, int enabled) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
+		ctx->c.profiling = enabled != 0;
+	});
+}
+
+int arma_ctx_profile(arma_ctx* ctx, const char* name, double* ms, uint64_t* launches) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && name && ms && launches, ARMA_EINVAL, "null argument");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		resolve_profile(&ctx->c);
+		auto it = ctx->c.prof_ms.find(name);
+		*ms = it == ctx->c.prof_ms.end() ? 0.0 : it->second;
+		auto jt = ctx->c.prof_count.find(name);
+		*launches = jt == ctx->c.prof_count.end() ? 0 : uint64_t(jt->second);
+	});
+}
+
+int arma_ctx_profile_reset(arma_ctx* ctx) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		resolve_profile(&ctx->c);
+		ctx->c.prof_ms.clear();
+		ctx->c.prof_count.clear();
+	});
+}
+
+// ---------------------------------------------------------------- MT sets
+int arma_mt19937_params(arma_mt_params* p) {
+	return guard([&] {
+		ARMA_REQUIRE(p, ARMA_EINVAL, "null output pointer");
+		std::memset(p, 0, sizeof(*p));
+		p->aaa = 0x9908b0dfu;
+		p->mm = 397;
+		p->nn = 624;
+		p->rr = 31;
+		p->ww = 32;
+		p->wmask = 0xffffffffu;
+		p->umask = 0x80000000u;
+		p->lmask = 0x7fffffffu;
+		p->shift0 = 11;
+		p->shift1 = 18;
+		p->shiftB = 7;
+		p->shiftC = 15;
+		p->maskB = 0x9d2c5680u;
+		p->maskC = 0xefc60000u;
+		p->i = 624;
+	});
+}
+
+namespace {
+constexpr size_t kMtRecord = 72;  // raw x86-64 mt_struct incl. padding + pointer
+
+bool read_record(std::ifstream& in, arma_mt_params* p) {
+	unsigned char hdr[kMtRecord];
+	if (!in.read(reinterpret_cast<char*>(hdr), kMtRecord)) return false;
+	std::memcpy(p, hdr, sizeof(arma_mt_params));
+	if (p->nn <= 0 || p->nn > (1 << 20)) throw Error{ARMA_EIO, "malformed MT configuration file"};
+	in.seekg(std::streamoff(p->nn) * 4, std::ios::cur);
+	return bool(in);
+}
+}  // namespace
+
+int arma_mt_file_count(const char* path, int* count) {
+	return guard([&] {
+		ARMA_REQUIRE(path && count, ARMA_EINVAL, "null argument");
+		std::ifstream in(path, std::ios::binary);
+		if (!in)
+			throw Error{ARMA_EIO,
+			            std::string("Mersenne Twister configuration file not found: ") + path};
+		int n = 0;
+		arma_mt_params p;
+		while (read_record(in, &p)) ++n;
+		*count = n;
+	});
+}
+
+int arma_mt_file_read(const char* path, int index, arma_mt_params* out) {
+	return guard([&] {
+		ARMA_REQUIRE(path && out && index >= 0, ARMA_EINVAL, "bad argument");
+		std::ifstream in(path, std::ios::binary);
+		if (!in)
+			throw Error{ARMA_EIO,
+			            std::string("Mersenne Twister configuration file not found: ") + path};
+		arma_mt_params p;
+		for (int k = 0; k <= index; ++k)
+			if (!read_record(in, &p))
+				throw Error{ARMA_EPRNG, "bad number of MT configs"};
+		*out = p;
+	});
+}
+
+int arma_mt_file_write(const char* path, const arma_mt_params* sets, int n) {
+	return guard([&] {
+		ARMA_REQUIRE(path && sets && n > 0, ARMA_EINVAL, "bad argument");
+		std::ofstream out(path, std::ios::binary);
+		ARMA_REQUIRE(bool(out), ARMA_EIO, std::string("cannot write ") + path);
+		for (int k = 0; k < n; ++k) {
+			require_mt(&sets[k]);
+			unsigned char hdr[kMtRecord] = {0};
+			std::memcpy(hdr, &sets[k], sizeof(arma_mt_params));
+			out.write(reinterpret_cast<const char*>(hdr), kMtRecord);
+			// state words: sgenrand_mt(0), which read_parallel_mts replaces anyway
+			uint32_t s = 0;
+			for (int i = 0; i < sets[k].nn; ++i) {
+				const uint32_t w = s & sets[k].wmask;
+				out.write(reinterpret_cast<const char*>(&w), 4);
+				s = 1812433253u * (s ^ (s >> 30)) + uint32_t(i + 1);
+			}
+		}
+		ARMA_REQUIRE(bool(out), ARMA_EIO, std::string("cannot write ") + path);
+	});
+}
+
+int arma_mt_genrand(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed, uint64_t offset,
+                    size_t n, uint32_t* d_out) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && d_out, ARMA_EINVAL, "null argument");
+		require_mt(p);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		launch_mt_generate(&ctx->c, *p, seed, offset, n, d_out);
+	});
+}
+
+// ---------------------------------------------------------------- fit
+int arma_acf_eval(int kind, double amplitude, double velocity, const double alpha[3],
+                  const double beta[2], const double delta[3], const int shape[3],
+                  double* acf) {
+	return guard([&] {
+		ARMA_REQUIRE(alpha && beta && delta && acf, ARMA_EINVAL, "null argument");
+		require_shape(shape, "acf");
+		ARMA_REQUIRE(kind == ARMA_ACF_STANDING || kind == ARMA_ACF_PROPAGATING, ARMA_EINVAL,
+		             "bad ACF function");
+		acf_eval(kind, amplitude, velocity, alpha, beta, delta, shape, acf);
+	});
+}
+
+int arma_ar_fit(const double* acf, const int acf_shape[3], const int order[3], int method,
+                double* phi, double* var_wn) {
+	return guard([&] {
+		ARMA_REQUIRE(acf && phi && var_wn, ARMA_EINVAL, "null argument");
+		require_shape(acf_shape, "acf");
+		require_shape(order, "order");
+		ARMA_REQUIRE(order[0] <= acf_shape[0] && order[1] <= acf_shape[1] &&
+		                 order[2] <= acf_shape[2],
+		             ARMA_EINVAL, "bad AR model order");
+		const int info = fit_gauss_table(acf, acf_shape, order, method, phi, var_wn);
+		ARMA_REQUIRE(info == 0, ARMA_ENUMERIC,
+		             "Yule-Walker matrix is not positive definite (pivot " +
+		                 std::to_string(info) + ")");
+	});
+}
+
+int arma_ar_fit_analytic(int kind, double amplitude, double velocity, const double alpha[3],
+                         const double beta[2], const double delta[3], const int order[3],
+                         double* phi, double* var_wn) {
+	return guard([&] {
+		ARMA_REQUIRE(alpha && beta && delta && phi && var_wn, ARMA_EINVAL, "null argument");
+		require_shape(order, "order");
+		const int info =
+		    fit_analytic(kind, amplitude, velocity, alpha, beta, delta, order, phi, var_wn);
+		ARMA_REQUIRE(info == 0, ARMA_ENUMERIC,
+		             "Yule-Walker matrix is not positive definite (pivot " +
+		                 std::to_string(info) + ")");
+	});
+}
+
+// ---------------------------------------------------------------- noise, AR
+int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed, double stddev,
+                     size_t n, int precision, void* d_out) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && d_out, ARMA_EINVAL, "null argument");
+		require_mt(p);
+		elem_size(precision);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		white_noise(&ctx->c, *p, seed, stddev, n, precision, d_out);
+	});
+}
+
+namespace {
+
+void ar_filter(Ctx* c, const double* phi, const int order[3], const int shape[3],
+               int precision, void* d_zeta) {
+	const int P = order[0] * order[1] * order[2];
+	if (precision == ARMA_FP64) {
+		double* d_phi = static_cast<double*>(scratch_take(c, sizeof(double) * P));
+		ARMA_CUDA_TRY(cudaMemcpyAsync(d_phi, phi, sizeof(double) * P, cudaMemcpyHostToDevice,
+		                              c->stream));
+		launch_ar64(c, d_phi, order, shape, static_cast<double*>(d_zeta));
+	} else {
+		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
+		std::vector<float> hphi(P);
+		for (int i = 0; i < P; ++i) hphi[i] = float(phi[i]);
+		std::vector<double> h(size_t(tx) * ty);
+		intra_slice_response(phi, order, tx, ty, h.data());
+		std::vector<float> hf(h.begin(), h.end());
+		float* d_phi = static_cast<float*>(scratch_take(c, sizeof(float) * P));
+		float* d_h = static_cast<float*>(scratch_take(c, sizeof(float) * hf.size()));
+		ARMA_CUDA_TRY(cudaMemcpyAsync(d_phi, hphi.data(), sizeof(float) * P,
+		                              cudaMemcpyHostToDevice, c->stream));
+		ARMA_CUDA_TRY(cudaMemcpyAsync(d_h, hf.data(), sizeof(float) * hf.size(),
+		                              cudaMemcpyHostToDevice, c->stream));
+		Ar32Surface s;
+		s.nt = shape[0];
+		s.nx = shape[1];
+		s.ny = shape[2];
+		s.pt = order[0];
+		s.px = order[1];
+		s.py = order[2];
+		s.zeta = static_cast<float*>(d_zeta);
+		s.phi = d_phi;
+		s.h = d_h;
+		s.tiles_x = (s.nx + tx - 1) / tx;
+		s.tiles_y = (s.ny + ty - 1) / ty;
+		launch_ar32c(c, {s}, tx, ty, 1);
+		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));  // host vectors go out of scope
+		check_device_error(c);
+	}
+}
+
+void require_order(const int order[3]) {
+	require_shape(order, "order");
+	ARMA_REQUIRE(order[0] <= 16 && order[1] <= 16 && order[2] <= 16, ARMA_ENOTSUP,
+	             "AR order above 16 per dimension is not supported on the device");
+}
+
+}  // namespace
+
+int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3], const int shape[3],
+                   int precision, void* d_zeta) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && phi && d_zeta, ARMA_EINVAL, "null argument");
+		require_shape(shape, "out_grid");
+		require_order(order);
+		elem_size(precision);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		ar_filter(&ctx->c, phi, order, shape, precision, d_zeta);
+	});
+}
+
+int arma_variance_renorm(arma_ctx* ctx, void* d_zeta, const int shape[3], int precision,
+                         double acf0, double* scale_out) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && d_zeta, ARMA_EINVAL, "null argument");
+		require_shape(shape, "out_grid");
+		elem_size(precision);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		double* d_scale = static_cast<double*>(scratch_take(&ctx->c, sizeof(double)));
+		launch_renorm(&ctx->c, d_zeta, shape, precision, acf0, d_scale);
+		double s = 0.0;
+		ARMA_CUDA_TRY(cudaMemcpyAsync(&s, d_scale, sizeof(double), cudaMemcpyDeviceToHost,
+		                              ctx->c.stream));
+		ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+		if (scale_out) *scale_out = s;
+	});
+}
+
+int arma_nit_apply(arma_ctx* ctx, int d, const double params[3], double stdev, int method,
+                   const double interval[2], double eps, int max_iter, int lut_nodes,
+                   double lut_range, size_t n, int precision, void* d_zeta) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && params && d_zeta, ARMA_EINVAL, "null argument");
+		ARMA_REQUIRE(d == ARMA_NIT_GRAM_CHARLIER || d == ARMA_NIT_SKEW_NORMAL, ARMA_EINVAL,
+		             "bad distribution");
+		ARMA_REQUIRE(stdev > 0.0, ARMA_EINVAL, "bad stdev");
+		elem_size(precision);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		if (method == ARMA_NIT_BISECTION) {
+			ARMA_REQUIRE(interval && max_iter > 0 && eps > 0.0, ARMA_EINVAL, "bad cdf_solver");
+			launch_nit_bisection(&ctx->c, d, params, stdev, interval[0], interval[1], eps,
+			                     max_iter, n, precision, d_zeta);
+		} else {
+			ARMA_REQUIRE(lut_nodes >= 4 && lut_range > 0.0, ARMA_EINVAL, "bad NIT table");
+			double x0, dx;
+			std::vector<double> y;
+			nit_build_lut(d, params, stdev, lut_nodes, lut_range, &x0, &dx, y);
+			std::vector<float> yf(y.begin(), y.end());
+			double* d_lut = static_cast<double*>(
+			    scratch_take(&ctx->c, sizeof(double) * lut_nodes + sizeof(float) * lut_nodes));
+			ARMA_CUDA_TRY(cudaMemcpyAsync(d_lut, y.data(), sizeof(double) * lut_nodes,
+			                              cudaMemcpyHostToDevice, ctx->c.stream));
+			ARMA_CUDA_TRY(cudaMemcpyAsync(d_lut + lut_nodes, yf.data(), sizeof(float) * lut_nodes,
+			                              cudaMemcpyHostToDevice, ctx->c.stream));
+			launch_nit_lut(&ctx->c, d_lut, lut_nodes, x0, dx, n, precision, d_zeta);
+			ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+		}
+	});
+}
+
+int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3], int precision,
+                         const double delta[3], double depth, const double* z, int nz,
+                         const int* t_idx, int ntd, void* d_phi_out) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && d_zeta && delta && z && t_idx && d_phi_out, ARMA_EINVAL,
+		             "null argument");
+		require_shape(shape, "out_grid");
+		ARMA_REQUIRE(nz > 0 && ntd > 0, ARMA_EINVAL, "Bad \"domain\": empty");
+		for (int i = 0; i < ntd; ++i)
+			ARMA_REQUIRE(t_idx[i] >= 0 && t_idx[i] < shape[0], ARMA_EINVAL,
+			             "Bad \"domain\": t outside the surface");
+		for (int j = 0; j < nz; ++j)
+			ARMA_REQUIRE(!(z[j] < -depth), ARMA_EINVAL, "min(z) is less than -h");
+		elem_size(precision);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		launch_velocity_linear(&ctx->c, d_zeta, shape, precision, delta, depth, z, nz, t_idx,
+		                       ntd, d_phi_out);
+		ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+	});
+}
+
+// ---------------------------------------------------------------- batches
+namespace {
+
+void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
+	const size_t es = elem_size(precision);
+	std::vector<void*> dz(n);
+	for (int k = 0; k < n; ++k) {
+		require_shape(s[k].shape, "out_grid");
+		require_order(s[k].order);
+		require_mt(&s[k].mt);
+		ARMA_REQUIRE(s[k].phi && s[k].d_zeta, ARMA_EINVAL, "null surface buffer");
+		ARMA_REQUIRE(s[k].var_wn >= 0.0, ARMA_EINVAL, "variance is less than zero");
+		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
+		dz[k] = host ? scratch_take(c, np * es) : s[k].d_zeta;
+	}
+	white_noise_batch(c, s, n, precision, dz);
+	if (precision == ARMA_FP64) {
+		for (int k = 0; k < n; ++k) ar_filter(c, s[k].phi, s[k].order, s[k].shape, precision, dz[k]);
+	} else {
+		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
+		std::vector<Ar32Surface> as(n);
+		std::vector<std::vector<float>> keep;
+		for (int k = 0; k < n; ++k) {
+			const int P = s[k].order[0] * s[k].order[1] * s[k].order[2];
+			std::vector<double> h(size_t(tx) * ty);
+			intra_slice_response(s[k].phi, s[k].order, tx, ty, h.data());
+			keep.emplace_back(P + h.size());
+			std::vector<float>& buf = keep.back();
+			for (int i = 0; i < P; ++i) buf[i] = float(s[k].phi[i]);
+			for (size_t i = 0; i < h.size(); ++i) buf[P + i] = float(h[i]);
+			float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
+			ARMA_CUDA_TRY(cudaMemcpyAsync(d, buf.data(), sizeof(float) * buf.size(),
+			                              cudaMemcpyHostToDevice, c->stream));
+			Ar32Surface& a = as[k];
+			a.nt = s[k].shape[0];
+			a.nx = s[k].shape[1];
+			a.ny = s[k].shape[2];
+			a.pt = s[k].order[0];
+			a.px = s[k].order[1];
+			a.py = s[k].order[2];
+			a.zeta = static_cast<float*>(dz[k]);
+			a.phi = d;
+			a.h = d + P;
+			a.tiles_x = (a.nx + tx - 1) / tx;
+			a.tiles_y = (a.ny + ty - 1) / ty;
+		}
+		launch_ar32c(c, as, tx, ty, 1);
+		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+		check_device_error(c);
+	}
+	double* d_scale = static_cast<double*>(scratch_take(c, sizeof(double) * n));
+	for (int k = 0; k < n; ++k)
+		if (s[k].acf0 > 0.0) launch_renorm(c, dz[k], s[k].shape, precision, s[k].acf0, d_scale + k);
+	if (host) {
+		for (int k = 0; k < n; ++k) {
+			const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
+			ARMA_CUDA_TRY(cudaMemcpyAsync(s[k].d_zeta, dz[k], np * es, cudaMemcpyDeviceToHost,
+			                              c->stream));
+		}
+	}
+	std::vector<double> sc(n, 1.0);
+	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+	for (int k = 0; k < n; ++k) {
+		if (s[k].acf0 > 0.0) {
+			ARMA_CUDA_TRY(cudaMemcpy(&sc[k], d_scale + k, sizeof(double), cudaMemcpyDeviceToHost));
+		}
+		s[k].scale = sc[k];
+	}
+}
+
+}  // namespace
+
+int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n, int precision) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && surfaces && n > 0, ARMA_EINVAL, "bad argument");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		batch(&ctx->c, surfaces, n, precision, false);
+	});
+}
+
+int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n, int precision) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && surfaces && n > 0, ARMA_EINVAL, "bad argument");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		batch(&ctx->c, surfaces, n, precision, true);
+	});
+}
+
+}  // extern "C"

@@ -1,0 +1,132 @@
+// Nonlinear inertialess transform (NIT) of a Gaussian surface to a target
+// distribution: each value z becomes y with F_target(y) = Phi_sigma(z)
+// (reference src/nonlinear/transforms.hh:58-75 driven by
+// src/nonlinear/nit_transform.cc:147-168).
+//
+// Two forms:
+//   bisection  the reference's per-point bisection (src/linalg.hh:199-213):
+//              midpoint, evaluate f(c), move the bracket by the sign of
+//              f(a)*f(c) and f(b)*f(c), stop after max_iter iterations or when
+//              the bracket is no wider than eps or |f(c)| <= eps.  FP64.
+//   LUT        a pointwise map through an FP64-built inverse-CDF table with
+//              cubic Lagrange interpolation between nodes and linear
+//              extrapolation beyond the end nodes.  HBM-bound: one read and
+//              one write per value.
+#include <cmath>
+
+#include "distributions.h"
+#include "internal.h"
+
+namespace armab {
+namespace {
+
+constexpr int kThreads = 256;
+
+__constant__ dist::GL20 c_gl20;
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+nit_bisection_kernel(T* __restrict__ z, unsigned long long n, int d, double p0, double p1,
+                     double p2, double stdev, double a0, double b0, double eps,
+                     int max_iter) {
+	const double p[3] = {p0, p1, p2};
+	const dist::GL20& g = c_gl20;
+	for (unsigned long long idx = blockIdx.x * (unsigned long long)kThreads + threadIdx.x;
+	     idx < n; idx += (unsigned long long)gridDim.x * kThreads) {
+		const double target = dist::gaussian_cdf(double(z[idx]), 0.0, stdev);
+		double a = a0, b = b0, c, fc;
+		int i = 0;
+		do {
+			c = 0.5 * (a + b);
+			fc = dist::target_cdf(d, p, c, g) - target;
+			if ((dist::target_cdf(d, p, a, g) - target) * fc < 0.0) b = c;
+			if ((dist::target_cdf(d, p, b, g) - target) * fc < 0.0) a = c;
+			i++;
+		} while (i < max_iter && (b - a) > eps && fabs(fc) > eps);
+		z[idx] = T(c);
+	}
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+nit_lut_kernel(T* __restrict__ z, unsigned long long n, const T* __restrict__ lut, int nodes,
+               T x0, T inv_dx) {
+	extern __shared__ unsigned char smem_raw[];
+	T* y = reinterpret_cast<T*>(smem_raw);
+	for (int i = threadIdx.x; i < nodes; i += kThreads) y[i] = lut[i];
+	__syncthreads();
+	for (unsigned long long idx = blockIdx.x * (unsigned long long)kThreads + threadIdx.x;
+	     idx < n; idx += (unsigned long long)gridDim.x * kThreads) {
+		const T u = (z[idx] - x0) * inv_dx;
+		T r;
+		if (u <= T(0)) {
+			r = y[0] + (y[1] - y[0]) * u;
+		} else if (u >= T(nodes - 1)) {
+			r = y[nodes - 1] + (y[nodes - 1] - y[nodes - 2]) * (u - T(nodes - 1));
+		} else {
+			int i = int(u);
+			i = min(max(i, 1), nodes - 3);
+			const T s = u - T(i);  // in [-1, 2) relative to node i
+			const T y0 = y[i - 1], y1 = y[i], y2 = y[i + 1], y3 = y[i + 2];
+			// cubic Lagrange through nodes i-1, i, i+1, i+2 at offsets -1,0,1,2
+			const T sm1 = s + T(1), s1 = s - T(1), s2 = s - T(2);
+			r = -y0 * s * s1 * s2 * T(1.0 / 6.0) + y1 * sm1 * s1 * s2 * T(0.5) -
+			    y2 * sm1 * s * s2 * T(0.5) + y3 * sm1 * s * s1 * T(1.0 / 6.0);
+		}
+		z[idx] = r;
+	}
+}
+
+void upload_gl20(Ctx* c) {
+	static bool done[64] = {false};
+	if (c->device >= 0 && c->device < 64 && !done[c->device]) {
+		const dist::GL20& g = dist::gl20_host();
+		ARMA_CUDA_TRY(cudaMemcpyToSymbol(c_gl20, &g, sizeof(g)));
+		done[c->device] = true;
+	}
+}
+
+int grid_for(unsigned long long n, int sms) {
+	const unsigned long long b = (n + kThreads - 1) / kThreads;
+	return int(b < (unsigned long long)(sms * 8) ? (b ? b : 1) : sms * 8);
+}
+
+}  // namespace
+
+void launch_nit_bisection(Ctx* c, int d, const double params[3], double stdev, double a,
+                          double b, double eps, int max_iter, uint64_t n, int precision,
+                          void* d_zeta) {
+	ProfScope prof_(c, "nit");
+	upload_gl20(c);
+	const int grid = grid_for(n, c->num_sms);
+	if (precision == ARMA_FP64)
+		nit_bisection_kernel<double><<<grid, kThreads, 0, c->stream>>>(
+		    static_cast<double*>(d_zeta), n, d, params[0], params[1], params[2], stdev, a, b,
+		    eps, max_iter);
+	else
+		nit_bisection_kernel<float><<<grid, kThreads, 0, c->stream>>>(
+		    static_cast<float*>(d_zeta), n, d, params[0], params[1], params[2], stdev, a, b,
+		    eps, max_iter);
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 1;
+}
+
+void launch_nit_lut(Ctx* c, const double* d_lut_y, int nodes, double x0, double dx,
+                    uint64_t n, int precision, void* d_zeta) {
+	ProfScope prof_(c, "nit");
+	ARMA_REQUIRE(nodes >= 4, ARMA_EINVAL, "NIT table needs at least 4 nodes");
+	const int grid = grid_for(n, c->num_sms);
+	if (precision == ARMA_FP64) {
+		nit_lut_kernel<double><<<grid, kThreads, sizeof(double) * nodes, c->stream>>>(
+		    static_cast<double*>(d_zeta), n, d_lut_y, nodes, x0, 1.0 / dx);
+	} else {
+		// the float table follows the double one in the same scratch block
+		const float* lf = reinterpret_cast<const float*>(d_lut_y + nodes);
+		nit_lut_kernel<float><<<grid, kThreads, sizeof(float) * nodes, c->stream>>>(
+		    static_cast<float*>(d_zeta), n, lf, nodes, float(x0), float(1.0 / dx));
+	}
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 1;
+}
+
+}  // namespace armab

@@ -1,0 +1,103 @@
+// Variance renormalisation of a generated surface.
+//
+// The reference scales the surface by sqrt(acf(0,0,0) / var) where var is
+// taken through stats::variance(Array) = gsl_stats_variance(view.data(), 1,
+// view.numElements()) on the view zeta(shape/2 : shape-1)
+// (src/generator/basic_arma_model.cc:102-106, src/stats/statistics.hh:35-44):
+// numElements() contiguous values starting at the view's first element.  The
+// unbiased variance is computed here in FP64 by a deterministic two-pass
+// reduction (mean, then sum of squared deviations), and the scale stays on
+// the device so the multiply needs no host round trip.
+#include "internal.h"
+
+namespace armab {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kBlocks = 592;  // 4 per SM on 148 SMs
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+partial_sum_kernel(const T* __restrict__ x, unsigned long long n,
+                   const double* __restrict__ mean, double* __restrict__ partial) {
+	__shared__ double sh[kThreads / 32];
+	const double m = mean ? *mean : 0.0;
+	double acc = 0.0;
+	for (unsigned long long i = blockIdx.x * (unsigned long long)kThreads + threadIdx.x; i < n;
+	     i += (unsigned long long)gridDim.x * kThreads) {
+		const double v = double(x[i]);
+		if (mean) {
+			const double d = v - m;
+			acc = fma(d, d, acc);
+		} else {
+			acc += v;
+		}
+	}
+	for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+	if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double s = 0.0;
+		for (int w = 0; w < kThreads / 32; ++w) s += sh[w];
+		partial[blockIdx.x] = s;
+	}
+}
+
+// Fixed-order sum of the block partials.  mode 0: mean = sum / n;
+// mode 1: scale = sqrt(acf0 / (sum / (n-1))).
+__global__ void finish_kernel(const double* __restrict__ partial, int nb,
+                              unsigned long long n, int mode, double acf0,
+                              double* __restrict__ out) {
+	__shared__ double sh[32];
+	double s = 0.0;
+	for (int i = threadIdx.x; i < nb; i += 32) s += partial[i];
+	sh[threadIdx.x] = s;
+	__syncwarp();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int i = 0; i < 32; ++i) t += sh[i];
+		if (mode == 0) *out = t / double(n);
+		else *out = sqrt(acf0 / (t / double(n - 1)));
+	}
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+scale_kernel(T* __restrict__ x, unsigned long long n, const double* __restrict__ scale) {
+	const double s = *scale;
+	for (unsigned long long i = blockIdx.x * (unsigned long long)kThreads + threadIdx.x; i < n;
+	     i += (unsigned long long)gridDim.x * kThreads)
+		x[i] = T(double(x[i]) * s);
+}
+
+template <class T>
+void renorm_impl(Ctx* c, T* z, const int shape[3], double acf0, double* d_scale) {
+	const long long nt = shape[0], nx = shape[1], ny = shape[2];
+	const unsigned long long off = (unsigned long long)((nt / 2) * nx + nx / 2) * ny + ny / 2;
+	const unsigned long long cnt =
+	    (unsigned long long)(nt - nt / 2) * (nx - nx / 2) * (ny - ny / 2);
+	const unsigned long long n = (unsigned long long)nt * nx * ny;
+	ARMA_REQUIRE(cnt >= 2, ARMA_EINVAL, "surface too small for variance renormalisation");
+	double* partial = static_cast<double*>(scratch_take(c, sizeof(double) * kBlocks));
+	double* mean = static_cast<double*>(scratch_take(c, sizeof(double)));
+	partial_sum_kernel<T><<<kBlocks, kThreads, 0, c->stream>>>(z + off, cnt, nullptr, partial);
+	finish_kernel<<<1, 32, 0, c->stream>>>(partial, kBlocks, cnt, 0, acf0, mean);
+	partial_sum_kernel<T><<<kBlocks, kThreads, 0, c->stream>>>(z + off, cnt, mean, partial);
+	finish_kernel<<<1, 32, 0, c->stream>>>(partial, kBlocks, cnt, 1, acf0, d_scale);
+	scale_kernel<T><<<kBlocks, kThreads, 0, c->stream>>>(z, n, d_scale);
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 5;
+}
+
+}  // namespace
+
+void launch_renorm(Ctx* c, void* d_zeta, const int shape[3], int precision,
+                   double acf0, double* d_scale) {
+	ProfScope prof_(c, "renorm");
+	if (precision == ARMA_FP64)
+		renorm_impl(c, static_cast<double*>(d_zeta), shape, acf0, d_scale);
+	else
+		renorm_impl(c, static_cast<float*>(d_zeta), shape, acf0, d_scale);
+}
+
+}  // namespace armab

@@ -1,0 +1,382 @@
+"""Benchmark: surface points/s of batched AR surface generation on B200.
+
+Workload (default ``batched``): 256 independent surfaces in one call, as the
+batched-realisations configuration specifies -- t uniform in [64, 512]; x and
+y drawn log-uniformly from {32, 64, 128, 256}; AR order per surface from
+{4, 6, 8, 10}^3; standing or propagating ACF with b in [0.03, 0.1]
+(standing: a=1.5, c=0.8, d=0.5; propagating: a=1, c=0.6, d=0.3, e=0.2);
+surface i uses dcmt parameter set i mod 16 and seed 42 + i.  Synthetic
+inputs, all drawn from numpy's generator seeded with 42 (per rank: 42 + 1000 *
+rank).  A step is one call of the batched generator: white noise for every
+surface, the FP32 compensated AR filter over all surfaces in one persistent
+launch, and the variance renormalisation.  Coefficients are fitted once
+(FP64) before timing, as model set-up.
+
+`value` is whole-job points/s with buffers resident in HBM; `e2e` is the same
+call writing into pinned host buffers (device->host copies inside the timed
+region).  The plain FP64 path (the reference's exact summation order, one
+surface after another) is timed on the same batch and reported beside it.
+The CPU baseline is the oracle's restatement of the reference's OpenMP block
+wavefront on a bounded sample of the batch.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "surface points/s: batched FP32 vs plain FP64 AR on 1 B200; p50/p99 latency"
+N_SURFACES = 256
+MT_SETS = 16
+
+
+# --------------------------------------------------------------------- workload
+def make_batch(rank: int = 0, n: int = N_SURFACES):
+    rng = np.random.default_rng(42 + 1000 * rank)
+    sizes = [32, 64, 128, 256]
+    orders = [4, 6, 8, 10]
+    out = []
+    for i in range(n):
+        nt = int(rng.integers(64, 513))
+        nx = int(sizes[rng.integers(0, 4)])
+        ny = int(sizes[rng.integers(0, 4)])
+        order = tuple(int(orders[rng.integers(0, 4)]) for _ in range(3))
+        kind = "propagating" if rng.random() < 0.5 else "standing"
+        b = float(rng.uniform(0.03, 0.1))
+        out.append(dict(shape=(nt, nx, ny), order=order, kind=kind, b=b,
+                        seed=42 + i + 1000 * rank, mtset=i % MT_SETS))
+    return out
+
+
+def acf_params(s):
+    if s["kind"] == "standing":
+        return dict(kind=0, amplitude=1.5, velocity=0.8, alpha=[s["b"]] * 3, beta=[0.5, 0.5])
+    return dict(kind=1, amplitude=1.0, velocity=0.6, alpha=[s["b"]] * 3, beta=[0.3, 0.2])
+
+
+def fit_batch(batch):
+    import arma_b200 as A
+    for s in batch:
+        p = acf_params(s)
+        phi, var = A.ar_fit_analytic(p["kind"], s["order"], p["amplitude"], p["velocity"],
+                                     p["alpha"], p["beta"])
+        s["phi"], s["var"], s["acf0"] = phi, var, p["amplitude"]
+    return batch
+
+
+def mt_sets():
+    """The dcmt parameter sets (mt.dat when present, else MT19937 only)."""
+    import arma_b200 as A
+    path = os.path.join(ROOT, "arma_b200", "data", "mt.dat")
+    if os.path.exists(path):
+        n = A.mt_file_count(path)
+        return [A.mt_file_read(path, k) for k in range(n)]
+    return [A.mt19937_params()]
+
+
+def points(batch):
+    return int(sum(np.prod(s["shape"]) for s in batch))
+
+
+def flops(batch):
+    """Algorithmic AR work: 2 (P - 1) flops per point."""
+    return float(sum(np.prod(s["shape"]) * 2 * (np.prod(s["order"]) - 1) for s in batch))
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------- CPU arms
+def cpu_sample(batch, seconds_hint: float):
+    """Pick a bounded sample of the batch for the CPU arms (small surfaces first
+    so the sample covers several orders), about `seconds_hint` of work."""
+    rate = 1.5e9  # flop/s per core, rough planning figure for the scalar loop
+    cores = os.cpu_count() or 1
+    budget = seconds_hint * rate * cores
+    chosen, acc = [], 0.0
+    for s in sorted(batch, key=lambda s: np.prod(s["shape"])):
+        f = np.prod(s["shape"]) * 2 * (np.prod(s["order"]) - 1)
+        if acc + f > budget and chosen:
+            break
+        chosen.append(s)
+        acc += f
+    return chosen
+
+
+def run_cpu(sample, sets, nthreads):
+    """Reference CPU path (oracle restatement of the OpenMP backend): white noise
+    per partition from per-thread MTs, block wavefront filter, renormalisation."""
+    import oracle as O
+    nthreads = nthreads or (os.cpu_count() or 1)
+    ps = [O.MtParams.from_buffer_copy(sets[k % len(sets)]) for k in range(nthreads)]
+    t0 = time.perf_counter()
+    for s in sample:
+        z = O.ar_generate_omp(s["shape"], s["phi"], float(np.sqrt(s["var"])), ps,
+                              [s["seed"] + k for k in range(nthreads)], nthreads)
+        O.variance_renorm(z, s["acf0"])
+    return time.perf_counter() - t0
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    batch = fit_batch(make_batch(0))
+    sets = mt_sets()
+    sample = cpu_sample(batch, 8.0)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        run_cpu(sample[:1], sets, cores)
+    times = [run_cpu(sample, sets, cores) for _ in range(args.steps)]
+    pts = points(sample)
+    t = max(statistics.median(times), 1e-9)
+    v = pts / t
+    desc = (f"{len(sample)} of the {N_SURFACES} surfaces ({pts} points, orders "
+            f"{sorted(set(s['order'] for s in sample))}); OpenMP block wavefront with per-thread "
+            f"MT noise + renormalisation, {cores} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batched-256-surfaces", "sample": desc},
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# --------------------------------------------------------------------- GPU arm
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import arma_b200 as A
+    from arma_b200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    batch = fit_batch(make_batch(rank))
+    sets = mt_sets()
+    ctx = A.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)  # events below bracket the library's stream
+    bufs32 = [torch.empty(s["shape"], dtype=torch.float32, device="cuda") for s in batch]
+    surf32 = [capi.make_surface(s["shape"], s["phi"], s["var"], s["acf0"],
+                                sets[s["mtset"] % len(sets)], s["seed"], b.data_ptr())
+              for s, b in zip(batch, bufs32)]
+    npts = points(batch)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident FP32 compensated batch
+    for _ in range(args.warmup):
+        ctx.batch_generate(surf32, A.FP32C)
+    barrier()
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    launches0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.batch_generate(surf32, A.FP32C)
+        ctx.synchronize()
+        ev1.record(stream)
+        barrier()
+        wall = time.perf_counter() - t0
+    launches = ctx.launch_count() - launches0
+    elapsed = max(ev0.elapsed_time(ev1) / 1e3, 1e-9)
+    elapsed = max_over_ranks(elapsed)
+    ar_ms, ar_n = ctx.profile("ar32c")
+    prof = {k: ctx.profile(k) for k in ("mt", "noise", "ar32c", "renorm")}
+    ctx.set_profiling(False)
+    value = world * npts * args.steps / elapsed
+
+    # ---- e2e: same call into pinned host buffers
+    host = [torch.empty(s["shape"], dtype=torch.float32, pin_memory=True) for s in batch]
+    surfh = [capi.make_surface(s["shape"], s["phi"], s["var"], s["acf0"],
+                               sets[s["mtset"] % len(sets)], s["seed"], h.data_ptr())
+             for s, h in zip(batch, host)]
+    ctx.batch_generate(surfh, A.FP32C, host=True)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        ctx.batch_generate(surfh, A.FP32C, host=True)
+    barrier()
+    e2e_t = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * npts * e2e_steps / e2e_t
+    # parity spot check of the host copy against the device result
+    assert torch.equal(host[0], bufs32[0].cpu())
+    del bufs32
+
+    # ---- plain FP64 path on the same batch (surface after surface)
+    plain = None
+    if not args.skip_plain:
+        bufs64 = [torch.empty(s["shape"], dtype=torch.float64, device="cuda") for s in batch]
+        surf64 = [capi.make_surface(s["shape"], s["phi"], s["var"], s["acf0"],
+                                    sets[s["mtset"] % len(sets)], s["seed"], b.data_ptr())
+                  for s, b in zip(batch, bufs64)]
+        ctx.batch_generate(surf64, A.FP64)  # builds and caches the plane graphs
+        barrier()
+        t0 = time.perf_counter()
+        ctx.batch_generate(surf64, A.FP64)
+        barrier()
+        t64 = max_over_ranks(time.perf_counter() - t0)
+        plain = world * npts / t64
+        del bufs64
+
+    # ---- roofline of the dominant kernel (ar32c)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s at the max SM clock
+    per_launch_flops = flops(batch)  # one ar32c pass over the batch per step
+    ar_s = ar_ms / 1e3 / max(args.steps, 1)
+    achieved = per_launch_flops / ar_s / 1e12 if ar_s > 0 else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        sample = cpu_sample(batch, args.cpu_seconds / 2)
+        cores = os.cpu_count() or 1
+        t = run_cpu(sample, sets, cores)
+        cpu = {"value": points(sample) / t, "unit": "points/s", "cores": cores, "kind": "port",
+               "sample": f"{len(sample)} smallest surfaces of the batch ({points(sample)} points), "
+                         f"OpenMP block wavefront restatement, {t:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (compensated), f64 fit",
+            "data": "synthetic (seeded numpy draws; no external dataset)",
+            "config": {"workload": "batched-256-surfaces",
+                       "surfaces": N_SURFACES, "points_per_rank": npts,
+                       "orders": "{4,6,8,10}^3", "precision": "fp32c",
+                       "l2": "inputs larger than L2 (%.1f GB per rank)" % (npts * 4 / 1e9),
+                       "parallelism": f"dp{world} (independent surfaces per rank)"},
+            "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": npts * 4},
+            "plain_fp64": {"value": plain, "unit": "points/s",
+                           "ratio_fp32c_over_fp64": (value / plain) if plain else None},
+            "gpu_launches": launches,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": (achieved / fp32_peak) if achieved else None,
+                         "traffic": None,
+                         "note": "ar32c: 2(P-1) flop per point over the batch / ar32c device "
+                                 "time; peak = 148 SMs x 128 FP32 lanes x 2 x max SM clock "
+                                 "(MEASURED_PEAKS.json has no FP32 figure)"},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "wall_s_timed": wall,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+/*
+ * arma_b200 — C ABI of the B200 implementation of the ARMA wavy-surface hot
+ * path: Yule-Walker fit, dcmt Mersenne Twister white noise, the causal 3-D AR
+ * filter, variance renormalisation, the nonlinear inertialess transform and
+ * the linear velocity-potential solver.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: ARMA_OK (0) or a negative
+ *     ARMA_E* code.  arma_last_error() returns the calling thread's message.
+ *     No C++ exception crosses this boundary.
+ *   - Arrays are C order with t slowest: zeta is (nt, nx, ny), phi is
+ *     (pt, px, py), velocity potentials are (nt_dom, nz, nx, ny), exactly the
+ *     blitz layouts of the reference (src/arma_driver.hh:56-57).
+ *   - Pointers named d_* are device pointers on the context's device; all
+ *     other pointers are host pointers.  Device work is enqueued on the
+ *     context's stream (arma_ctx_set_stream); calls that return host results
+ *     synchronise that stream.
+ *   - A context is used by one host thread at a time.
+ *
+ * The reference has no C ABI; its operator API is the C++ generator/solver
+ * registry (src/arma_driver.hh:124-134) with the virtual interfaces cited on
+ * each entry point below.  The cgo/ctypes-style binding a maintainer would add
+ * is shown in INTEGRATION.md.
+ */
+#ifndef ARMA_B200_H
+#define ARMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ARMA_B200_VERSION 100
+
+enum {
+	ARMA_OK = 0,
+	ARMA_EINVAL = -1,     /* bad argument (std::invalid_argument in the reference) */
+	ARMA_ECUDA = -2,      /* CUDA runtime error */
+	ARMA_ENOMEM = -3,     /* device allocation failed */
+	ARMA_ETIMEDOUT = -4,  /* a bounded device-side wait gave up */
+	ARMA_EIO = -5,        /* file missing or malformed (std::runtime_error) */
+	ARMA_EPRNG = -6,      /* too few MT parameter sets (PRNG_error, src/errors.hh:10-33) */
+	ARMA_ENUMERIC = -7,   /* singular YW system or negative white-noise variance */
+	ARMA_ENOTSUP = -8     /* registered but not built in this library */
+};
+
+typedef enum { ARMA_FP64 = 0, ARMA_FP32C = 1 } arma_precision;
+typedef enum { ARMA_ACF_STANDING = 0, ARMA_ACF_PROPAGATING = 1 } arma_acf_kind;
+typedef enum {
+	ARMA_FIT_BUNCH_KAUFMAN = 0, /* reference dsysv semantics, per-axis |lag| matrix */
+	ARMA_FIT_CHOLESKY = 1       /* LL^T, per-axis |lag| matrix */
+} arma_fit_method;
+typedef enum { ARMA_NIT_GRAM_CHARLIER = 0, ARMA_NIT_SKEW_NORMAL = 1 } arma_nit_dist;
+typedef enum { ARMA_NIT_BISECTION = 0, ARMA_NIT_LUT = 1 } arma_nit_method;
+
+/* One dcmt parameter set: the reference's mt_struct fields in order
+ * (src/parallel_mt.hh:109-123; on disk in mt.dat as the raw x86-64 struct,
+ * 72 bytes, followed by nn state words). */
+typedef struct {
+	uint32_t aaa;
+	int32_t mm, nn, rr, ww;
+	uint32_t wmask, umask, lmask;
+	int32_t shift0, shift1, shiftB, shiftC;
+	uint32_t maskB, maskC;
+	int32_t i;
+} arma_mt_params;
+
+typedef struct arma_ctx arma_ctx;
+
+/* ---------------------------------------------------------------- context */
+int arma_version(void);
+int arma_last_error(char* buf, size_t len);
+int arma_ctx_create(int device, arma_ctx** out);
+int arma_ctx_destroy(arma_ctx* ctx);
+int arma_ctx_set_stream(arma_ctx* ctx, void* cuda_stream);
+int arma_ctx_synchronize(arma_ctx* ctx);
+/* Kernel launches issued through this context since creation (counter). */
+int arma_ctx_launch_count(arma_ctx* ctx, uint64_t* count);
+/* Per-kernel-class device timing: when enabled, CUDA events are recorded on
+ * the context's stream around each launch of the named classes ("mt",
+ * "noise", "ar64", "ar32c", "renorm", "nit", "velocity").  arma_ctx_profile
+ * synchronises and returns the accumulated milliseconds and launch count of
+ * one class (zeros if none ran); arma_ctx_profile_reset clears them. */
+int arma_ctx_set_profiling(arma_ctx* ctx, int enabled);
+int arma_ctx_profile(arma_ctx* ctx, const char* name, double* ms, uint64_t* launches);
+int arma_ctx_profile_reset(arma_ctx* ctx);
+
+/* ------------------------------------------------- A6: dcmt parameter sets */
+/* Replaces read_parallel_mt_config / read_parallel_mts
+ * (src/parallel_mt.hh:153-168, src/parallel_mt.cc:28-59). */
+int arma_mt_file_count(const char* path, int* count);
+int arma_mt_file_read(const char* path, int index, arma_mt_params* out);
+/* Writes n sets, each followed by nn state words seeded with 0 (the
+ * reference's arma-dcmt writes its creator state; seeding replaces it). */
+int arma_mt_file_write(const char* path, const arma_mt_params* sets, int n);
+/* The standard MT19937 parameter set in dcmt form. */
+int arma_mt19937_params(arma_mt_params* out);
+/* n tempered words of the stream seeded with `seed` (sgenrand_mt then
+ * genrand_mt, src/parallel_mt.hh:236,259), starting at word `offset`. */
+int arma_mt_genrand(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed,
+                    uint64_t offset, size_t n, uint32_t* d_out);
+
+/* ------------------------------------------------------ A1-A5: model fit */
+/* Analytic ACF on the non-negative lag grid (src/acf.hh:18-62). */
+int arma_acf_eval(int kind, double amplitude, double velocity,
+                  const double alpha[3], const double beta[2],
+                  const double delta[3], const int shape[3], double* acf);
+/* Gauss-elimination Yule-Walker fit on a tabulated ACF with the reference's
+ * per-axis |lag| block-Toeplitz matrix (determine_coefficients_gauss,
+ * src/generator/ar_model.cc:97-135; white_noise_variance :55-61). FP64. */
+int arma_ar_fit(const double* acf, const int acf_shape[3], const int order[3],
+                int method, double* phi, double* var_wn);
+/* Same fit for an analytic ACF with the signed-lag matrix
+ * R[p,q] = gamma(p - q) (an extension: equal to the reference's matrix for
+ * standing waves; SPD for propagating waves, where the reference's |lag|
+ * matrix is indefinite).  LL^T Cholesky, FP64. */
+int arma_ar_fit_analytic(int kind, double amplitude, double velocity,
+                         const double alpha[3], const double beta[2],
+                         const double delta[3], const int order[3],
+                         double* phi, double* var_wn);
+
+/* ------------------------------------------------------ A7: white noise */
+/* n normals N(0, stddev^2) in C order from one stream, as
+ * prng::generate_white_noise + std::normal_distribution (Marsaglia polar over
+ * generate_canonical) produce them (src/white_noise.hh:23-58,
+ * src/generator/basic_arma_model.cc:36-48).  precision selects double or
+ * float output (float = the double value rounded). */
+int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed,
+                     double stddev, size_t n, int precision, void* d_out);
+
+/* ------------------------------------------------------ A8: AR filter */
+/* In-place causal AR filter over zeta holding the white noise
+ * (ar_generate_surface, src/generator/ar_model_surf.cc:5-36; backend seam
+ * AR_model::generate_surface, src/generator/ar_model.hh:102-103).
+ * ARMA_FP64 follows the reference's summation order exactly;
+ * ARMA_FP32C runs the compensated FP32 tile wavefront. */
+int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3],
+                   const int shape[3], int precision, void* d_zeta);
+
+/* ------------------------------------------ A10: variance renormalisation */
+/* zeta *= sqrt(acf0 / var) with var the unbiased variance of the
+ * numElements() contiguous values starting at zeta(nt/2, nx/2, ny/2)
+ * (src/generator/basic_arma_model.cc:102-106). */
+int arma_variance_renorm(arma_ctx* ctx, void* d_zeta, const int shape[3],
+                         int precision, double acf0, double* scale_out);
+
+/* ------------------------------------------------------------ A11: NIT */
+/* In place over n values (NIT_transform::transform_realisation,
+ * src/nonlinear/nit_transform.cc:127-168).  params: Gram-Charlier
+ * {skewness, kurtosis(non-excess)}; skew normal {mean, stdev, alpha}.
+ * ARMA_NIT_BISECTION reproduces the per-point bisection on `interval` with
+ * absolute error eps and max_iter iterations; ARMA_NIT_LUT maps through an
+ * inverse-CDF table of lut_nodes nodes over [-lut_range, lut_range]*stdev
+ * built in FP64. */
+int arma_nit_apply(arma_ctx* ctx, int dist, const double params[3],
+                   double stdev, int method, const double interval[2],
+                   double eps, int max_iter, int lut_nodes, double lut_range,
+                   size_t n, int precision, void* d_zeta);
+
+/* ------------------------------------------- V1-V5: linear velocity solver */
+/* Velocity_potential_solver::operator() with the Linear_solver hooks
+ * (src/velocity/basic_solver.cc:38-77, src/velocity/linear_solver.cc:20-184).
+ * t_idx: integer slice indices (the reference truncates domain t values);
+ * z: depth levels; depth may be +INFINITY.  d_phi_out: (ntd, nz, nx, ny). */
+int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3],
+                         int precision, const double delta[3], double depth,
+                         const double* z, int nz, const int* t_idx, int ntd,
+                         void* d_phi_out);
+
+/* ------------------------------------------------ batched generation */
+/* One surface of a batch.  phi/var_wn come from a fit; the noise stream is
+ * (mt, seed); zeta is a device buffer of shape[0]*shape[1]*shape[2] elements
+ * of the batch precision.  acf0 > 0 enables the variance renormalisation. */
+typedef struct {
+	int shape[3];
+	int order[3];
+	const double* phi; /* host, pt*px*py */
+	double var_wn;
+	double acf0;
+	arma_mt_params mt;
+	uint32_t seed;
+	void* d_zeta;
+	double scale; /* out: renormalisation factor */
+} arma_surface;
+
+/* White noise + AR filter (+ renormalisation) for n independent surfaces.
+ * ARMA_FP32C runs all surfaces in one persistent launch; ARMA_FP64 runs the
+ * plain filter surface by surface. */
+int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n,
+                        int precision);
+/* Same, writing each surface into a HOST buffer (d_zeta is then a host
+ * pointer of doubles); host<->device copies are part of the call. */
+int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n,
+                             int precision);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARMA_B200_H */

@@ -1,0 +1,218 @@
+"""GPU parity tests: every device row against the CPU oracle through the C ABI.
+
+Tolerances (stated per test):
+  * MT words: bit-exact.
+  * white noise: the accepted-attempt pattern is bit-exact; values agree to
+    4e-16 relative (device log() vs glibc log()).
+  * FP64 AR filter: bit-exact with the oracle given the same noise (same
+    summation order, explicitly rounded operations).
+  * FP32 compensated AR filter: RMS error <= 1e-5 relative to the FP64 result
+    on the same noise; max-abs error reported.
+  * renormalisation: 1e-12 relative.
+  * NIT bisection: 2e-6 absolute (bisection tolerance 1e-6); NIT LUT: 5e-5.
+"""
+import numpy as np
+import pytest
+
+import arma_b200 as A
+from arma_b200 import capi
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a)).to(dtype).cuda().contiguous()
+
+
+def test_mt_words_bit_exact(ctx, golden):
+    p = A.mt19937_params()
+    out = torch.zeros(4096, dtype=torch.int32, device="cuda")
+    ctx.mt_genrand(p, 42, 4096, out.data_ptr())
+    ctx.synchronize()
+    got = out.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, golden["mt19937_seed42"])
+    # offset: words [1000, 1500)
+    out2 = torch.zeros(500, dtype=torch.int32, device="cuda")
+    ctx.mt_genrand(p, 42, 500, out2.data_ptr(), offset=1000)
+    ctx.synchronize()
+    assert np.array_equal(out2.cpu().numpy().view(np.uint32), golden["mt19937_seed42"][1000:1500])
+
+
+def test_mt_other_parameter_set_and_seed(ctx):
+    p = A.mt19937_params()
+    q = capi.MtParams.from_buffer_copy(p)
+    q.maskB, q.maskC = 0x9d2c5680 ^ 0x10, 0xefc60000
+    for seed in (0, 7, 0xFFFFFFFF):
+        out = torch.zeros(3000, dtype=torch.int32, device="cuda")
+        ctx.mt_genrand(q, seed, 3000, out.data_ptr())
+        ctx.synchronize()
+        oq = O.MtParams.from_buffer_copy(q)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), O.mt_genrand(oq, seed, 3000))
+
+
+@pytest.mark.parametrize("n", [1, 2, 5001, 100000])
+def test_white_noise(ctx, n):
+    p = A.mt19937_params()
+    ref = O.white_noise(O.mt19937_params(), 42, 0.5, n)
+    out = torch.zeros(n, dtype=torch.float64, device="cuda")
+    ctx.white_noise(p, 42, 0.5, n, A.FP64, out.data_ptr())
+    ctx.synchronize()
+    got = out.cpu().numpy()
+    assert np.allclose(got, ref, rtol=4e-16, atol=0)
+    # float output is the double value rounded
+    outf = torch.zeros(n, dtype=torch.float32, device="cuda")
+    ctx.white_noise(p, 42, 0.5, n, A.FP32C, outf.data_ptr())
+    ctx.synchronize()
+    assert np.array_equal(outf.cpu().numpy(), got.astype(np.float32))
+
+
+def test_white_noise_golden(ctx, golden):
+    out = torch.zeros(5001, dtype=torch.float64, device="cuda")
+    ctx.white_noise(A.mt19937_params(), 42, 0.5, 5001, A.FP64, out.data_ptr())
+    ctx.synchronize()
+    assert np.allclose(out.cpu().numpy(), golden["wn_seed42"], rtol=4e-16, atol=0)
+
+
+@pytest.mark.parametrize("case", ["333", "777"])
+def test_ar64_bit_exact(ctx, golden, case):
+    eps, phi = golden["ar_eps_" + case], golden["ar_phi_" + case]
+    z = dev(eps)
+    ctx.ar_filter(phi, eps.shape, A.FP64, z.data_ptr())
+    ctx.synchronize()
+    assert np.array_equal(z.cpu().numpy(), golden["ar_zeta_" + case])
+
+
+@pytest.mark.parametrize("shape,order", [((1, 1, 1), (1, 1, 1)), ((5, 3, 2), (2, 3, 4)),
+                                         ((9, 40, 7), (4, 2, 3)), ((30, 33, 65), (5, 5, 5))])
+def test_ar64_ragged_and_edge(ctx, shape, order):
+    rng = np.random.default_rng(sum(shape) + sum(order))
+    phi = rng.uniform(-0.05, 0.05, order)
+    phi.flat[0] = 0.0
+    eps = rng.standard_normal(shape)
+    z = dev(eps)
+    ctx.ar_filter(phi, shape, A.FP64, z.data_ptr())
+    ctx.synchronize()
+    assert np.array_equal(z.cpu().numpy(), O.ar_filter(eps, phi))
+
+
+def rel_err(a, b):
+    d = a.astype(np.float64) - b
+    return np.sqrt(np.mean(d * d)) / np.sqrt(np.mean(b * b)), np.abs(d).max()
+
+
+@pytest.mark.parametrize("shape,order,kind", [
+    ((24, 20, 20), (7, 7, 7), "standing"),
+    ((40, 50, 70), (4, 6, 8), "standing"),
+    ((64, 48, 40), (10, 10, 10), "propagating"),
+    ((3, 17, 33), (3, 2, 5), "standing"),
+])
+def test_ar32c_vs_fp64(ctx, shape, order, kind):
+    if kind == "standing":
+        phi, var = A.ar_fit_analytic(A.ACF_STANDING, order, 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    else:
+        phi, var = A.ar_fit_analytic(A.ACF_PROPAGATING, order, 1.0, 0.6, [0.04] * 3, [0.3, 0.2])
+    eps = O.white_noise(O.mt19937_params(), 11, np.sqrt(var), int(np.prod(shape))).reshape(shape)
+    ref = O.ar_filter(eps, phi)
+    z = dev(eps.astype(np.float32), torch.float32)
+    ctx.ar_filter(phi, shape, A.FP32C, z.data_ptr())
+    ctx.synchronize()
+    rms, mx = rel_err(z.cpu().numpy(), ref)
+    assert rms <= 1e-5, (rms, mx)
+
+
+def test_renorm(ctx, golden):
+    z = dev(golden["ar_zeta_777"])
+    s = ctx.variance_renorm(z.data_ptr(), z.shape, A.FP64, 1.5)
+    assert abs(s - golden["renorm_scale_777"][0]) <= 1e-12 * s
+    assert np.allclose(z.cpu().numpy(), golden["renorm_zeta_777"], rtol=1e-12, atol=0)
+
+
+def test_nit_bisection(ctx, golden):
+    sd = np.sqrt(1.5)
+    for dist, params, key in [(A.NIT_GRAM_CHARLIER, [0.3, 3.2], "nit_gc"),
+                              (A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.5], "nit_sn")]:
+        z = dev(golden["nit_in"])
+        ctx.nit_apply(dist, params, sd, A.NIT_BISECTION, z.numel(), A.FP64, z.data_ptr(),
+                      interval=(-5, 5))
+        ctx.synchronize()
+        assert np.abs(z.cpu().numpy() - golden[key]).max() <= 2e-6
+
+
+def test_nit_lut(ctx, golden):
+    sd = np.sqrt(1.5)
+    for dist, params, key in [(A.NIT_GRAM_CHARLIER, [0.3, 3.2], "nit_gc"),
+                              (A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.5], "nit_sn")]:
+        for prec, dt in [(A.FP64, torch.float64), (A.FP32C, torch.float32)]:
+            z = dev(golden["nit_in"], dt)
+            ctx.nit_apply(dist, params, sd, A.NIT_LUT, z.numel(), prec, z.data_ptr(),
+                          lut_nodes=1024, lut_range=5.0)
+            ctx.synchronize()
+            assert np.abs(z.cpu().numpy() - golden[key]).max() <= 5e-5
+
+
+def test_batch_fp64_matches_sequential_oracle(ctx):
+    p = A.mt19937_params()
+    shapes = [(20, 16, 24), (12, 33, 9), (30, 8, 8)]
+    orders = [(3, 3, 3), (2, 4, 3), (4, 2, 2)]
+    bufs, surfs, refs = [], [], []
+    for k, (sh, od) in enumerate(zip(shapes, orders)):
+        phi, var = A.ar_fit_analytic(A.ACF_STANDING, od, 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+        b = torch.zeros(sh, dtype=torch.float64, device="cuda")
+        bufs.append(b)
+        surfs.append(capi.make_surface(sh, phi, var, 1.5, p, 42 + k, b.data_ptr()))
+        eps = O.white_noise(O.mt19937_params(), 42 + k, np.sqrt(var), int(np.prod(sh))).reshape(sh)
+        refs.append(O.variance_renorm(O.ar_filter(eps, phi), 1.5))
+    scales = ctx.batch_generate(surfs, A.FP64)
+    for b, (rz, rs), s in zip(bufs, refs, scales):
+        assert abs(s - rs) <= 1e-12 * rs
+        assert np.allclose(b.cpu().numpy(), rz, rtol=1e-12, atol=1e-12)
+
+
+def test_batch_fp32c_alone_equals_in_batch(ctx):
+    """Each surface of an FP32 batch is the same alone and in the mix."""
+    p = A.mt19937_params()
+    shapes = [(40, 64, 64), (25, 32, 96), (60, 20, 40), (16, 100, 33)]
+    orders = [(4, 4, 4), (6, 4, 8), (3, 5, 4), (8, 8, 8)]
+    fits = [A.ar_fit_analytic(A.ACF_STANDING, od, 1.5, 0.8, [0.05] * 3, [0.5, 0.5]) for od in orders]
+
+    def run(idx):
+        bufs, surfs = [], []
+        for k in idx:
+            b = torch.zeros(shapes[k], dtype=torch.float32, device="cuda")
+            bufs.append(b)
+            phi, var = fits[k]
+            surfs.append(capi.make_surface(shapes[k], phi, var, 1.5, p, 100 + k, b.data_ptr()))
+        ctx.batch_generate(surfs, A.FP32C)
+        return [b.cpu().numpy() for b in bufs]
+
+    together = run([0, 1, 2, 3])
+    for k in range(4):
+        alone = run([k])[0]
+        assert np.array_equal(alone, together[k])
+        # and against the FP64 oracle chain on the same noise
+        phi, var = fits[k]
+        eps = O.white_noise(O.mt19937_params(), 100 + k, np.sqrt(var),
+                            int(np.prod(shapes[k]))).reshape(shapes[k])
+        ref, _ = O.variance_renorm(O.ar_filter(eps, phi), 1.5)
+        rms, mx = rel_err(alone, ref)
+        assert rms <= 1e-5, (k, rms, mx)
+
+
+def test_batch_host_buffers(ctx):
+    p = A.mt19937_params()
+    phi, var = A.ar_fit_analytic(A.ACF_STANDING, (3, 3, 3), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    host = np.zeros((10, 12, 14), np.float64)
+    s = capi.make_surface(host.shape, phi, var, 1.5, p, 5, host.ctypes.data)
+    ctx.batch_generate([s], A.FP64, host=True)
+    eps = O.white_noise(O.mt19937_params(), 5, np.sqrt(var), host.size).reshape(host.shape)
+    ref, _ = O.variance_renorm(O.ar_filter(eps, phi), 1.5)
+    assert np.allclose(host, ref, rtol=1e-12, atol=1e-12)
+
+
+def test_errors_are_reported(ctx):
+    with pytest.raises(capi.ArmaError):
+        ctx.ar_filter(np.zeros((2, 2, 2)), (0, 4, 4), A.FP64, 0)
+    with pytest.raises(capi.ArmaError):
+        ctx.white_noise(A.mt19937_params(), 1, -1.0, 10, A.FP64, 0)

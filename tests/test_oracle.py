@@ -1,0 +1,193 @@
+"""CPU tests: pin the oracle against the reference's known answers, against
+libstdc++'s std::mt19937, and against the committed golden fixtures; check the
+oracle's internal consistency (OpenMP wavefront == sequential filter)."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def test_mt_matches_std_mt19937(golden):
+    p = O.mt19937_params()
+    assert np.array_equal(O.mt_genrand(p, 42, 4096), golden["mt19937_seed42"])
+    assert np.array_equal(O.std_mt19937(42, 4096), golden["mt19937_seed42"])
+
+
+def test_mt_10000th_draw_known_answer():
+    # The C++ standard requires the 10000th draw of a default-seeded
+    # std::mt19937 (seed 5489) to be 4123659995.
+    p = O.mt19937_params()
+    assert int(O.mt_genrand(p, 5489, 10000)[-1]) == 4123659995
+
+
+@pytest.mark.parametrize("seed", [0, 1, 42, 0xFFFFFFFF])
+def test_mt_seeds(seed):
+    p = O.mt19937_params()
+    assert np.array_equal(O.mt_genrand(p, seed, 2000), O.std_mt19937(seed, 2000))
+
+
+def test_owen_t_known_answers(known_answers):
+    for h, a, v in known_answers["owen_t"]:
+        assert abs(O.owen_t(h, a) - v) <= 1e-5
+    # identities asserted by the reference test
+    assert abs(O.owen_t(1, 0)) <= 1e-5
+    assert abs(O.owen_t(1, 1) - O.owen_t(-1, 1)) <= 1e-5
+    assert abs(O.owen_t(1, -1) + O.owen_t(1, 1)) <= 1e-5
+
+
+def test_skew_normal_known_answers(known_answers):
+    sn = known_answers["skew_normal"]
+    m, s, a = sn["params"]
+    for x, v in sn["cdf"]:
+        assert abs(O.skew_normal_cdf(x, m, s, a) - v) <= sn["tolerance"]
+
+
+def test_sysv_known_answer(known_answers):
+    k = known_answers["sysv_3x3"]
+    x = O.sysv(np.array(k["a"]).reshape(3, 3), np.array(k["b"]))
+    assert np.allclose(x, k["x"], atol=k["tolerance"])
+
+
+def test_sysv_identity_and_pivoting():
+    assert np.array_equal(O.sysv(np.eye(10), np.ones(10)), np.ones(10))
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((40, 40))
+    a = a + a.T  # symmetric indefinite: exercises 2x2 pivots
+    b = rng.standard_normal(40)
+    assert np.allclose(O.sysv(a, b), np.linalg.solve(a, b), rtol=1e-9, atol=1e-9)
+
+
+def test_ac_matrix_structure():
+    acf = O.acf("standing_wave", (3, 4, 5), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    R = O.ac_matrix(acf, (3, 4, 5))
+    assert R.shape == (60, 60)
+    assert np.array_equal(R, R.T)
+    # entry ((t,x,y),(t',x',y')) = acf(|dt|,|dx|,|dy|)
+    r = (1 * 4 + 3) * 5 + 0
+    c = (2 * 4 + 0) * 5 + 4
+    assert R[r, c] == acf[1, 3, 4]
+
+
+def test_fit_bunch_kaufman_vs_cholesky():
+    acf = O.acf("standing_wave", (7, 7, 7), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    phi_bk, v_bk = O.ar_fit(acf, (7, 7, 7))
+    phi_ch, v_ch = O.ar_fit(acf, (7, 7, 7), "cholesky")
+    assert phi_bk[0, 0, 0] == 0.0
+    assert np.allclose(phi_bk, phi_ch, rtol=0, atol=1e-9)
+    assert v_bk > 0 and abs(v_bk - v_ch) < 1e-12
+
+
+def test_propagating_reference_matrix_is_indefinite():
+    # the reference's per-axis |lag| matrix gives a negative white-noise
+    # variance for the propagating wave (the reference throws there)
+    acf = O.acf("propagating_wave", (10, 10, 10), 1.0, 0.6, [0.04] * 3, [0.3, 0.2])
+    phi, v = O.ar_fit(acf, (10, 10, 10))
+    assert v < 0
+
+
+def test_golden_oracle_outputs(golden):
+    p = O.mt19937_params()
+    assert np.array_equal(O.white_noise(p, 42, 0.5, 5001), golden["wn_seed42"])
+    assert np.array_equal(O.ar_filter(golden["ar_eps_333"], golden["ar_phi_333"]),
+                          golden["ar_zeta_333"])
+    assert np.array_equal(O.ar_filter(golden["ar_eps_777"], golden["ar_phi_777"]),
+                          golden["ar_zeta_777"])
+
+
+def test_white_noise_stats():
+    p = O.mt19937_params()
+    x = O.white_noise(p, 3, 2.0, 200001)
+    assert abs(x.mean()) < 0.02 and abs(x.std() - 2.0) < 0.02
+    # four words per polar attempt, acceptance pi/4
+    w = O.white_noise_words(p, 3, 200001)
+    assert w % 4 == 0
+    assert abs((100001 / (w / 4)) - np.pi / 4) < 0.01
+
+
+def test_ar_filter_impulse_and_truncation():
+    phi = np.zeros((2, 2, 2))
+    phi[0, 0, 1] = 0.5
+    phi[1, 0, 0] = 0.25
+    eps = np.zeros((3, 1, 4))
+    eps[0, 0, 0] = 1.0
+    z = O.ar_filter(eps, phi)
+    # y-direction geometric decay in slice 0, then the two-tap recursion
+    assert np.allclose(z[0, 0], [1, 0.5, 0.25, 0.125])
+    expect = np.zeros(4)
+    for y in range(4):
+        expect[y] = 0.25 * z[0, 0, y] + (0.5 * expect[y - 1] if y else 0.0)
+    assert np.allclose(z[1, 0], expect)
+
+
+@pytest.mark.parametrize("partition", [(0, 0, 0), (3, 4, 5), (7, 7, 7)])
+def test_omp_wavefront_equals_sequential(golden, partition):
+    eps, phi = golden["ar_eps_777"], golden["ar_phi_777"]
+    z = O.ar_filter_omp(eps, phi, nthreads=4, partition=partition)
+    assert np.array_equal(z, golden["ar_zeta_777"])
+
+
+def test_partition_shape_formula():
+    # get_partition_shape (reference src/generator/ar_model.cc:23-50):
+    # guess1 = max(2*order, 10), guess2 = ceil(grid / (7*cbrt(threads))),
+    # result = min + |diff| / 2
+    assert O.partition_shape((400, 128, 128), (10, 10, 10), 8) == (24, 15, 15)
+    assert O.partition_shape((200, 40, 40), (7, 7, 7), 1) == (21, 10, 10)
+    assert O.partition_shape((9, 9, 9), (2, 2, 2), 8, (3, 3, 3)) == (3, 3, 3)
+
+
+def test_omp_generate_with_per_thread_streams():
+    acf = O.acf("standing_wave", (3, 3, 3), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    phi, var = O.ar_fit(acf, (3, 3, 3), "cholesky")
+    p = O.mt19937_params()
+    z = O.ar_generate_omp((20, 16, 16), phi, np.sqrt(var), [p, p], [1, 2], 2)
+    assert np.isfinite(z).all() and z.std() > 0
+    with pytest.raises(RuntimeError):
+        O.ar_generate_omp((20, 16, 16), phi, np.sqrt(var), [p], [1], 2)
+
+
+def test_renorm_contiguous_window(golden):
+    z, s = O.variance_renorm(golden["ar_zeta_777"], 1.5)
+    nt, nx, ny = z.shape
+    off = ((nt // 2) * nx + nx // 2) * ny + ny // 2
+    cnt = (nt - nt // 2) * (nx - nx // 2) * (ny - ny // 2)
+    flat = golden["ar_zeta_777"].ravel()[off:off + cnt]
+    assert abs(s - np.sqrt(1.5 / flat.var(ddof=1))) < 1e-12 * s
+    assert np.array_equal(z, golden["renorm_zeta_777"])
+
+
+def test_nit_bisection(golden):
+    sd = np.sqrt(1.5)
+    y = O.nit_transform(golden["nit_in"], sd, "gram_charlier", [0.3, 3.2], (-5, 5))
+    assert np.array_equal(y, golden["nit_gc"])
+    # the transform is monotone and solves F_target(y) = Phi(x)
+    order = np.argsort(golden["nit_in"])
+    assert np.all(np.diff(y[order]) >= -2e-6)
+    for x, v in list(zip(golden["nit_in"], y))[:50]:
+        assert abs(O.gram_charlier_cdf(v, 0.3, 3.2) - O.gaussian_cdf(x, 0, sd)) < 2e-6
+
+
+def test_fft_matches_numpy():
+    rng = np.random.default_rng(0)
+    for shape in [(8, 16), (12, 10), (32, 32)]:
+        a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        assert np.allclose(O.fft2(a, -1), np.fft.fft2(a), atol=1e-10)
+        assert np.allclose(O.fft2(a, +1), np.fft.ifft2(a) * a.size, atol=1e-10)
+
+
+def test_window_function_infinite_depth_limit():
+    w_inf = O.window_function(16, 16, (0.5, 0.5), -1.0, np.inf)
+    w_deep = O.window_function(16, 16, (0.5, 0.5), -1.0, 1e3)
+    assert np.allclose(w_inf, w_deep, rtol=1e-12)
+    assert np.isfinite(w_inf).all()
+
+
+def test_velocity_golden(golden):
+    v = O.velocity_linear(golden["vel_zeta"], (1.0, 1.0, 1.0), 12.0, [0.0, -1.0, -2.0], [3, 10])
+    assert np.array_equal(v, golden["vel_phi"])
+
+
+def test_zeta_bin_is_big_endian(tmp_path):
+    z = np.arange(24, dtype=np.float64).reshape(2, 3, 4) * 0.5
+    p = str(tmp_path / "zeta.bin")
+    assert O.write_zeta_bin(p, z) == 0
+    assert np.array_equal(np.fromfile(p, dtype=">f8").reshape(2, 3, 4), z)
