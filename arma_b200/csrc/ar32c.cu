@@ -19,8 +19,10 @@
 //      quarter-plane convolution zeta = H * S, where H is the impulse response
 //      of 1 / (1 - A0(z1,z2)) on the tile (precomputed in FP64),
 //   5. stores the slice to the ring and to global memory and publishes it.
-// Sums are plain FP32 FMAs over one (k,i) row of taps, combined across rows
-// with Kahan compensation.  Tiles are handed out through a global ticket
+// The coefficients are carried as hi + lo float pairs (rounding phi to one
+// float perturbs a high-gain recursion far more than FP32 summation does):
+// each (k,i) row of taps is two FP32 FMA chains over one register window, and
+// row totals are combined with Kahan compensation; H likewise.  Tiles are handed out through a global ticket
 // counter in dependency order, so a CTA only ever waits on tiles that are
 // already owned by running CTAs.
 #include <algorithm>
@@ -48,8 +50,10 @@ struct Task {
 	int tiles_x, tiles_y;
 	int ticket_base;
 	float* zeta;
-	const float* phi;
-	const float* h;
+	const float* phi;     // hi part, pt*px*py
+	const float* phi_lo;  // lo part: phi - hi, pt*px*py
+	const float* h;       // hi part of the intra-slice response, TX*TY
+	const float* h_lo;
 	int* flags;
 };
 
@@ -96,16 +100,22 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 	const long long sst = (long long)tk.nx * tk.ny;
 
 	float* ring = smem;                                  // pt slots
-	float* sphi = ring + pt * slot_sz;                   // pt*px*PYP
-	float* sh = sphi + pt * px * PYP;                    // TX*TY
-	float* ss = sh + TX * TY;                            // TX*SW
+	float* sphi = ring + pt * slot_sz;                   // pt*px*PYP (hi)
+	float* slo = sphi + pt * px * PYP;                   // pt*px*PYP (lo)
+	float* sh = slo + pt * px * PYP;                     // TX*TY (hi)
+	float* shl = sh + TX * TY;                           // TX*TY (lo)
+	float* ss = shl + TX * TY;                           // TX*SW
 
 	// stage coefficients (rows padded with zeros), H, zero the ring and S pads
 	for (int q = tid; q < pt * px * PYP; q += NTHREADS) {
 		const int j = q % PYP, ki = q / PYP;
 		sphi[q] = j < PY ? tk.phi[ki * PY + j] : 0.0f;
+		slo[q] = j < PY ? tk.phi_lo[ki * PY + j] : 0.0f;
 	}
-	for (int q = tid; q < TX * TY; q += NTHREADS) sh[q] = tk.h[q];
+	for (int q = tid; q < TX * TY; q += NTHREADS) {
+		sh[q] = tk.h[q];
+		shl[q] = tk.h_lo[q];
+	}
 	for (int q = tid; q < pt * slot_sz; q += NTHREADS) ring[q] = 0.0f;
 	for (int q = tid; q < TX * SW; q += NTHREADS) ss[q] = 0.0f;
 	__syncthreads();
@@ -130,8 +140,12 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		// the slice is solved)
 		for (int q = tid; q < slot_sz; q += NTHREADS) cur[q] = 0.0f;
 
+		// One (k, i) row of taps at a time: the hi and lo coefficient parts are
+		// applied as two FP32 FMA chains over the same register window, and the
+		// row total is Kahan-added to the running sum.
 		auto accumulate_rows = [&](const float* slot, int k) {
 			const float* prow = sphi + (k * px) * PYP;
+			const float* lrow = slo + (k * px) * PYP;
 			for (int i = 0; i < px; ++i) {
 				const float* zr = slot + (xl + hx - i) * W + yl0;
 				float win[R + LH];
@@ -143,7 +157,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 					win[4 * q + 2] = v.z;
 					win[4 * q + 3] = v.w;
 				}
-				float ph[PYP];
+				float ph[PYP], pl[PYP];
 #pragma unroll
 				for (int q = 0; q < PYP / 4; ++q) {
 					const float4 v = reinterpret_cast<const float4*>(prow + i * PYP)[q];
@@ -151,13 +165,21 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 					ph[4 * q + 1] = v.y;
 					ph[4 * q + 2] = v.z;
 					ph[4 * q + 3] = v.w;
+					const float4 u = reinterpret_cast<const float4*>(lrow + i * PYP)[q];
+					pl[4 * q] = u.x;
+					pl[4 * q + 1] = u.y;
+					pl[4 * q + 2] = u.z;
+					pl[4 * q + 3] = u.w;
 				}
 #pragma unroll
 				for (int r = 0; r < R; ++r) {
-					float p = 0.0f;
+					float p = 0.0f, q = 0.0f;
 #pragma unroll
-					for (int j = 0; j < PY; ++j) p = fmaf(ph[j], win[LH + r - j], p);
-					kahan_add(s[r], c[r], p);
+					for (int j = 0; j < PY; ++j) {
+						p = fmaf(ph[j], win[LH + r - j], p);
+						q = fmaf(pl[j], win[LH + r - j], q);
+					}
+					kahan_add(s[r], c[r], p + q);
 				}
 			}
 		};
@@ -206,9 +228,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		for (int dx = 0; dx <= xl; ++dx) {
 			const float* srow = ss + (xl - dx) * SW + SPAD;
 			const float* hrow = sh + dx * TY;
-			float p[R];
-#pragma unroll
-			for (int r = 0; r < R; ++r) p[r] = 0.0f;
+			const float* hlrow = shl + dx * TY;
 			for (int dy0 = 0; dy0 <= yl0; dy0 += R) {
 				// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
 				float w[2 * R];
@@ -221,8 +241,9 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 					w[4 * q + 2] = v.z;
 					w[4 * q + 3] = v.w;
 				}
-				float hv[R];
+				float hv[R], hl[R];
 				const float4* hp = reinterpret_cast<const float4*>(hrow + dy0);
+				const float4* hq = reinterpret_cast<const float4*>(hlrow + dy0);
 #pragma unroll
 				for (int q = 0; q < R / 4; ++q) {
 					const float4 v = hp[q];
@@ -230,14 +251,23 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 					hv[4 * q + 1] = v.y;
 					hv[4 * q + 2] = v.z;
 					hv[4 * q + 3] = v.w;
+					const float4 u = hq[q];
+					hl[4 * q] = u.x;
+					hl[4 * q + 1] = u.y;
+					hl[4 * q + 2] = u.z;
+					hl[4 * q + 3] = u.w;
 				}
 #pragma unroll
-				for (int dd = 0; dd < R; ++dd)
+				for (int r = 0; r < R; ++r) {
+					float p = 0.0f, q = 0.0f;
 #pragma unroll
-					for (int r = 0; r < R; ++r) p[r] = fmaf(hv[dd], w[R + r - dd], p[r]);
+					for (int dd = 0; dd < R; ++dd) {
+						p = fmaf(hv[dd], w[R + r - dd], p);
+						q = fmaf(hl[dd], w[R + r - dd], q);
+					}
+					kahan_add(a[r], ac[r], p + q);
+				}
 			}
-#pragma unroll
-			for (int r = 0; r < R; ++r) kahan_add(a[r], ac[r], p[r]);
 		}
 
 		// 5. store the solved slice and publish it
@@ -257,7 +287,8 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 	}
 }
 
-template <int PY>
+// One launch for the whole batch: each ticket's surface selects the
+// instantiation for its tap count py (warp-uniform switch).
 __global__ void __launch_bounds__(NTHREADS)
 ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
              int* __restrict__ ticket_counter, int* __restrict__ err) {
@@ -278,7 +309,15 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
 		}
 		const Task tk = tasks[lo];
 		const int local = ticket - tk.ticket_base;
-		run_tile<PY>(tk, local / tk.tiles_y, local % tk.tiles_y, smem, err);
+		const int bx = local / tk.tiles_y, by = local % tk.tiles_y;
+		switch (tk.py) {
+#define ARMA_PY_CASE(N) case N: run_tile<N>(tk, bx, by, smem, err); break;
+			ARMA_PY_CASE(1) ARMA_PY_CASE(2) ARMA_PY_CASE(3) ARMA_PY_CASE(4) ARMA_PY_CASE(5)
+			ARMA_PY_CASE(6) ARMA_PY_CASE(7) ARMA_PY_CASE(8) ARMA_PY_CASE(9) ARMA_PY_CASE(10)
+			ARMA_PY_CASE(11) ARMA_PY_CASE(12) ARMA_PY_CASE(13)
+#undef ARMA_PY_CASE
+			default: break;
+		}
 		__syncthreads();
 	}
 }
@@ -286,29 +325,7 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
 size_t smem_bytes(int pt, int px, int py) {
 	const int rows = TX + px - 1;
 	const int pyp = (py + 3) & ~3;
-	return sizeof(float) * (size_t(pt) * rows * W + size_t(pt) * px * pyp + TX * TY + TX * SW);
-}
-
-template <int PY>
-void launch_group(Ctx* c, const std::vector<Task>& tasks, int total, int pt_max, int px_max) {
-	Task* d_tasks = static_cast<Task*>(scratch_take(c, sizeof(Task) * tasks.size()));
-	int* d_ticket = static_cast<int*>(scratch_take(c, sizeof(int)));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_tasks, tasks.data(), sizeof(Task) * tasks.size(),
-	                              cudaMemcpyHostToDevice, c->stream));
-	ARMA_CUDA_TRY(cudaMemsetAsync(d_ticket, 0, sizeof(int), c->stream));
-	const size_t smem = smem_bytes(pt_max, px_max, PY);
-	ARMA_CUDA_TRY(cudaFuncSetAttribute(ar32c_kernel<PY>,
-	                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-	int per_sm = 0;
-	ARMA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ar32c_kernel<PY>,
-	                                                            NTHREADS, smem));
-	ARMA_REQUIRE(per_sm > 0, ARMA_EINVAL, "AR tile does not fit in shared memory");
-	const int grid = std::min(total, per_sm * c->num_sms);
-	ProfScope prof_(c, "ar32c");
-	ar32c_kernel<PY><<<grid, NTHREADS, smem, c->stream>>>(d_tasks, int(tasks.size()), total,
-	                                                     d_ticket, c->d_err);
-	ARMA_CUDA_TRY(cudaGetLastError());
-	c->launches += 1;
+	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + 2 * TX * TY + TX * SW);
 }
 
 }  // namespace
@@ -318,51 +335,59 @@ int ar32c_tile_y() { return TY; }
 
 void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int ty, int) {
 	ARMA_REQUIRE(tx == TX && ty == TY, ARMA_EINVAL, "unsupported AR tile shape");
-	// group by py (compile-time tap count); order each group by work, largest first
-	std::vector<std::vector<int>> groups(MAXO + 1);
+	std::vector<int> order(surfaces.size());
+	size_t smem = 0;
 	for (size_t k = 0; k < surfaces.size(); ++k) {
 		const Ar32Surface& s = surfaces[k];
 		ARMA_REQUIRE(s.px <= TX + 1 && s.py <= MAXO && s.pt >= 1 && s.px >= 1 && s.py >= 1,
 		             ARMA_ENOTSUP, "AR order not supported by the FP32 tile kernel");
-		groups[s.py].push_back(int(k));
+		order[k] = int(k);
+		smem = std::max(smem, smem_bytes(s.pt, s.px, s.py));
 	}
-	for (int py = 1; py <= MAXO; ++py) {
-		auto& g = groups[py];
-		if (g.empty()) continue;
-		std::sort(g.begin(), g.end(), [&](int a, int b) {
-			const Ar32Surface &A = surfaces[a], &B = surfaces[b];
-			return double(A.nt) * A.nx * A.ny * A.pt * A.px > double(B.nt) * B.nx * B.ny * B.pt * B.px;
-		});
-		std::vector<Task> tasks;
-		int total = 0, pt_max = 1, px_max = 1;
-		size_t nflags = 0;
-		for (int k : g) nflags += size_t(surfaces[k].tiles_x) * surfaces[k].tiles_y;
-		int* flags = static_cast<int*>(scratch_take(c, sizeof(int) * nflags));
-		ARMA_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int) * nflags, c->stream));
-		size_t foff = 0;
-		for (int k : g) {
-			const Ar32Surface& s = surfaces[k];
-			Task t;
-			t.nt = s.nt; t.nx = s.nx; t.ny = s.ny;
-			t.pt = s.pt; t.px = s.px; t.py = s.py;
-			t.tiles_x = s.tiles_x; t.tiles_y = s.tiles_y;
-			t.ticket_base = total;
-			t.zeta = s.zeta; t.phi = s.phi; t.h = s.h;
-			t.flags = flags + foff;
-			foff += size_t(s.tiles_x) * s.tiles_y;
-			total += s.tiles_x * s.tiles_y;
-			pt_max = std::max(pt_max, s.pt);
-			px_max = std::max(px_max, s.px);
-			tasks.push_back(t);
-		}
-		switch (py) {
-#define ARMA_PY_CASE(N) case N: launch_group<N>(c, tasks, total, pt_max, px_max); break;
-			ARMA_PY_CASE(1) ARMA_PY_CASE(2) ARMA_PY_CASE(3) ARMA_PY_CASE(4) ARMA_PY_CASE(5)
-			ARMA_PY_CASE(6) ARMA_PY_CASE(7) ARMA_PY_CASE(8) ARMA_PY_CASE(9) ARMA_PY_CASE(10)
-			ARMA_PY_CASE(11) ARMA_PY_CASE(12) ARMA_PY_CASE(13)
-#undef ARMA_PY_CASE
-		}
+	// longest dependency chains first: a surface's wavefront needs about
+	// nt + tiles_x + tiles_y slice steps, each proportional to pt*px*py
+	auto chain = [&](const Ar32Surface& s) {
+		return double(s.nt + s.tiles_x + s.tiles_y) * s.pt * s.px * s.py;
+	};
+	std::sort(order.begin(), order.end(),
+	          [&](int a, int b) { return chain(surfaces[a]) > chain(surfaces[b]); });
+	size_t nflags = 0;
+	for (const auto& s : surfaces) nflags += size_t(s.tiles_x) * s.tiles_y;
+	int* flags = static_cast<int*>(scratch_take(c, sizeof(int) * nflags));
+	ARMA_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int) * nflags, c->stream));
+	std::vector<Task> tasks;
+	int total = 0;
+	size_t foff = 0;
+	for (int k : order) {
+		const Ar32Surface& s = surfaces[k];
+		Task t;
+		t.nt = s.nt; t.nx = s.nx; t.ny = s.ny;
+		t.pt = s.pt; t.px = s.px; t.py = s.py;
+		t.tiles_x = s.tiles_x; t.tiles_y = s.tiles_y;
+		t.ticket_base = total;
+		t.zeta = s.zeta; t.phi = s.phi; t.phi_lo = s.phi_lo; t.h = s.h; t.h_lo = s.h_lo;
+		t.flags = flags + foff;
+		foff += size_t(s.tiles_x) * s.tiles_y;
+		total += s.tiles_x * s.tiles_y;
+		tasks.push_back(t);
 	}
+	Task* d_tasks = static_cast<Task*>(scratch_take(c, sizeof(Task) * tasks.size()));
+	int* d_ticket = static_cast<int*>(scratch_take(c, sizeof(int)));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d_tasks, tasks.data(), sizeof(Task) * tasks.size(),
+	                              cudaMemcpyHostToDevice, c->stream));
+	ARMA_CUDA_TRY(cudaMemsetAsync(d_ticket, 0, sizeof(int), c->stream));
+	ARMA_CUDA_TRY(cudaFuncSetAttribute(ar32c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                   int(smem)));
+	int per_sm = 0;
+	ARMA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ar32c_kernel, NTHREADS,
+	                                                            smem));
+	ARMA_REQUIRE(per_sm > 0, ARMA_EINVAL, "AR tile does not fit in shared memory");
+	const int grid = std::min(total, per_sm * c->num_sms);
+	ProfScope prof_(c, "ar32c");
+	ar32c_kernel<<<grid, NTHREADS, smem, c->stream>>>(d_tasks, int(tasks.size()), total, d_ticket,
+	                                                  c->d_err);
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 1;
 }
 
 }  // namespace armab

@@ -461,6 +461,45 @@ int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed, doub
 
 namespace {
 
+// Device copies of the hi/lo float split of phi and of the intra-slice
+// response H for the FP32 tile kernel.
+Ar32Surface ar32_surface(Ctx* c, const double* phi, const int order[3], const int shape[3],
+                         float* d_zeta) {
+	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
+	const int P = order[0] * order[1] * order[2];
+	std::vector<double> h(size_t(tx) * ty);
+	intra_slice_response(phi, order, tx, ty, h.data());
+	const size_t nh = h.size();
+	std::vector<float> buf(2 * P + 2 * nh);
+	for (int i = 0; i < P; ++i) {
+		buf[i] = float(phi[i]);
+		buf[P + i] = float(phi[i] - double(buf[i]));
+	}
+	for (size_t i = 0; i < nh; ++i) {
+		buf[2 * P + i] = float(h[i]);
+		buf[2 * P + nh + i] = float(h[i] - double(buf[2 * P + i]));
+	}
+	float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice,
+	                              c->stream));
+	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));  // buf is pageable and local
+	Ar32Surface s;
+	s.nt = shape[0];
+	s.nx = shape[1];
+	s.ny = shape[2];
+	s.pt = order[0];
+	s.px = order[1];
+	s.py = order[2];
+	s.zeta = d_zeta;
+	s.phi = d;
+	s.phi_lo = d + P;
+	s.h = d + 2 * P;
+	s.h_lo = d + 2 * P + nh;
+	s.tiles_x = (s.nx + tx - 1) / tx;
+	s.tiles_y = (s.ny + ty - 1) / ty;
+	return s;
+}
+
 void ar_filter(Ctx* c, const double* phi, const int order[3], const int shape[3],
                int precision, void* d_zeta) {
 	const int P = order[0] * order[1] * order[2];
@@ -471,31 +510,8 @@ void ar_filter(Ctx* c, const double* phi, const int order[3], const int shape[3]
 		launch_ar64(c, d_phi, order, shape, static_cast<double*>(d_zeta));
 	} else {
 		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
-		std::vector<float> hphi(P);
-		for (int i = 0; i < P; ++i) hphi[i] = float(phi[i]);
-		std::vector<double> h(size_t(tx) * ty);
-		intra_slice_response(phi, order, tx, ty, h.data());
-		std::vector<float> hf(h.begin(), h.end());
-		float* d_phi = static_cast<float*>(scratch_take(c, sizeof(float) * P));
-		float* d_h = static_cast<float*>(scratch_take(c, sizeof(float) * hf.size()));
-		ARMA_CUDA_TRY(cudaMemcpyAsync(d_phi, hphi.data(), sizeof(float) * P,
-		                              cudaMemcpyHostToDevice, c->stream));
-		ARMA_CUDA_TRY(cudaMemcpyAsync(d_h, hf.data(), sizeof(float) * hf.size(),
-		                              cudaMemcpyHostToDevice, c->stream));
-		Ar32Surface s;
-		s.nt = shape[0];
-		s.nx = shape[1];
-		s.ny = shape[2];
-		s.pt = order[0];
-		s.px = order[1];
-		s.py = order[2];
-		s.zeta = static_cast<float*>(d_zeta);
-		s.phi = d_phi;
-		s.h = d_h;
-		s.tiles_x = (s.nx + tx - 1) / tx;
-		s.tiles_y = (s.ny + ty - 1) / ty;
+		Ar32Surface s = ar32_surface(c, phi, order, shape, static_cast<float*>(d_zeta));
 		launch_ar32c(c, {s}, tx, ty, 1);
-		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));  // host vectors go out of scope
 		check_device_error(c);
 	}
 }
@@ -615,31 +631,8 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 	} else {
 		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
 		std::vector<Ar32Surface> as(n);
-		std::vector<std::vector<float>> keep;
-		for (int k = 0; k < n; ++k) {
-			const int P = s[k].order[0] * s[k].order[1] * s[k].order[2];
-			std::vector<double> h(size_t(tx) * ty);
-			intra_slice_response(s[k].phi, s[k].order, tx, ty, h.data());
-			keep.emplace_back(P + h.size());
-			std::vector<float>& buf = keep.back();
-			for (int i = 0; i < P; ++i) buf[i] = float(s[k].phi[i]);
-			for (size_t i = 0; i < h.size(); ++i) buf[P + i] = float(h[i]);
-			float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
-			ARMA_CUDA_TRY(cudaMemcpyAsync(d, buf.data(), sizeof(float) * buf.size(),
-			                              cudaMemcpyHostToDevice, c->stream));
-			Ar32Surface& a = as[k];
-			a.nt = s[k].shape[0];
-			a.nx = s[k].shape[1];
-			a.ny = s[k].shape[2];
-			a.pt = s[k].order[0];
-			a.px = s[k].order[1];
-			a.py = s[k].order[2];
-			a.zeta = static_cast<float*>(dz[k]);
-			a.phi = d;
-			a.h = d + P;
-			a.tiles_x = (a.nx + tx - 1) / tx;
-			a.tiles_y = (a.ny + ty - 1) / ty;
-		}
+		for (int k = 0; k < n; ++k)
+			as[k] = ar32_surface(c, s[k].phi, s[k].order, s[k].shape, static_cast<float*>(dz[k]));
 		launch_ar32c(c, as, tx, ty, 1);
 		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 		check_device_error(c);

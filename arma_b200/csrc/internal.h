@@ -115,8 +115,10 @@ struct Ar32Surface {
 	int nt, nx, ny;
 	int pt, px, py;
 	float* zeta;           // device, in place (noise in, surface out)
-	const float* phi;      // device, pt*px*py
-	const float* h;        // device, intra-slice impulse response (TX*TY)
+	const float* phi;      // device, pt*px*py, hi part of the FP64 coefficients
+	const float* phi_lo;   // device, pt*px*py, phi - hi
+	const float* h;        // device, intra-slice impulse response (TX*TY), hi
+	const float* h_lo;     // device, lo part of h
 	int tiles_x, tiles_y;  // spatial tile grid
 };
 void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx,

@@ -216,3 +216,39 @@ def test_errors_are_reported(ctx):
         ctx.ar_filter(np.zeros((2, 2, 2)), (0, 4, 4), A.FP64, 0)
     with pytest.raises(capi.ArmaError):
         ctx.white_noise(A.mt19937_params(), 1, -1.0, 10, A.FP64, 0)
+
+
+def test_velocity_fp64_golden(ctx, golden):
+    """Linear solver, FP64: equal to the oracle up to FFT rounding
+    (tolerance 1e-9 of the largest |phi|)."""
+    zeta = golden["vel_zeta"]
+    ref = golden["vel_phi"]
+    z = dev(zeta)
+    out = torch.zeros(ref.shape, dtype=torch.float64, device="cuda")
+    ctx.velocity_linear(z.data_ptr(), zeta.shape, A.FP64, (1.0, 1.0, 1.0), 12.0,
+                        [0.0, -1.0, -2.0], [3, 10], out.data_ptr())
+    got = out.cpu().numpy()
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 1e-9 * scale
+
+
+@pytest.mark.parametrize("shape,depth,zs,tidx", [
+    ((12, 32, 64), np.inf, [0.0, -1.0, -2.0, -4.0], [0, 5, 11]),
+    ((6, 16, 16), 12.0, [0.0, -3.0], [0, 1, 4, 5]),
+    ((3, 64, 32), np.inf, [0.0], [0, 1, 2]),
+])
+def test_velocity_vs_oracle(ctx, shape, depth, zs, tidx):
+    """FP64 within 1e-9 and FP32 within 2e-4 of max|phi| against the oracle,
+    including the first/last slice one-sided derivatives and infinite depth."""
+    phi, var = A.ar_fit_analytic(A.ACF_PROPAGATING, (3, 3, 3), 1.0, 0.6, [0.04] * 3, [0.3, 0.2])
+    eps = O.white_noise(O.mt19937_params(), 3, np.sqrt(var), int(np.prod(shape))).reshape(shape)
+    zeta = O.ar_filter(eps, phi)
+    ref = O.velocity_linear(zeta, (1.0, 1.0, 1.0), depth, zs, tidx)
+    scale = np.abs(ref).max()
+    for prec, dt, tol in [(A.FP64, torch.float64, 1e-9), (A.FP32C, torch.float32, 2e-4)]:
+        z = dev(zeta, dt)
+        out = torch.zeros(ref.shape, dtype=dt, device="cuda")
+        ctx.velocity_linear(z.data_ptr(), shape, prec, (1.0, 1.0, 1.0), depth, zs, tidx,
+                            out.data_ptr())
+        got = out.cpu().numpy().astype(np.float64)
+        assert np.abs(got - ref).max() <= tol * scale, (prec, np.abs(got - ref).max() / scale)
