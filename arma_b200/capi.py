@@ -35,7 +35,7 @@ EXPORTS = (
     "arma_mt19937_params", "arma_mt_genrand", "arma_acf_eval", "arma_ar_fit",
     "arma_ar_fit_analytic", "arma_white_noise", "arma_ar_filter",
     "arma_variance_renorm", "arma_nit_apply", "arma_velocity_linear",
-    "arma_batch_generate", "arma_batch_generate_host",
+    "arma_batch_generate", "arma_batch_generate_host", "arma_ar_filter_fp32c_noalloc",
 )
 
 
@@ -112,6 +112,7 @@ def lib():
             "arma_velocity_linear": (i, [vp, vp, ip, i, dp, d, dp, i, ip, i, vp]),
             "arma_batch_generate": (i, [vp, C.POINTER(Surface), i, i]),
             "arma_batch_generate_host": (i, [vp, C.POINTER(Surface), i, i]),
+            "arma_ar_filter_fp32c_noalloc": (i, [vp, dp, ip, ip, vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -291,6 +292,14 @@ class Context:
         for k, s in enumerate(surfaces):
             s.scale = arr[k].scale
         return [arr[k].scale for k in range(len(surfaces))]
+
+
+def ar_filter_fp32c_noalloc(stream_ptr: int, phi, shape, d_zeta: int):
+    """Allocation-free FP32 AR filter of one surface on `stream_ptr` (0 = the
+    default stream); see ``arma_ar_filter_fp32c_noalloc`` in the header."""
+    phi = np.ascontiguousarray(phi, np.float64)
+    _check(lib().arma_ar_filter_fp32c_noalloc(C.c_void_p(stream_ptr), _dp(phi), _i3(phi.shape),
+                                              _i3(shape), C.c_void_p(d_zeta)))
 
 
 def make_surface(shape, phi, var_wn, acf0, mt: MtParams, seed: int, buf_ptr: int) -> Surface:

@@ -391,3 +391,146 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 }
 
 }  // namespace armab
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot allocate device memory at the point where they filter a
+// surface: code that runs inside another framework's memory pool and must not
+// make stray cudaMalloc calls, latency-bound serving loops that forbid
+// allocation (and its implicit synchronisation) on the request path, and
+// plugins loaded into processes whose allocator owns the whole device.  This
+// entry point runs the same FP32 filter kernel on one surface with every
+// piece of scratch it needs (the tile task, the ticket counter, the error
+// word, the per-tile publication counters and the hi/lo coefficient and
+// intra-slice-response tables) in one file-scope __device__ array of
+// kStaticScratchBytes (64 KiB), which every GPU that loads this library holds
+// until the process exits.
+//
+//   * Limits: at most kStaticMaxTiles (8192) tiles of 16 x 32 points per time
+//     slice and at most kStaticMaxTaps (2048) AR coefficients; larger
+//     requests are rejected with ARMA_EINVAL.
+//   * The first call on a device looks up the array's device address with
+//     cudaGetSymbolAddress and raises the kernel's shared-memory limit; make
+//     that first call before any stream capture.
+//   * Every call reuses the same array and leaves the last call's contents in
+//     it; each call clears the counters it relies on.  Calls whose work
+//     overlaps on the GPU (other streams or threads) race on the array and
+//     must be serialised by the caller.
+//   * It calls no cudaMalloc, cudaFree or allocating library routine.
+namespace armab {
+namespace {
+
+constexpr size_t kStaticScratchBytes = 64 * 1024;
+constexpr int kStaticMaxTiles = 8192;
+constexpr int kStaticMaxTaps = 2048;
+// byte offsets inside the array
+constexpr size_t kOffTask = 0;
+constexpr size_t kOffTicket = 256;
+constexpr size_t kOffErr = 260;
+constexpr size_t kOffFlags = 512;
+constexpr size_t kOffPhi = kOffFlags + sizeof(int) * kStaticMaxTiles;
+constexpr size_t kOffH = kOffPhi + 2 * sizeof(float) * kStaticMaxTaps;
+constexpr size_t kStaticEnd = kOffH + 2 * sizeof(float) * TX * TY;
+static_assert(kStaticEnd <= kStaticScratchBytes, "static scratch layout overflows");
+static_assert(sizeof(Task) <= kOffTicket, "task record overflows its slot");
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_static_addr[kMaxDevices] = {nullptr};
+bool g_static_ready[kMaxDevices] = {false};
+
+}  // namespace
+}  // namespace armab
+
+extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, const int order[3],
+                                            const int shape[3], float* d_zeta) {
+	using namespace armab;
+	auto fail = [](int code, const char* msg) {
+		set_error(msg);
+		return code;
+	};
+	if (!phi || !order || !shape || !d_zeta) return fail(ARMA_EINVAL, "null argument");
+	if (shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0)
+		return fail(ARMA_EINVAL, "Bad \"out_grid\": dimensions must be positive");
+	if (order[0] < 1 || order[1] < 1 || order[2] < 1 || order[1] > TX + 1 || order[2] > MAXO)
+		return fail(ARMA_ENOTSUP, "AR order not supported by the FP32 tile kernel");
+	const int P = order[0] * order[1] * order[2];
+	if (P > kStaticMaxTaps)
+		return fail(ARMA_EINVAL, "allocation-free AR filter: more than 2048 coefficients");
+	const int tiles_x = (shape[1] + TX - 1) / TX, tiles_y = (shape[2] + TY - 1) / TY;
+	if ((long long)tiles_x * tiles_y > kStaticMaxTiles)
+		return fail(ARMA_EINVAL,
+		            "allocation-free AR filter: slice needs more than 8192 tiles of 16x32 points");
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+		return fail(ARMA_ECUDA, "cudaGetDevice failed");
+	const size_t smem = smem_bytes(order[0], order[1], order[2]);
+	if (!g_static_ready[dev]) {
+		void* p = nullptr;
+		if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess)
+			return fail(ARMA_ECUDA, "cudaGetSymbolAddress of the static scratch failed");
+		g_static_addr[dev] = static_cast<unsigned char*>(p);
+		g_static_ready[dev] = true;
+	}
+	if (cudaFuncSetAttribute(ar32c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                         int(smem)) != cudaSuccess)
+		return fail(ARMA_ECUDA, "cudaFuncSetAttribute failed");
+	unsigned char* base = g_static_addr[dev];
+	float* d_phi = reinterpret_cast<float*>(base + kOffPhi);
+	float* d_h = reinterpret_cast<float*>(base + kOffH);
+	// host-side tables on the stack
+	double h[TX * TY];
+	intra_slice_response(phi, order, TX, TY, h);
+	float hbuf[2 * TX * TY];
+	for (int i = 0; i < TX * TY; ++i) {
+		hbuf[i] = float(h[i]);
+		hbuf[TX * TY + i] = float(h[i] - double(hbuf[i]));
+	}
+	float pbuf[2 * kStaticMaxTaps];
+	for (int i = 0; i < P; ++i) {
+		pbuf[i] = float(phi[i]);
+		pbuf[P + i] = float(phi[i] - double(pbuf[i]));
+	}
+	Task t;
+	t.nt = shape[0]; t.nx = shape[1]; t.ny = shape[2];
+	t.pt = order[0]; t.px = order[1]; t.py = order[2];
+	t.tiles_x = tiles_x; t.tiles_y = tiles_y;
+	t.ticket_base = 0;
+	t.zeta = d_zeta;
+	t.phi = d_phi;
+	t.phi_lo = d_phi + P;
+	t.h = d_h;
+	t.h_lo = d_h + TX * TY;
+	t.flags = reinterpret_cast<int*>(base + kOffFlags);
+	int* d_ticket = reinterpret_cast<int*>(base + kOffTicket);
+	int* d_err = reinterpret_cast<int*>(base + kOffErr);
+	const int ntiles = tiles_x * tiles_y;
+	int per_sm = 0, sms = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ar32c_kernel, NTHREADS, smem) !=
+	        cudaSuccess ||
+	    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+		return fail(ARMA_ECUDA, "occupancy query failed");
+	if (per_sm <= 0) return fail(ARMA_EINVAL, "AR tile does not fit in shared memory");
+	const int grid = std::min(ntiles, per_sm * sms);
+	if (cudaMemcpyAsync(base + kOffTask, &t, sizeof(t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+	    cudaMemcpyAsync(d_phi, pbuf, sizeof(float) * 2 * P, cudaMemcpyHostToDevice, st) !=
+	        cudaSuccess ||
+	    cudaMemcpyAsync(d_h, hbuf, sizeof(hbuf), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+	    cudaMemsetAsync(base + kOffTicket, 0, 8, st) != cudaSuccess ||
+	    cudaMemsetAsync(t.flags, 0, sizeof(int) * ntiles, st) != cudaSuccess)
+		return fail(ARMA_ECUDA, "staging the allocation-free AR filter failed");
+	ar32c_kernel<<<grid, NTHREADS, smem, st>>>(reinterpret_cast<const Task*>(base + kOffTask), 1,
+	                                           ntiles, d_ticket, d_err);
+	if (cudaGetLastError() != cudaSuccess) return fail(ARMA_ECUDA, "AR kernel launch failed");
+	int herr = 0;
+	if (cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+	    cudaStreamSynchronize(st) != cudaSuccess)
+		return fail(ARMA_ECUDA, "AR kernel failed");
+	if (herr == DEV_TIMEOUT)
+		return fail(ARMA_ETIMEDOUT, "a bounded device wait gave up (tile dependency not met)");
+	if (herr != DEV_OK) return fail(ARMA_ECUDA, "device-side check failed");
+	return ARMA_OK;
+}

@@ -139,6 +139,21 @@ int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed,
 int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3],
                    const int shape[3], int precision, void* d_zeta);
 
+/* Allocation-free variant of arma_ar_filter(..., ARMA_FP32C, ...) for one
+ * surface: no counterpart in the reference.  For callers that cannot allocate
+ * device memory on their calling path (code inside another framework's memory
+ * pool, serving loops that forbid allocation, plugins whose host process owns
+ * the device allocator).  It needs no context: work goes to `stream` (0 = the
+ * legacy default stream) on the current device, and all scratch lives in one
+ * 64 KiB __device__ array that every GPU loading the library holds until exit.
+ * Limits: <= 2048 coefficients and <= 8192 tiles of 16x32 points per slice;
+ * larger requests fail with ARMA_EINVAL.  The first call on a device sets up
+ * the array's address and the kernel's shared-memory limit, so make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  Synchronises `stream`. */
+int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, const int order[3],
+                                 const int shape[3], float* d_zeta);
+
 /* ------------------------------------------ A10: variance renormalisation */
 /* zeta *= sqrt(acf0 / var) with var the unbiased variance of the
  * numElements() contiguous values starting at zeta(nt/2, nx/2, ny/2)
