@@ -37,7 +37,8 @@ constexpr int TX = 16;            // tile rows (x)
 constexpr int TY = 32;            // tile columns (y)
 constexpr int R = 8;              // outputs per thread along y
 constexpr int STRIPS = TY / R;    // threads per tile row
-constexpr int NTHREADS = TX * STRIPS;
+constexpr int GROUP = TX * STRIPS; // threads covering the tile once
+constexpr int NTHREADS = 2 * GROUP; // two groups split the tap rows
 constexpr int LH = 12;            // left (y) halo columns held in the ring
 constexpr int W = LH + TY;        // ring row width (floats)
 constexpr int SPAD = TY + 8;      // zero padding left of each S row
@@ -89,22 +90,25 @@ __device__ bool wait_flag(const int* flag, int need, int* err) {
 template <int PY>
 __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) {
 	const int tid = threadIdx.x;
-	const int xl = tid / STRIPS;            // tile-local row
-	const int yl0 = (tid % STRIPS) * R;     // tile-local first column
+	const int grp = tid / GROUP;                 // 0 or 1: halves of the tap rows
+	const int lt = tid % GROUP;
+	const int xl = lt / STRIPS;                  // tile-local row
+	const int yl0 = (lt % STRIPS) * R;           // tile-local first column
 	const int pt = tk.pt, px = tk.px;
 	const int hx = px - 1;
 	const int rows = TX + hx;
 	const int slot_sz = rows * W;
-	constexpr int PYP = (PY + 3) & ~3;      // padded tap row
+	constexpr int PYP = (PY + 3) & ~3;           // padded tap row
 	const int x0 = bx * TX, y0 = by * TY;
 	const long long sst = (long long)tk.nx * tk.ny;
 
-	float* ring = smem;                                  // pt slots
-	float* sphi = ring + pt * slot_sz;                   // pt*px*PYP (hi)
-	float* slo = sphi + pt * px * PYP;                   // pt*px*PYP (lo)
-	float* sh = slo + pt * px * PYP;                     // TX*TY (hi)
-	float* shl = sh + TX * TY;                           // TX*TY (lo)
-	float* ss = shl + TX * TY;                           // TX*SW
+	float* ring = smem;                          // pt slots
+	float* sphi = ring + pt * slot_sz;           // pt*px*PYP (hi)
+	float* slo = sphi + pt * px * PYP;           // pt*px*PYP (lo)
+	float* sh = slo + pt * px * PYP;             // TX*TY (hi)
+	float* shl = sh + TX * TY;                   // TX*TY (lo)
+	float* ss = shl + TX * TY;                   // TX*SW
+	float* comb = ss + TX * SW;                  // GROUP*R: group 1 partials
 
 	// stage coefficients (rows padded with zeros), H, zero the ring and S pads
 	for (int q = tid; q < pt * px * PYP; q += NTHREADS) {
@@ -124,29 +128,36 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 	const int* fW = (bx > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by : nullptr;
 	const int* fN = (by > 0) ? tk.flags + bx * tk.tiles_y + by - 1 : nullptr;
 	const int* fNW = (bx > 0 && by > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by - 1 : nullptr;
+	// H-phase share of this group: rows 0-7 split dx at 4, rows 8-15 at 8, so
+	// every warp runs at most 8 dx iterations
+	const int half = xl >> 3;
+	const int dx_lo = grp == 0 ? 0 : (half ? 8 : 4);
+	const int dx_hi = grp == 0 ? (half ? 8 : 4) : TX;
 
 	for (int t = 0; t < tk.nt; ++t) {
 		float* cur = ring + (t % pt) * slot_sz;
 		float* zt = tk.zeta + t * sst;
-		// noise of this thread's strip (own tile: written by an earlier kernel)
+		// group 0 starts from the noise of its strip (own tile: written by an
+		// earlier kernel), group 1 from zero
 		float s[R], c[R];
 #pragma unroll
 		for (int r = 0; r < R; ++r) {
 			const int gy = y0 + yl0 + r;
-			s[r] = (gx < tk.nx && gy < tk.ny) ? zt[(long long)gx * tk.ny + gy] : 0.0f;
+			s[r] = (grp == 0 && gx < tk.nx && gy < tk.ny) ? zt[(long long)gx * tk.ny + gy] : 0.0f;
 			c[r] = 0.0f;
 		}
 		// clear the current slot (halo is refilled below; in-tile stays 0 until
 		// the slice is solved)
 		for (int q = tid; q < slot_sz; q += NTHREADS) cur[q] = 0.0f;
 
-		// One (k, i) row of taps at a time: the hi and lo coefficient parts are
-		// applied as two FP32 FMA chains over the same register window, and the
-		// row total is Kahan-added to the running sum.
+		// One (k, i) row of taps at a time, rows alternating between the two
+		// groups: the hi and lo coefficient parts are applied as two FP32 FMA
+		// chains over the same register window, and the row total is
+		// Kahan-added to the running sum.
 		auto accumulate_rows = [&](const float* slot, int k) {
 			const float* prow = sphi + (k * px) * PYP;
 			const float* lrow = slo + (k * px) * PYP;
-			for (int i = 0; i < px; ++i) {
+			for (int i = (k * px + grp) & 1; i < px; i += 2) {
 				const float* zr = slot + (xl + hx - i) * W + yl0;
 				float win[R + LH];
 #pragma unroll
@@ -213,11 +224,18 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		accumulate_rows(cur, 0);
 
 		// 4. S = noise + all terms outside the unknown in-tile part
+		if (grp == 1) {
 #pragma unroll
-		for (int r = 0; r < R; ++r) {
-			const int gy = y0 + yl0 + r;
-			const bool valid = gx < tk.nx && gy < tk.ny;
-			ss[xl * SW + SPAD + yl0 + r] = valid ? (s[r] - c[r]) : 0.0f;
+			for (int r = 0; r < R; ++r) comb[lt * R + r] = s[r] - c[r];
+		}
+		__syncthreads();
+		if (grp == 0) {
+#pragma unroll
+			for (int r = 0; r < R; ++r) {
+				const int gy = y0 + yl0 + r;
+				const bool valid = gx < tk.nx && gy < tk.ny;
+				ss[xl * SW + SPAD + yl0 + r] = valid ? (s[r] + (comb[lt * R + r] - c[r])) : 0.0f;
+			}
 		}
 		__syncthreads();
 
@@ -225,7 +243,8 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		float a[R], ac[R];
 #pragma unroll
 		for (int r = 0; r < R; ++r) { a[r] = 0.0f; ac[r] = 0.0f; }
-		for (int dx = 0; dx <= xl; ++dx) {
+		const int dx_end = min(dx_hi - 1, xl);
+		for (int dx = dx_lo; dx <= dx_end; ++dx) {
 			const float* srow = ss + (xl - dx) * SW + SPAD;
 			const float* hrow = sh + dx * TY;
 			const float* hlrow = shl + dx * TY;
@@ -271,13 +290,20 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		}
 
 		// 5. store the solved slice and publish it
-		float* own = cur + hx * W + LH;
+		if (grp == 1) {
 #pragma unroll
-		for (int r = 0; r < R; ++r) {
-			const float v = a[r] - ac[r];
-			own[xl * W + yl0 + r] = v;
-			const int gy = y0 + yl0 + r;
-			if (gx < tk.nx && gy < tk.ny) zt[(long long)gx * tk.ny + gy] = v;
+			for (int r = 0; r < R; ++r) comb[lt * R + r] = a[r] - ac[r];
+		}
+		__syncthreads();
+		if (grp == 0) {
+			float* own = cur + hx * W + LH;
+#pragma unroll
+			for (int r = 0; r < R; ++r) {
+				const float v = a[r] + (comb[lt * R + r] - ac[r]);
+				own[xl * W + yl0 + r] = v;
+				const int gy = y0 + yl0 + r;
+				if (gx < tk.nx && gy < tk.ny) zt[(long long)gx * tk.ny + gy] = v;
+			}
 		}
 		__syncthreads();
 		if (tid == 0) {
@@ -289,7 +315,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 
 // One launch for the whole batch: each ticket's surface selects the
 // instantiation for its tap count py (warp-uniform switch).
-__global__ void __launch_bounds__(NTHREADS)
+__global__ void __launch_bounds__(NTHREADS, 3)
 ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
              int* __restrict__ ticket_counter, int* __restrict__ err) {
 	extern __shared__ __align__(16) float smem[];
@@ -325,7 +351,8 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
 size_t smem_bytes(int pt, int px, int py) {
 	const int rows = TX + px - 1;
 	const int pyp = (py + 3) & ~3;
-	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + 2 * TX * TY + TX * SW);
+	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + 2 * TX * TY + TX * SW +
+	                        GROUP * R);
 }
 
 }  // namespace

@@ -242,6 +242,8 @@ int arma_ctx_destroy(arma_ctx* ctx) {
 			cudaEventDestroy(p.stop);
 		}
 		for (auto& kv : ctx->c.graphs) cudaGraphExecDestroy(kv.second);
+		for (auto& kv : ctx->c.mt_tables)
+			for (int32_t* d : kv.second.bits) cudaFree(d);
 		for (auto& ch : ctx->chunks) cudaFree(ch.first);
 		cudaFree(ctx->c.d_err);
 		if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);

@@ -51,6 +51,13 @@ struct Ctx {
 	int num_sms = 148;
 	// cached CUDA graphs for the FP64 plane sweep, keyed by a string
 	std::map<std::string, cudaGraphExec_t> graphs;
+	// MT jump tables per parameter set: set-bit lists of t^(J 2^l) mod phi
+	struct MtTable {
+		bool ok = false;
+		std::vector<int32_t*> bits;  // device arrays, one per level
+		std::vector<int> nbits;
+	};
+	std::map<std::vector<uint32_t>, MtTable> mt_tables;
 	// optional per-kernel-class timing with CUDA events on `stream`
 	bool profiling = false;
 	struct Pending {

@@ -8,18 +8,52 @@
 // with x[0..n-1] the seeded state (sgenrand_mt), output word w is
 // temper(x[n+w]).  Every word of a chunk [j0, j0+n-m) depends only on words
 // before j0, so one CTA produces n-m words per barrier step with all
-// arithmetic in 32-bit integers.  The results are bit-identical to the
-// sequential generator.
+// arithmetic in 32-bit integers.
+//
+// Long streams are cut into segments of J = 2^20 words generated by separate
+// CTAs.  The window of nn raw words at the start of segment k is obtained by
+// jumping: with g(t) = t^(J 2^l) mod phi(t) (phi the characteristic
+// polynomial, mt_jump.cc), the window D positions ahead is the XOR of the
+// windows of the raw sequence at the set bits of g.  Segment starts are built
+// as a binary tree: level l turns every known start k*2^(l+1) into
+// k*2^(l+1) + 2^l.  All of it is bit-identical to the sequential generator.
+#include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "internal.h"
 
 namespace armab {
+
+// Defined in mt_jump.cc.
+bool mt_jump_tables(const arma_mt_params& prm, int log2_jump, int levels,
+                    std::vector<std::vector<int32_t>>* set_bits, int* degree);
+
 namespace {
 
 constexpr int kRingBits = 12;
 constexpr int kRing = 1 << kRingBits;  // ring of raw words, >= nn + (nn-mm)
 constexpr int kThreads = 256;
+constexpr int kLog2Seg = 20;           // segment length J = 2^20 words
+constexpr int kLevels = 16;            // jump tables for J * 2^l, l < 16
+
+struct SegJob {
+	arma_mt_params p;
+	uint32_t seed;
+	const uint32_t* state;     // window of nn raw words, or null: seed it
+	unsigned long long first;  // output index of the segment's first word
+	unsigned long long count;  // words in the segment
+	unsigned long long offset; // words before `offset` are not stored
+	uint32_t* out;             // out[w - offset] for output index w
+};
+
+struct JumpJob {
+	arma_mt_params p;
+	const uint32_t* src;  // window at position a
+	uint32_t* dst;        // window at position a + D
+	const int32_t* bits;  // set bits of t^D mod phi
+	int nbits;
+};
 
 __device__ __forceinline__ uint32_t temper(uint32_t y, const arma_mt_params& p) {
 	y ^= y >> p.shift0;
@@ -29,26 +63,29 @@ __device__ __forceinline__ uint32_t temper(uint32_t y, const arma_mt_params& p) 
 	return y;
 }
 
+__device__ __forceinline__ void seed_state(uint32_t* dst, uint32_t seed, const arma_mt_params& p) {
+	// sgenrand_mt: Knuth's 1812433253 initialisation masked by wmask.
+	uint32_t s = seed;
+	for (int k = 0; k < p.nn; ++k) {
+		dst[k] = s & p.wmask;
+		s = 1812433253u * (s ^ (s >> 30)) + uint32_t(k + 1);
+	}
+}
+
 __global__ void __launch_bounds__(kThreads)
-mt_generate_kernel(const MtJob* __restrict__ jobs) {
+mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	__shared__ uint32_t ring[kRing];
-	const arma_mt_params p = jobs[blockIdx.x].p;
-	const uint32_t seed = jobs[blockIdx.x].seed;
-	const unsigned long long offset = jobs[blockIdx.x].offset;
-	const unsigned long long count = jobs[blockIdx.x].count;
-	uint32_t* __restrict__ out = jobs[blockIdx.x].out;
+	const SegJob& jb = jobs[blockIdx.x];
+	const arma_mt_params p = jb.p;
 	const int n = p.nn, m = p.mm;
 	const int chunk = n - m;
-	if (threadIdx.x == 0) {
-		// sgenrand_mt: Knuth's 1812433253 initialisation masked by wmask.
-		uint32_t s = seed;
-		for (int k = 0; k < n; ++k) {
-			ring[k] = s & p.wmask;
-			s = 1812433253u * (s ^ (s >> 30)) + uint32_t(k + 1);
-		}
+	if (jb.state) {
+		for (int k = threadIdx.x; k < n; k += blockDim.x) ring[k] = jb.state[k];
+	} else if (threadIdx.x == 0) {
+		seed_state(ring, jb.seed, p);
 	}
 	__syncthreads();
-	const unsigned long long end = (unsigned long long)n + offset + count;
+	const unsigned long long end = (unsigned long long)n + jb.count;
 	const uint32_t mask = kRing - 1;
 	auto compute = [&](unsigned long long j0) {
 		for (int t = threadIdx.x; t < chunk; t += blockDim.x) {
@@ -67,8 +104,8 @@ mt_generate_kernel(const MtJob* __restrict__ jobs) {
 		for (int t = threadIdx.x; t < chunk; t += blockDim.x) {
 			const unsigned long long j = j0 + t;
 			if (j < end) {
-				const unsigned long long w = j - n;  // output word index
-				if (w >= offset) out[w - offset] = temper(ring[j & mask], p);
+				const unsigned long long w = jb.first + (j - n);  // output index
+				if (w >= jb.offset) jb.out[w - jb.offset] = temper(ring[j & mask], p);
 			}
 		}
 		compute(j0 + chunk);
@@ -77,21 +114,185 @@ mt_generate_kernel(const MtJob* __restrict__ jobs) {
 	}
 }
 
+__global__ void mt_seed_kernel(const arma_mt_params* __restrict__ ps,
+                               const uint32_t* __restrict__ seeds, uint32_t* const* dst) {
+	if (threadIdx.x == 0) seed_state(dst[blockIdx.x], seeds[blockIdx.x], ps[blockIdx.x]);
+}
+
+// One CTA per jump: raw words y[0 .. p+n-2] from the source window in shared
+// memory, then dst[w] = XOR over the set bits i of y[i + w].
+__global__ void __launch_bounds__(1024)
+mt_jump_kernel(const JumpJob* __restrict__ jobs) {
+	extern __shared__ uint32_t y[];
+	const JumpJob& jb = jobs[blockIdx.x];
+	const arma_mt_params p = jb.p;
+	const int n = p.nn, m = p.mm, chunk = n - m;
+	const int deg = 32 * n - p.rr;
+	const int len = deg + n - 1;
+	for (int k = threadIdx.x; k < n; k += blockDim.x) y[k] = jb.src[k];
+	__syncthreads();
+	for (int j0 = n; j0 < len; j0 += chunk) {
+		for (int t = threadIdx.x; t < chunk; t += blockDim.x) {
+			const int j = j0 + t;
+			if (j < len) {
+				const uint32_t v = (y[j - n] & p.umask) | (y[j - n + 1] & p.lmask);
+				y[j] = y[j - n + m] ^ (v >> 1) ^ ((v & 1u) ? p.aaa : 0u);
+			}
+		}
+		__syncthreads();
+	}
+	for (int w = threadIdx.x; w < n; w += blockDim.x) {
+		uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0;
+		int it = 0;
+		const int nb4 = jb.nbits & ~3;
+		for (; it < nb4; it += 4) {
+			const int4 b = *reinterpret_cast<const int4*>(jb.bits + it);
+			r0 ^= y[b.x + w];
+			r1 ^= y[b.y + w];
+			r2 ^= y[b.z + w];
+			r3 ^= y[b.w + w];
+		}
+		for (; it < jb.nbits; ++it) r0 ^= y[jb.bits[it] + w];
+		jb.dst[w] = r0 ^ r1 ^ r2 ^ r3;
+	}
+}
+
+std::vector<uint32_t> params_key(const arma_mt_params& p) {
+	std::vector<uint32_t> k(sizeof(p) / 4);
+	std::memcpy(k.data(), &p, sizeof(p));
+	k.back() = 0;  // the `i` field does not affect the stream
+	return k;
+}
+
+const Ctx::MtTable& jump_table(Ctx* c, const arma_mt_params& p) {
+	auto key = params_key(p);
+	auto it = c->mt_tables.find(key);
+	if (it != c->mt_tables.end()) return it->second;
+	Ctx::MtTable t;
+	std::vector<std::vector<int32_t>> bits;
+	int deg = 0;
+	t.ok = mt_jump_tables(p, kLog2Seg, kLevels, &bits, &deg);
+	if (t.ok) {
+		for (auto& b : bits) {
+			// pad to a multiple of 4 for vector loads (pads are never read)
+			std::vector<int32_t> v = b;
+			while (v.size() % 4) v.push_back(0);
+			int32_t* d = nullptr;
+			ARMA_CUDA_TRY(cudaMalloc(&d, sizeof(int32_t) * std::max<size_t>(v.size(), 4)));
+			ARMA_CUDA_TRY(cudaMemcpy(d, v.data(), sizeof(int32_t) * v.size(), cudaMemcpyHostToDevice));
+			t.bits.push_back(d);
+			t.nbits.push_back(int(b.size()));
+		}
+	}
+	return c->mt_tables.emplace(key, std::move(t)).first->second;
+}
+
 }  // namespace
 
 void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs) {
 	ProfScope prof_(c, "mt");
 	for (const MtJob& j : jobs) {
-		ARMA_REQUIRE(j.p.nn > 1 && j.p.mm > 0 && j.p.mm < j.p.nn, ARMA_EINVAL,
+		ARMA_REQUIRE(j.p.nn > 1 && j.p.mm > 0 && j.p.mm < j.p.nn && j.p.ww == 32, ARMA_EINVAL,
 		             "bad MT parameter set");
 		ARMA_REQUIRE(j.p.nn + (j.p.nn - j.p.mm) <= kRing, ARMA_EINVAL,
 		             "MT state too large for the device generator");
 	}
 	if (jobs.empty()) return;
-	MtJob* d_jobs = static_cast<MtJob*>(scratch_take(c, sizeof(MtJob) * jobs.size()));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(MtJob) * jobs.size(),
+	const unsigned long long J = 1ull << kLog2Seg;
+	// segments per job; jobs with more than one segment need jump tables
+	std::vector<int> K(jobs.size());
+	std::vector<const Ctx::MtTable*> tab(jobs.size(), nullptr);
+	int Kmax = 1;
+	size_t nstates = 0;
+	for (size_t q = 0; q < jobs.size(); ++q) {
+		const unsigned long long total = jobs[q].offset + jobs[q].count;
+		ARMA_REQUIRE((total + J - 1) / J <= (1ull << kLevels), ARMA_EINVAL, "MT stream too long");
+		K[q] = int(std::max(1ull, (total + J - 1) / J));
+		if (K[q] > 1) {
+			tab[q] = &jump_table(c, jobs[q].p);
+			if (!tab[q]->ok) K[q] = 1;  // not a full-period set: one sequential segment
+		}
+		if (K[q] > 1) nstates += size_t(K[q]) * jobs[q].p.nn;
+		Kmax = std::max(Kmax, K[q]);
+	}
+	std::vector<uint32_t*> state0(jobs.size(), nullptr);  // per job: K windows of nn words
+	if (nstates) {
+		uint32_t* states = static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * nstates));
+		size_t off = 0;
+		std::vector<arma_mt_params> ps;
+		std::vector<uint32_t> seeds;
+		std::vector<uint32_t*> dst;
+		for (size_t q = 0; q < jobs.size(); ++q) {
+			if (K[q] <= 1) continue;
+			state0[q] = states + off;
+			off += size_t(K[q]) * jobs[q].p.nn;
+			ps.push_back(jobs[q].p);
+			seeds.push_back(jobs[q].seed);
+			dst.push_back(state0[q]);
+		}
+		auto* d_ps = static_cast<arma_mt_params*>(scratch_take(c, sizeof(arma_mt_params) * ps.size()));
+		auto* d_seeds = static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * seeds.size()));
+		auto* d_dst = static_cast<uint32_t**>(scratch_take(c, sizeof(uint32_t*) * dst.size()));
+		ARMA_CUDA_TRY(cudaMemcpyAsync(d_ps, ps.data(), sizeof(arma_mt_params) * ps.size(),
+		                              cudaMemcpyHostToDevice, c->stream));
+		ARMA_CUDA_TRY(cudaMemcpyAsync(d_seeds, seeds.data(), sizeof(uint32_t) * seeds.size(),
+		                              cudaMemcpyHostToDevice, c->stream));
+		ARMA_CUDA_TRY(cudaMemcpyAsync(d_dst, dst.data(), sizeof(uint32_t*) * dst.size(),
+		                              cudaMemcpyHostToDevice, c->stream));
+		mt_seed_kernel<<<int(ps.size()), 32, 0, c->stream>>>(d_ps, d_seeds, d_dst);
+		c->launches += 1;
+		// binary tree of jumps, widest stride first
+		int levels = 0;
+		while ((1 << levels) < Kmax) ++levels;
+		size_t smem = 0;
+		for (size_t q = 0; q < jobs.size(); ++q)
+			if (K[q] > 1)
+				smem = std::max(smem, sizeof(uint32_t) * size_t(32 * jobs[q].p.nn - jobs[q].p.rr +
+				                                                jobs[q].p.nn));
+		ARMA_CUDA_TRY(cudaFuncSetAttribute(mt_jump_kernel,
+		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		for (int lv = levels - 1; lv >= 0; --lv) {
+			std::vector<JumpJob> jj;
+			const int step = 1 << lv;
+			for (size_t q = 0; q < jobs.size(); ++q) {
+				if (K[q] <= 1) continue;
+				const int nn = jobs[q].p.nn;
+				for (int base = 0; base + step < K[q]; base += 2 * step)
+					jj.push_back(JumpJob{jobs[q].p, state0[q] + size_t(base) * nn,
+					                     state0[q] + size_t(base + step) * nn, tab[q]->bits[lv],
+					                     tab[q]->nbits[lv]});
+			}
+			if (jj.empty()) continue;
+			auto* d_jj = static_cast<JumpJob*>(scratch_take(c, sizeof(JumpJob) * jj.size()));
+			ARMA_CUDA_TRY(cudaMemcpyAsync(d_jj, jj.data(), sizeof(JumpJob) * jj.size(),
+			                              cudaMemcpyHostToDevice, c->stream));
+			mt_jump_kernel<<<int(jj.size()), 640, smem, c->stream>>>(d_jj);
+			ARMA_CUDA_TRY(cudaGetLastError());
+			c->launches += 1;
+		}
+	}
+	// generation: one CTA per segment
+	std::vector<SegJob> seg;
+	for (size_t q = 0; q < jobs.size(); ++q) {
+		const unsigned long long total = jobs[q].offset + jobs[q].count;
+		for (int k = 0; k < K[q]; ++k) {
+			const unsigned long long first = (unsigned long long)k * J;
+			if (K[q] > 1 && first + J <= jobs[q].offset) continue;  // entirely skipped
+			SegJob s;
+			s.p = jobs[q].p;
+			s.seed = jobs[q].seed;
+			s.state = K[q] > 1 ? state0[q] + size_t(k) * jobs[q].p.nn : nullptr;
+			s.first = first;
+			s.count = K[q] > 1 ? std::min(J, total - first) : total;
+			s.offset = jobs[q].offset;
+			s.out = jobs[q].out;
+			seg.push_back(s);
+		}
+	}
+	auto* d_seg = static_cast<SegJob*>(scratch_take(c, sizeof(SegJob) * seg.size()));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d_seg, seg.data(), sizeof(SegJob) * seg.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
-	mt_generate_kernel<<<int(jobs.size()), kThreads, 0, c->stream>>>(d_jobs);
+	mt_generate_kernel<<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg);
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 }
@@ -100,7 +301,7 @@ void launch_mt_generate(Ctx* c, const arma_mt_params& p, uint32_t seed,
                         uint64_t offset, uint64_t n, uint32_t* d_out) {
 	if (n == 0) return;
 	launch_mt_generate_batch(c, {MtJob{p, seed, offset, n, d_out}});
-	// the job table lives in scratch: keep it alive until the kernel has read it
+	// the job tables live in scratch and pageable host vectors: finish first
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 }
 
