@@ -75,13 +75,18 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 	asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Wait until *flag >= need.  Gives up after kSpinLimit polls (or when another
-// CTA already gave up) and reports DEV_TIMEOUT; returns false then.
-__device__ bool wait_flag(const int* flag, int need, int* err) {
+// Wait until every non-null flag is >= need; the three acquire loads of a
+// poll are issued together so one L2 round trip covers them.  Gives up after
+// kSpinLimit polls (or when another CTA already gave up) and reports
+// DEV_TIMEOUT; returns false then.
+__device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need, int* err) {
 	for (long long it = 0; it < kSpinLimit; ++it) {
-		if (ld_acquire(flag) >= need) return true;
+		const int a = f0 ? ld_acquire(f0) : need;
+		const int b = f1 ? ld_acquire(f1) : need;
+		const int c = f2 ? ld_acquire(f2) : need;
+		if (a >= need && b >= need && c >= need) return true;
 		if ((it & 63) == 63 && *((volatile int*)err) != DEV_OK) return false;
-		__nanosleep(128);
+		__nanosleep(64);
 	}
 	atomicExch(err, DEV_TIMEOUT);
 	return false;
@@ -201,13 +206,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 
 		// 2. neighbours' slice t
 		__shared__ int s_ok;
-		if (tid == 0) {
-			bool ok = true;
-			if (fW) ok = ok && wait_flag(fW, t + 1, err);
-			if (ok && fN) ok = ok && wait_flag(fN, t + 1, err);
-			if (ok && fNW) ok = ok && wait_flag(fNW, t + 1, err);
-			s_ok = ok ? 1 : 0;
-		}
+		if (tid == 0) s_ok = wait_flags(fW, fN, fNW, t + 1, err) ? 1 : 0;
 		__syncthreads();
 		if (!s_ok) return;
 

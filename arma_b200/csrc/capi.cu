@@ -103,11 +103,12 @@ void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
 	}
 	long long* d_pairs = static_cast<long long*>(scratch_take(c, sizeof(long long) * n));
 	launch_mt_generate_batch(c, jobs);
+	std::vector<NoiseSpec> specs(n);
 	for (int k = 0; k < n; ++k) {
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
-		enqueue_white_noise(c, jobs[k].out, 4 * att[k], std::sqrt(s[k].var_wn), np, precision,
-		                    dz[k], d_pairs + k);
+		specs[k] = NoiseSpec{jobs[k].out, 4 * att[k], np, std::sqrt(s[k].var_wn), dz[k]};
 	}
+	enqueue_white_noise_batch(c, specs, precision, d_pairs);
 	std::vector<long long> pairs(n);
 	ARMA_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(long long) * n,
 	                              cudaMemcpyDeviceToHost, c->stream));
@@ -464,42 +465,54 @@ int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed, doub
 namespace {
 
 // Device copies of the hi/lo float split of phi and of the intra-slice
-// response H for the FP32 tile kernel.
-Ar32Surface ar32_surface(Ctx* c, const double* phi, const int order[3], const int shape[3],
-                         float* d_zeta) {
+// response H for the FP32 tile kernel, for n surfaces in one upload.
+std::vector<Ar32Surface> ar32_surfaces(Ctx* c, int n, const double* const* phis,
+                                       const int* const* orders, const int* const* shapes,
+                                       float* const* zetas) {
 	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
-	const int P = order[0] * order[1] * order[2];
-	std::vector<double> h(size_t(tx) * ty);
-	intra_slice_response(phi, order, tx, ty, h.data());
-	const size_t nh = h.size();
-	std::vector<float> buf(2 * P + 2 * nh);
-	for (int i = 0; i < P; ++i) {
-		buf[i] = float(phi[i]);
-		buf[P + i] = float(phi[i] - double(buf[i]));
-	}
-	for (size_t i = 0; i < nh; ++i) {
-		buf[2 * P + i] = float(h[i]);
-		buf[2 * P + nh + i] = float(h[i] - double(buf[2 * P + i]));
+	const size_t nh = size_t(tx) * ty;
+	std::vector<size_t> off(n + 1, 0);
+	for (int k = 0; k < n; ++k)
+		off[k + 1] = off[k] + 2 * size_t(orders[k][0]) * orders[k][1] * orders[k][2] + 2 * nh;
+	std::vector<float> buf(off[n]);
+	std::vector<double> h(nh);
+	for (int k = 0; k < n; ++k) {
+		const int P = orders[k][0] * orders[k][1] * orders[k][2];
+		float* b = buf.data() + off[k];
+		intra_slice_response(phis[k], orders[k], tx, ty, h.data());
+		for (int i = 0; i < P; ++i) {
+			b[i] = float(phis[k][i]);
+			b[P + i] = float(phis[k][i] - double(b[i]));
+		}
+		for (size_t i = 0; i < nh; ++i) {
+			b[2 * P + i] = float(h[i]);
+			b[2 * P + nh + i] = float(h[i] - double(b[2 * P + i]));
+		}
 	}
 	float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice,
 	                              c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));  // buf is pageable and local
-	Ar32Surface s;
-	s.nt = shape[0];
-	s.nx = shape[1];
-	s.ny = shape[2];
-	s.pt = order[0];
-	s.px = order[1];
-	s.py = order[2];
-	s.zeta = d_zeta;
-	s.phi = d;
-	s.phi_lo = d + P;
-	s.h = d + 2 * P;
-	s.h_lo = d + 2 * P + nh;
-	s.tiles_x = (s.nx + tx - 1) / tx;
-	s.tiles_y = (s.ny + ty - 1) / ty;
-	return s;
+	std::vector<Ar32Surface> out(n);
+	for (int k = 0; k < n; ++k) {
+		const int P = orders[k][0] * orders[k][1] * orders[k][2];
+		float* dk = d + off[k];
+		Ar32Surface& s = out[k];
+		s.nt = shapes[k][0];
+		s.nx = shapes[k][1];
+		s.ny = shapes[k][2];
+		s.pt = orders[k][0];
+		s.px = orders[k][1];
+		s.py = orders[k][2];
+		s.zeta = zetas[k];
+		s.phi = dk;
+		s.phi_lo = dk + P;
+		s.h = dk + 2 * P;
+		s.h_lo = dk + 2 * P + nh;
+		s.tiles_x = (s.nx + tx - 1) / tx;
+		s.tiles_y = (s.ny + ty - 1) / ty;
+	}
+	return out;
 }
 
 void ar_filter(Ctx* c, const double* phi, const int order[3], const int shape[3],
@@ -512,8 +525,9 @@ void ar_filter(Ctx* c, const double* phi, const int order[3], const int shape[3]
 		launch_ar64(c, d_phi, order, shape, static_cast<double*>(d_zeta));
 	} else {
 		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
-		Ar32Surface s = ar32_surface(c, phi, order, shape, static_cast<float*>(d_zeta));
-		launch_ar32c(c, {s}, tx, ty, 1);
+		float* z = static_cast<float*>(d_zeta);
+		std::vector<Ar32Surface> s = ar32_surfaces(c, 1, &phi, &order, &shape, &z);
+		launch_ar32c(c, s, tx, ty, 1);
 		check_device_error(c);
 	}
 }
@@ -632,16 +646,28 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 		for (int k = 0; k < n; ++k) ar_filter(c, s[k].phi, s[k].order, s[k].shape, precision, dz[k]);
 	} else {
 		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
-		std::vector<Ar32Surface> as(n);
-		for (int k = 0; k < n; ++k)
-			as[k] = ar32_surface(c, s[k].phi, s[k].order, s[k].shape, static_cast<float*>(dz[k]));
+		std::vector<const double*> phis(n);
+		std::vector<const int*> ords(n), shps(n);
+		std::vector<float*> zs(n);
+		for (int k = 0; k < n; ++k) {
+			phis[k] = s[k].phi;
+			ords[k] = s[k].order;
+			shps[k] = s[k].shape;
+			zs[k] = static_cast<float*>(dz[k]);
+		}
+		std::vector<Ar32Surface> as =
+		    ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
 		launch_ar32c(c, as, tx, ty, 1);
 		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 		check_device_error(c);
 	}
 	double* d_scale = static_cast<double*>(scratch_take(c, sizeof(double) * n));
+	std::vector<RenormSpec> rs;
 	for (int k = 0; k < n; ++k)
-		if (s[k].acf0 > 0.0) launch_renorm(c, dz[k], s[k].shape, precision, s[k].acf0, d_scale + k);
+		if (s[k].acf0 > 0.0)
+			rs.push_back(RenormSpec{dz[k], {s[k].shape[0], s[k].shape[1], s[k].shape[2]}, s[k].acf0,
+			                        d_scale + k});
+	launch_renorm_batch(c, rs, precision);
 	if (host) {
 		for (int k = 0; k < n; ++k) {
 			const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
@@ -650,13 +676,10 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 		}
 	}
 	std::vector<double> sc(n, 1.0);
+	ARMA_CUDA_TRY(cudaMemcpyAsync(sc.data(), d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost,
+	                              c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
-	for (int k = 0; k < n; ++k) {
-		if (s[k].acf0 > 0.0) {
-			ARMA_CUDA_TRY(cudaMemcpy(&sc[k], d_scale + k, sizeof(double), cudaMemcpyDeviceToHost));
-		}
-		s[k].scale = sc[k];
-	}
+	for (int k = 0; k < n; ++k) s[k].scale = s[k].acf0 > 0.0 ? sc[k] : 1.0;
 }
 
 }  // namespace

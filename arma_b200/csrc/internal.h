@@ -112,6 +112,17 @@ void enqueue_white_noise(Ctx* c, const uint32_t* d_words, uint64_t n_words,
                          long long* d_pairs);
 bool launch_white_noise(Ctx* c, const uint32_t* d_words, uint64_t n_words,
                         double stddev, uint64_t n, int precision, void* d_out);
+// All surfaces of a batch in three launches; d_pairs[k] receives surface k's
+// number of accepted pairs (no synchronisation).
+struct NoiseSpec {
+	const uint32_t* words;
+	uint64_t n_words;
+	uint64_t n;
+	double stddev;
+	void* out;
+};
+void enqueue_white_noise_batch(Ctx* c, const std::vector<NoiseSpec>& specs, int precision,
+                               long long* d_pairs);
 
 // FP64 exact-order AR filter.
 void launch_ar64(Ctx* c, const double* d_phi, const int order[3],
@@ -136,6 +147,13 @@ int ar32c_tile_y();
 // Variance renormalisation: computes scale on device (d_scale) and applies it.
 void launch_renorm(Ctx* c, void* d_zeta, const int shape[3], int precision,
                    double acf0, double* d_scale);
+struct RenormSpec {
+	void* z;
+	int shape[3];
+	double acf0;
+	double* d_scale;
+};
+void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int precision);
 
 // NIT.
 void launch_nit_bisection(Ctx* c, int dist, const double params[3], double stdev,

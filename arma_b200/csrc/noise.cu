@@ -179,3 +179,137 @@ bool launch_white_noise(Ctx* c, const uint32_t* d_words, uint64_t n_words,
 }
 
 }  // namespace armab
+
+// ---------------------------------------------------------------------------
+// Batched form: every surface's polar transform in three launches.  Global
+// block g belongs to the surface whose [block_base, next block_base) range
+// holds it (binary search over the surface table).
+namespace armab {
+namespace {
+
+struct NoiseJob {
+	const uint4* words;
+	unsigned long long n_attempts;
+	unsigned long long n;
+	double stddev;
+	void* out;
+	int block_base;
+	int nblocks;
+};
+
+__device__ __forceinline__ int find_job(const NoiseJob* jobs, int njobs, int g) {
+	int lo = 0, hi = njobs - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) / 2;
+		if (jobs[mid].block_base <= g) lo = mid; else hi = mid - 1;
+	}
+	return lo;
+}
+
+__global__ void __launch_bounds__(kThreads)
+noise_count_batch_kernel(const NoiseJob* __restrict__ jobs, int njobs, int* __restrict__ counts) {
+	const NoiseJob& jb = jobs[find_job(jobs, njobs, blockIdx.x)];
+	const unsigned long long lb = blockIdx.x - jb.block_base;
+	const unsigned long long a0 = lb * kPerBlock + (unsigned long long)threadIdx.x * kPerThread;
+	int cnt = 0;
+#pragma unroll
+	for (int k = 0; k < kPerThread; ++k) {
+		const unsigned long long a = a0 + k;
+		if (a < jb.n_attempts) cnt += attempt(jb.words[a]).ok ? 1 : 0;
+	}
+	int total;
+	block_exclusive_scan(cnt, &total);
+	if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kThreads)
+scan_counts_batch_kernel(const NoiseJob* __restrict__ jobs, const int* __restrict__ counts,
+                         long long* __restrict__ offsets, long long* __restrict__ pairs) {
+	const NoiseJob& jb = jobs[blockIdx.x];
+	__shared__ long long carry;
+	if (threadIdx.x == 0) carry = 0;
+	__syncthreads();
+	for (int base = 0; base < jb.nblocks; base += kThreads) {
+		const int i = base + threadIdx.x;
+		const int v = i < jb.nblocks ? counts[jb.block_base + i] : 0;
+		int tot;
+		const int ex = block_exclusive_scan(v, &tot);
+		if (i < jb.nblocks) offsets[jb.block_base + i] = carry + ex;
+		__syncthreads();
+		if (threadIdx.x == 0) carry += tot;
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) pairs[blockIdx.x] = carry;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+noise_scatter_batch_kernel(const NoiseJob* __restrict__ jobs, int njobs,
+                           const long long* __restrict__ offsets) {
+	const NoiseJob& jb = jobs[find_job(jobs, njobs, blockIdx.x)];
+	const unsigned long long lb = blockIdx.x - jb.block_base;
+	const unsigned long long a0 = lb * kPerBlock + (unsigned long long)threadIdx.x * kPerThread;
+	T* out = static_cast<T*>(jb.out);
+	Attempt at[kPerThread];
+	int cnt = 0;
+#pragma unroll
+	for (int k = 0; k < kPerThread; ++k) {
+		const unsigned long long a = a0 + k;
+		if (a < jb.n_attempts) {
+			at[k] = attempt(jb.words[a]);
+		} else {
+			at[k].ok = false;
+		}
+		cnt += at[k].ok ? 1 : 0;
+	}
+	int total;
+	long long rank = offsets[blockIdx.x] + block_exclusive_scan(cnt, &total);
+#pragma unroll
+	for (int k = 0; k < kPerThread; ++k) {
+		if (!at[k].ok) continue;
+		const unsigned long long i0 = 2ull * (unsigned long long)rank;
+		if (i0 < jb.n) {
+			const double m = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, log(at[k].r2)), at[k].r2));
+			out[i0] = T(__dadd_rn(__dmul_rn(__dmul_rn(at[k].y, m), jb.stddev), 0.0));
+			if (i0 + 1 < jb.n)
+				out[i0 + 1] = T(__dadd_rn(__dmul_rn(__dmul_rn(at[k].x, m), jb.stddev), 0.0));
+		}
+		++rank;
+	}
+}
+
+}  // namespace
+
+void enqueue_white_noise_batch(Ctx* c, const std::vector<NoiseSpec>& specs, int precision,
+                               long long* d_pairs) {
+	ProfScope prof_(c, "noise");
+	std::vector<NoiseJob> jobs(specs.size());
+	long long total_blocks = 0;
+	for (size_t k = 0; k < specs.size(); ++k) {
+		const uint64_t na = specs[k].n_words / 4;
+		const long long nb = (long long)std::max<uint64_t>(1, (na + kPerBlock - 1) / kPerBlock);
+		jobs[k] = NoiseJob{reinterpret_cast<const uint4*>(specs[k].words), na, specs[k].n,
+		                   specs[k].stddev, specs[k].out, int(total_blocks), int(nb)};
+		total_blocks += nb;
+	}
+	ARMA_REQUIRE(total_blocks < (1ll << 31), ARMA_EINVAL, "white noise batch too large");
+	if (jobs.empty()) return;
+	auto* d_jobs = static_cast<NoiseJob*>(scratch_take(c, sizeof(NoiseJob) * jobs.size()));
+	int* counts = static_cast<int*>(scratch_take(c, sizeof(int) * total_blocks));
+	long long* offsets = static_cast<long long*>(scratch_take(c, sizeof(long long) * total_blocks));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(NoiseJob) * jobs.size(),
+	                              cudaMemcpyHostToDevice, c->stream));
+	const int nj = int(jobs.size());
+	noise_count_batch_kernel<<<int(total_blocks), kThreads, 0, c->stream>>>(d_jobs, nj, counts);
+	scan_counts_batch_kernel<<<nj, kThreads, 0, c->stream>>>(d_jobs, counts, offsets, d_pairs);
+	if (precision == ARMA_FP64)
+		noise_scatter_batch_kernel<double><<<int(total_blocks), kThreads, 0, c->stream>>>(
+		    d_jobs, nj, offsets);
+	else
+		noise_scatter_batch_kernel<float><<<int(total_blocks), kThreads, 0, c->stream>>>(
+		    d_jobs, nj, offsets);
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 3;
+}
+
+}  // namespace armab

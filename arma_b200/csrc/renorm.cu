@@ -101,3 +101,113 @@ void launch_renorm(Ctx* c, void* d_zeta, const int shape[3], int precision,
 }
 
 }  // namespace armab
+
+// ---------------------------------------------------------------------------
+// Batched form: the renormalisation of many surfaces in five launches.
+namespace armab {
+namespace {
+
+constexpr int kBatchBlocks = 32;  // partial sums per surface
+
+struct RenormJob {
+	void* z;
+	unsigned long long off, cnt, n;
+	double acf0;
+	double* scale;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+partial_batch_kernel(const RenormJob* __restrict__ jobs, const double* __restrict__ means,
+                     double* __restrict__ partial) {
+	__shared__ double sh[kThreads / 32];
+	const int s = blockIdx.x / kBatchBlocks, b = blockIdx.x % kBatchBlocks;
+	const RenormJob& jb = jobs[s];
+	const T* x = static_cast<const T*>(jb.z) + jb.off;
+	const double m = means ? means[s] : 0.0;
+	double acc = 0.0;
+	for (unsigned long long i = (unsigned long long)b * kThreads + threadIdx.x; i < jb.cnt;
+	     i += (unsigned long long)kBatchBlocks * kThreads) {
+		const double v = double(x[i]);
+		if (means) {
+			const double d = v - m;
+			acc = fma(d, d, acc);
+		} else {
+			acc += v;
+		}
+	}
+	for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+	if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < kThreads / 32; ++w) t += sh[w];
+		partial[blockIdx.x] = t;
+	}
+}
+
+__global__ void finish_batch_kernel(const RenormJob* __restrict__ jobs,
+                                    const double* __restrict__ partial, int mode,
+                                    double* __restrict__ means) {
+	const RenormJob& jb = jobs[blockIdx.x];
+	if (threadIdx.x != 0) return;
+	double t = 0.0;
+	for (int i = 0; i < kBatchBlocks; ++i) t += partial[blockIdx.x * kBatchBlocks + i];
+	if (mode == 0) means[blockIdx.x] = t / double(jb.cnt);
+	else *jb.scale = sqrt(jb.acf0 / (t / double(jb.cnt - 1)));
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+scale_batch_kernel(const RenormJob* __restrict__ jobs, int blocks_per_job) {
+	const int s = blockIdx.x / blocks_per_job, b = blockIdx.x % blocks_per_job;
+	const RenormJob& jb = jobs[s];
+	T* x = static_cast<T*>(jb.z);
+	const double sc = *jb.scale;
+	for (unsigned long long i = (unsigned long long)b * kThreads + threadIdx.x; i < jb.n;
+	     i += (unsigned long long)blocks_per_job * kThreads)
+		x[i] = T(double(x[i]) * sc);
+}
+
+}  // namespace
+
+void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int precision) {
+	ProfScope prof_(c, "renorm");
+	if (specs.empty()) return;
+	std::vector<RenormJob> jobs(specs.size());
+	for (size_t k = 0; k < specs.size(); ++k) {
+		const long long nt = specs[k].shape[0], nx = specs[k].shape[1], ny = specs[k].shape[2];
+		RenormJob& j = jobs[k];
+		j.z = specs[k].z;
+		j.off = (unsigned long long)((nt / 2) * nx + nx / 2) * ny + ny / 2;
+		j.cnt = (unsigned long long)(nt - nt / 2) * (nx - nx / 2) * (ny - ny / 2);
+		j.n = (unsigned long long)nt * nx * ny;
+		j.acf0 = specs[k].acf0;
+		j.scale = specs[k].d_scale;
+		ARMA_REQUIRE(j.cnt >= 2, ARMA_EINVAL, "surface too small for variance renormalisation");
+	}
+	const int ns = int(jobs.size());
+	auto* d_jobs = static_cast<RenormJob*>(scratch_take(c, sizeof(RenormJob) * jobs.size()));
+	double* partial = static_cast<double*>(scratch_take(c, sizeof(double) * ns * kBatchBlocks));
+	double* means = static_cast<double*>(scratch_take(c, sizeof(double) * ns));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(RenormJob) * jobs.size(),
+	                              cudaMemcpyHostToDevice, c->stream));
+	const int g = ns * kBatchBlocks;
+	if (precision == ARMA_FP64) {
+		partial_batch_kernel<double><<<g, kThreads, 0, c->stream>>>(d_jobs, nullptr, partial);
+		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 0, means);
+		partial_batch_kernel<double><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
+		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
+		scale_batch_kernel<double><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
+	} else {
+		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, nullptr, partial);
+		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 0, means);
+		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
+		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
+		scale_batch_kernel<float><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
+	}
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 5;
+}
+
+}  // namespace armab
