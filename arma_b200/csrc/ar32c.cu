@@ -65,6 +65,15 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
 	s = t;
 }
 
+__device__ __forceinline__ void cp_async16(float* dst_smem, const float* src) {
+	const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst_smem));
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+	asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ int ld_acquire(const int* p) {
 	int v;
 	asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -92,6 +101,64 @@ __device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need
 	return false;
 }
 
+// zeta = H * S over the quarter plane of one tile for the output strip
+// (xl, yl0 .. yl0+R-1), dx restricted to [dx_lo, min(dx_hi, xl+1)): writes the
+// Kahan-compensated partial strip to out[0..R).  Shared by every tap-count
+// instantiation of run_tile, so its code exists once.
+__device__ __noinline__ void h_phase(const float* ss, const float* sh, const float* shl, int xl,
+                                     int yl0, int dx_lo, int dx_hi, float* out) {
+	float a[R], ac[R];
+#pragma unroll
+	for (int r = 0; r < R; ++r) { a[r] = 0.0f; ac[r] = 0.0f; }
+	const int dx_end = min(dx_hi - 1, xl);
+	for (int dx = dx_lo; dx <= dx_end; ++dx) {
+		const float* srow = ss + (xl - dx) * SW + SPAD;
+		const float* hrow = sh + dx * TY;
+		const float* hlrow = shl + dx * TY;
+		for (int dy0 = 0; dy0 <= yl0; dy0 += R) {
+			// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
+			float w[2 * R];
+			const float4* sp = reinterpret_cast<const float4*>(srow + yl0 - dy0 - R);
+#pragma unroll
+			for (int q = 0; q < 2 * R / 4; ++q) {
+				const float4 v = sp[q];
+				w[4 * q] = v.x;
+				w[4 * q + 1] = v.y;
+				w[4 * q + 2] = v.z;
+				w[4 * q + 3] = v.w;
+			}
+			float hv[R], hl[R];
+			const float4* hp = reinterpret_cast<const float4*>(hrow + dy0);
+			const float4* hq = reinterpret_cast<const float4*>(hlrow + dy0);
+#pragma unroll
+			for (int q = 0; q < R / 4; ++q) {
+				const float4 v = hp[q];
+				hv[4 * q] = v.x;
+				hv[4 * q + 1] = v.y;
+				hv[4 * q + 2] = v.z;
+				hv[4 * q + 3] = v.w;
+				const float4 u = hq[q];
+				hl[4 * q] = u.x;
+				hl[4 * q + 1] = u.y;
+				hl[4 * q + 2] = u.z;
+				hl[4 * q + 3] = u.w;
+			}
+#pragma unroll
+			for (int r = 0; r < R; ++r) {
+				float p = 0.0f, q = 0.0f;
+#pragma unroll
+				for (int dd = 0; dd < R; ++dd) {
+					p = fmaf(hv[dd], w[R + r - dd], p);
+					q = fmaf(hl[dd], w[R + r - dd], q);
+				}
+				kahan_add(a[r], ac[r], p + q);
+			}
+		}
+	}
+#pragma unroll
+	for (int r = 0; r < R; ++r) out[r] = a[r] - ac[r];
+}
+
 template <int PY>
 __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) {
 	const int tid = threadIdx.x;
@@ -114,6 +181,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 	float* shl = sh + TX * TY;                   // TX*TY (lo)
 	float* ss = shl + TX * TY;                   // TX*SW
 	float* comb = ss + TX * SW;                  // GROUP*R: group 1 partials
+	float* hres = comb + GROUP * R;              // NTHREADS*R: H-phase partials
 
 	// stage coefficients (rows padded with zeros), H, zero the ring and S pads
 	for (int q = tid; q < pt * px * PYP; q += NTHREADS) {
@@ -130,6 +198,9 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 	__syncthreads();
 
 	const int gx = x0 + xl;
+	// 16-byte halo chunks need 16-byte aligned rows in global memory
+	const bool vec_ok = (tk.ny % 4 == 0) && ((reinterpret_cast<uintptr_t>(tk.zeta) & 15) == 0) &&
+	                    ((sst % 4) == 0);
 	const int* fW = (bx > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by : nullptr;
 	const int* fN = (by > 0) ? tk.flags + bx * tk.tiles_y + by - 1 : nullptr;
 	const int* fNW = (bx > 0 && by > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by - 1 : nullptr;
@@ -211,13 +282,32 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		if (!s_ok) return;
 
 		// 3. halo of slice t: rows above the tile (all columns) and the left
-		//    columns of the tile rows
-		for (int q = tid; q < rows * W; q += NTHREADS) {
-			const int rr = q / W, cc = q % W;
-			if (rr >= hx && cc >= LH) continue;  // in-tile: stays zero
-			const int x = x0 - hx + rr, y = y0 - LH + cc;
-			if (x < 0 || y < 0 || x >= tk.nx || y >= tk.ny) continue;
-			cur[q] = __ldcg(zt + (long long)x * tk.ny + y);
+		//    columns of the tile rows, in 16-byte chunks copied with
+		//    L2-only asynchronous copies (scalar loads at ragged edges)
+		{
+			const int top = hx * (W / 4);
+			const int nch = top + TX * (LH / 4);
+			for (int q = tid; q < nch; q += NTHREADS) {
+				int rr, c4;
+				if (q < top) {
+					rr = q / (W / 4);
+					c4 = q % (W / 4);
+				} else {
+					rr = hx + (q - top) / (LH / 4);
+					c4 = (q - top) % (LH / 4);
+				}
+				const int x = x0 - hx + rr, y = y0 - LH + 4 * c4;
+				if (x < 0 || x >= tk.nx) continue;  // stays zero
+				float* dst = cur + rr * W + 4 * c4;
+				const float* src = zt + (long long)x * tk.ny + y;
+				if (vec_ok && y >= 0 && y + 4 <= tk.ny) {
+					cp_async16(dst, src);
+				} else {
+					for (int e = 0; e < 4; ++e)
+						if (y + e >= 0 && y + e < tk.ny) dst[e] = __ldcg(src + e);
+				}
+			}
+			cp_async_wait_all();
 		}
 		__syncthreads();
 		accumulate_rows(cur, 0);
@@ -239,66 +329,15 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		__syncthreads();
 
 		//    zeta = H * S over the quarter plane of the tile
-		float a[R], ac[R];
-#pragma unroll
-		for (int r = 0; r < R; ++r) { a[r] = 0.0f; ac[r] = 0.0f; }
-		const int dx_end = min(dx_hi - 1, xl);
-		for (int dx = dx_lo; dx <= dx_end; ++dx) {
-			const float* srow = ss + (xl - dx) * SW + SPAD;
-			const float* hrow = sh + dx * TY;
-			const float* hlrow = shl + dx * TY;
-			for (int dy0 = 0; dy0 <= yl0; dy0 += R) {
-				// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
-				float w[2 * R];
-				const float4* sp = reinterpret_cast<const float4*>(srow + yl0 - dy0 - R);
-#pragma unroll
-				for (int q = 0; q < 2 * R / 4; ++q) {
-					const float4 v = sp[q];
-					w[4 * q] = v.x;
-					w[4 * q + 1] = v.y;
-					w[4 * q + 2] = v.z;
-					w[4 * q + 3] = v.w;
-				}
-				float hv[R], hl[R];
-				const float4* hp = reinterpret_cast<const float4*>(hrow + dy0);
-				const float4* hq = reinterpret_cast<const float4*>(hlrow + dy0);
-#pragma unroll
-				for (int q = 0; q < R / 4; ++q) {
-					const float4 v = hp[q];
-					hv[4 * q] = v.x;
-					hv[4 * q + 1] = v.y;
-					hv[4 * q + 2] = v.z;
-					hv[4 * q + 3] = v.w;
-					const float4 u = hq[q];
-					hl[4 * q] = u.x;
-					hl[4 * q + 1] = u.y;
-					hl[4 * q + 2] = u.z;
-					hl[4 * q + 3] = u.w;
-				}
-#pragma unroll
-				for (int r = 0; r < R; ++r) {
-					float p = 0.0f, q = 0.0f;
-#pragma unroll
-					for (int dd = 0; dd < R; ++dd) {
-						p = fmaf(hv[dd], w[R + r - dd], p);
-						q = fmaf(hl[dd], w[R + r - dd], q);
-					}
-					kahan_add(a[r], ac[r], p + q);
-				}
-			}
-		}
+		h_phase(ss, sh, shl, xl, yl0, dx_lo, dx_hi, hres + tid * R);
 
 		// 5. store the solved slice and publish it
-		if (grp == 1) {
-#pragma unroll
-			for (int r = 0; r < R; ++r) comb[lt * R + r] = a[r] - ac[r];
-		}
 		__syncthreads();
 		if (grp == 0) {
 			float* own = cur + hx * W + LH;
 #pragma unroll
 			for (int r = 0; r < R; ++r) {
-				const float v = a[r] + (comb[lt * R + r] - ac[r]);
+				const float v = hres[tid * R + r] + hres[(tid + GROUP) * R + r];
 				own[xl * W + yl0 + r] = v;
 				const int gy = y0 + yl0 + r;
 				if (gx < tk.nx && gy < tk.ny) zt[(long long)gx * tk.ny + gy] = v;
@@ -351,7 +390,7 @@ size_t smem_bytes(int pt, int px, int py) {
 	const int rows = TX + px - 1;
 	const int pyp = (py + 3) & ~3;
 	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + 2 * TX * TY + TX * SW +
-	                        GROUP * R);
+	                        GROUP * R + NTHREADS * R);
 }
 
 }  // namespace
