@@ -223,7 +223,7 @@ def gpu_arm(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    batch = fit_batch(make_batch(rank))
+    batch = fit_batch(make_batch(rank)[:args.surfaces])
     sets = mt_sets()
     ctx = A.Context(local)
     stream = torch.cuda.current_stream()
@@ -273,21 +273,25 @@ def gpu_arm(args):
     value = world * npts * args.steps / elapsed
 
     # ---- e2e: same call into pinned host buffers
-    host = [torch.empty(s["shape"], dtype=torch.float32, pin_memory=True) for s in batch]
-    surfh = [capi.make_surface(s["shape"], s["phi"], s["var"], s["acf0"],
-                               sets[s["mtset"] % len(sets)], s["seed"], h.data_ptr())
-             for s, h in zip(batch, host)]
-    ctx.batch_generate(surfh, A.FP32C, host=True)
-    barrier()
-    t0 = time.perf_counter()
-    e2e_steps = max(1, min(args.steps, 3))
-    for _ in range(e2e_steps):
+    e2e = None
+    if args.skip_e2e:
+        host = []
+    else:
+        host = [torch.empty(s["shape"], dtype=torch.float32, pin_memory=True) for s in batch]
+        surfh = [capi.make_surface(s["shape"], s["phi"], s["var"], s["acf0"],
+                                   sets[s["mtset"] % len(sets)], s["seed"], h.data_ptr())
+                 for s, h in zip(batch, host)]
         ctx.batch_generate(surfh, A.FP32C, host=True)
-    barrier()
-    e2e_t = max_over_ranks(time.perf_counter() - t0)
-    e2e = world * npts * e2e_steps / e2e_t
-    # parity spot check of the host copy against the device result
-    assert torch.equal(host[0], bufs32[0].cpu())
+        barrier()
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for _ in range(e2e_steps):
+            ctx.batch_generate(surfh, A.FP32C, host=True)
+        barrier()
+        e2e_t = max_over_ranks(time.perf_counter() - t0)
+        e2e = world * npts * e2e_steps / e2e_t
+        # parity spot check of the host copy against the device result
+        assert torch.equal(host[0], bufs32[0].cpu())
     del bufs32
 
     # ---- plain FP64 path on the same batch (surface after surface)
@@ -316,6 +320,13 @@ def gpu_arm(args):
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s at the max SM clock
     per_launch_flops = flops(batch)  # one ar32c pass over the batch per step
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ar32c_dram_traffic.json")) as f:
+            tr = json.load(f)
+        traffic = (tr["dram_bytes_read"] + tr["dram_bytes_write"]) * npts / tr["points"]
+    except (OSError, KeyError, ValueError):
+        pass
     ar_s = ar_ms / 1e3 / max(args.steps, 1)
     achieved = per_launch_flops / ar_s / 1e12 if ar_s > 0 else None
 
@@ -336,19 +347,22 @@ def gpu_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (compensated), f64 fit",
             "data": "synthetic (seeded numpy draws; no external dataset)",
             "config": {"workload": "batched-256-surfaces",
-                       "surfaces": N_SURFACES, "points_per_rank": npts,
+                       "surfaces": len(batch), "points_per_rank": npts,
                        "orders": "{4,6,8,10}^3", "precision": "fp32c",
                        "l2": "inputs larger than L2 (%.1f GB per rank)" % (npts * 4 / 1e9),
                        "parallelism": f"dp{world} (independent surfaces per rank)"},
             "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": npts * 4},
+                    "d2h_bytes_per_step": npts * 4} if e2e else None,
             "plain_fp64": {"value": plain, "unit": "points/s",
                            "ratio_fp32c_over_fp64": (value / plain) if plain else None},
             "gpu_launches": launches,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": (achieved / fp32_peak) if achieved else None,
-                         "traffic": None,
+                         "traffic": traffic,
+                         "traffic_unit": "bytes per launch (ncu dram read+write, 24-surface "
+                                         "capture scaled by points)",
+                         "algorithmic_bytes": npts * 8,
                          "note": "ar32c: 2(P-1) flop per point over the batch / ar32c device "
                                  "time; peak = 148 SMs x 128 FP32 lanes x 2 x max SM clock "
                                  "(MEASURED_PEAKS.json has no FP32 figure)"},
@@ -371,6 +385,9 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--surfaces", type=int, default=N_SURFACES,
+                    help="use the first N surfaces of the batch (profiling runs)")
+    ap.add_argument("--skip-e2e", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
