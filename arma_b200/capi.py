@@ -21,6 +21,7 @@ ACF_STANDING, ACF_PROPAGATING = 0, 1
 FIT_BUNCH_KAUFMAN, FIT_CHOLESKY = 0, 1
 NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL = 0, 1
 NIT_BISECTION, NIT_LUT = 0, 1
+OUTPUT_FLAGS = ("none", "summary", "qq", "waves", "acf", "csv", "blitz", "binary", "surface")
 
 ERRORS = {
     -1: "ARMA_EINVAL", -2: "ARMA_ECUDA", -3: "ARMA_ENOMEM", -4: "ARMA_ETIMEDOUT",
@@ -36,6 +37,9 @@ EXPORTS = (
     "arma_ar_fit_analytic", "arma_white_noise", "arma_ar_filter",
     "arma_variance_renorm", "arma_nit_apply", "arma_velocity_linear",
     "arma_batch_generate", "arma_batch_generate_host", "arma_ar_filter_fp32c_noalloc",
+    "arma_driver_open", "arma_driver_close", "arma_driver_generate",
+    "arma_driver_compute_velocity", "arma_driver_write_all", "arma_driver_info",
+    "arma_driver_copy",
 )
 
 
@@ -113,6 +117,13 @@ def lib():
             "arma_batch_generate": (i, [vp, C.POINTER(Surface), i, i]),
             "arma_batch_generate_host": (i, [vp, C.POINTER(Surface), i, i]),
             "arma_ar_filter_fp32c_noalloc": (i, [vp, dp, ip, ip, vp]),
+            "arma_driver_open": (i, [C.c_char_p, i, C.POINTER(vp)]),
+            "arma_driver_close": (i, [vp]),
+            "arma_driver_generate": (i, [vp, vp]),
+            "arma_driver_compute_velocity": (i, [vp, vp]),
+            "arma_driver_write_all": (i, [vp, C.c_char_p]),
+            "arma_driver_info": (i, [vp, ip, dp, ip, dp, ip, C.POINTER(C.c_uint)]),
+            "arma_driver_copy": (i, [vp, i, dp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -317,3 +328,69 @@ def make_surface(shape, phi, var_wn, acf0, mt: MtParams, seed: int, buf_ptr: int
     s.d_zeta = buf_ptr
     s.scale = 0.0
     return s
+
+
+class Driver:
+    """An ``arma_driver``: a parsed ``.arma`` programme (the reference's
+    ARMA_driver) -- ``generate_wavy_surface``, ``compute_velocity_potentials``
+    and ``write_all`` run through the library."""
+
+    def __init__(self, config: str, is_path: bool = False):
+        h = C.c_void_p()
+        _check(lib().arma_driver_open(config.encode(), 1 if is_path else 0, C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def open(cls, path: str) -> "Driver":
+        return cls(path, is_path=True)
+
+    def close(self):
+        if self._h:
+            lib().arma_driver_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        shape, order, vs = (C.c_int * 3)(), (C.c_int * 3)(), (C.c_int * 4)()
+        delta = (C.c_double * 3)()
+        var = C.c_double()
+        fl = C.c_uint()
+        _check(lib().arma_driver_info(self._h, shape, delta, order, C.byref(var), vs,
+                                      C.byref(fl)))
+        return {"shape": tuple(shape), "delta": tuple(delta), "order": tuple(order),
+                "var_wn": var.value, "velocity_shape": tuple(vs),
+                "output": [n for k, n in enumerate(OUTPUT_FLAGS) if fl.value >> k & 1]}
+
+    def generate_wavy_surface(self, ctx: Context):
+        _check(lib().arma_driver_generate(ctx.handle, self._h))
+
+    def compute_velocity_potentials(self, ctx: Context):
+        _check(lib().arma_driver_compute_velocity(ctx.handle, self._h))
+
+    def write_all(self, directory: str = ""):
+        _check(lib().arma_driver_write_all(self._h, directory.encode()))
+
+    def _copy(self, what: int, shape) -> np.ndarray:
+        out = np.empty(tuple(shape), np.float64)
+        _check(lib().arma_driver_copy(self._h, what, _dp(out)))
+        return out
+
+    def zeta(self) -> np.ndarray:
+        return self._copy(0, self.info()["shape"])
+
+    def phi(self) -> np.ndarray:
+        return self._copy(1, self.info()["order"])
+
+    def velocity_potentials(self) -> np.ndarray:
+        return self._copy(2, self.info()["velocity_shape"])

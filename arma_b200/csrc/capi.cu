@@ -5,6 +5,7 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <sstream>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -684,6 +685,16 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 
 }  // namespace
 
+}  // extern "C"
+
+namespace armab {
+void batch_generate_device(Ctx* c, arma_surface* s, int n, int precision) {
+	batch(c, s, n, precision, false);
+}
+}  // namespace armab
+
+extern "C" {
+
 int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n, int precision) {
 	return guard([&] {
 		ARMA_REQUIRE(ctx && surfaces && n > 0, ARMA_EINVAL, "bad argument");
@@ -699,6 +710,94 @@ int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n, int p
 		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
 		scratch_begin(&ctx->c, 0);
 		batch(&ctx->c, surfaces, n, precision, true);
+	});
+}
+
+// ---------------------------------------------------------------- driver
+struct arma_driver {
+	armab::Driver* d;
+};
+
+int arma_driver_open(const char* config, int is_path, arma_driver** out) {
+	return guard([&] {
+		ARMA_REQUIRE(config && out, ARMA_EINVAL, "null argument");
+		std::string text;
+		if (is_path) {
+			std::ifstream f(config);
+			if (!f) throw Error{ARMA_EIO, std::string("cannot open ") + config};
+			std::ostringstream ss;
+			ss << f.rdbuf();
+			text = ss.str();
+		} else {
+			text = config;
+		}
+		std::unique_ptr<arma_driver> h(new arma_driver{nullptr});
+		h->d = driver_open(text);
+		*out = h.release();
+	});
+}
+
+int arma_driver_close(arma_driver* drv) {
+	return guard([&] {
+		if (!drv) return;
+		driver_close(drv->d);
+		delete drv;
+	});
+}
+
+int arma_driver_generate(arma_ctx* ctx, arma_driver* drv) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && drv, ARMA_EINVAL, "null argument");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		driver_generate(&ctx->c, drv->d);
+	});
+}
+
+int arma_driver_compute_velocity(arma_ctx* ctx, arma_driver* drv) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && drv, ARMA_EINVAL, "null argument");
+		ARMA_REQUIRE(driver_zeta(drv->d), ARMA_EINVAL, "no wavy surface: generate first");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		driver_velocity(&ctx->c, drv->d);
+	});
+}
+
+int arma_driver_write_all(arma_driver* drv, const char* dir) {
+	return guard([&] {
+		ARMA_REQUIRE(drv, ARMA_EINVAL, "null argument");
+		driver_write(drv->d, dir ? dir : "");
+	});
+}
+
+int arma_driver_info(arma_driver* drv, int shape[3], double delta[3], int order[3],
+                     double* var_wn, int vshape[4], unsigned* output_flags) {
+	return guard([&] {
+		ARMA_REQUIRE(drv, ARMA_EINVAL, "null argument");
+		driver_info(drv->d, shape, delta, order, var_wn, vshape, output_flags);
+	});
+}
+
+int arma_driver_copy(arma_driver* drv, int what, double* out) {
+	return guard([&] {
+		ARMA_REQUIRE(drv && out, ARMA_EINVAL, "null argument");
+		int shape[3], order[3], vs[4];
+		driver_info(drv->d, shape, nullptr, order, nullptr, vs, nullptr);
+		const double* src = nullptr;
+		size_t n = 0;
+		if (what == 0) {
+			src = driver_zeta(drv->d);
+			n = size_t(shape[0]) * shape[1] * shape[2];
+		} else if (what == 1) {
+			src = driver_phi(drv->d);
+			n = size_t(order[0]) * order[1] * order[2];
+		} else if (what == 2) {
+			src = driver_velocity_data(drv->d);
+			n = size_t(vs[0]) * vs[1] * vs[2] * vs[3];
+		}
+		ARMA_REQUIRE(src, ARMA_EINVAL, "nothing to copy (generate / compute first)");
+		std::memcpy(out, src, n * sizeof(double));
 	});
 }
 

@@ -181,6 +181,22 @@ void acf_eval(int kind, double amplitude, double velocity, const double alpha[3]
 // tx x ty quarter plane, FP64.
 void intra_slice_response(const double* phi, const int order[3], int tx, int ty,
                           double* h);
+// White noise + AR filter (+ renormalisation) into device buffers (capi.cu).
+void batch_generate_device(Ctx* c, arma_surface* s, int n, int precision);
+
+// The `.arma` programme layer (driver.cc).
+struct Driver;
+Driver* driver_open(const std::string& text);
+void driver_close(Driver* d);
+void driver_generate(Ctx* c, Driver* d);
+void driver_velocity(Ctx* c, Driver* d);
+void driver_write(Driver* d, const std::string& dir);
+void driver_info(const Driver* d, int shape[3], double delta[3], int order[3], double* var_wn,
+                 int vshape[4], unsigned* oflags);
+const double* driver_zeta(const Driver* d);
+const double* driver_phi(const Driver* d);
+const double* driver_velocity_data(const Driver* d);
+
 // Inverse-CDF table for the NIT LUT path.
 void nit_build_lut(int dist, const double params[3], double stdev, int nodes,
                    double range, double* x0, double* dx, std::vector<double>& y);

@@ -210,6 +210,29 @@ int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n,
 int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n,
                              int precision);
 
+/* ------------------------------------------------ programme layer */
+/* The reference's ARMA_driver (src/arma_driver.hh:43-150): parses a `.arma`
+ * configuration (`model = AR {...}`, `velocity_potential_solver = linear
+ * {...}`; the other registered names return ARMA_ENOTSUP), runs
+ * generate_wavy_surface / compute_velocity_potentials on the device, and
+ * writes zeta / zeta.csv / zeta.bin / phi / phi.csv like write_all
+ * (src/arma_driver.cc:29-178).  Extensions: `seed`, `mt_file`,
+ * `precision = fp64|fp32c`, `depth = inf`, `z_levels = [..]`. */
+typedef struct arma_driver arma_driver;
+int arma_driver_open(const char* config, int is_path, arma_driver** out);
+int arma_driver_close(arma_driver* drv);
+int arma_driver_generate(arma_ctx* ctx, arma_driver* drv);
+int arma_driver_compute_velocity(arma_ctx* ctx, arma_driver* drv);
+int arma_driver_write_all(arma_driver* drv, const char* dir);
+/* shape/delta of zeta, AR order, white-noise variance, velocity shape
+ * (nt_dom, nz, nx, ny) and the output flags (bit k = flag k of none,
+ * summary, qq, waves, acf, csv, blitz, binary, surface as in
+ * src/output_flags.cc:13-23); any pointer may be null. */
+int arma_driver_info(arma_driver* drv, int shape[3], double delta[3], int order[3],
+                     double* var_wn, int vshape[4], unsigned* output_flags);
+/* Copies zeta (what = 0), phi coefficients (1) or velocity potentials (2). */
+int arma_driver_copy(arma_driver* drv, int what, double* out);
+
 #ifdef __cplusplus
 }
 #endif
