@@ -7,7 +7,7 @@ to a CPU implementation -- if the library is missing, importing
 :mod:`arma_b200.capi` raises.
 """
 from .capi import (  # noqa: F401
-    ArmaError, Context, Driver, MtParams, Surface, lib, library_path,
+    ArmaError, Context, Driver, MtParams, Server, server_config, Surface, lib, library_path,
     FP64, FP32C, ACF_STANDING, ACF_PROPAGATING,
     NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL, NIT_BISECTION, NIT_LUT,
     acf_eval, ar_fit, ar_fit_analytic, mt19937_params, mt_file_count,

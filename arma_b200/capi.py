@@ -39,7 +39,9 @@ EXPORTS = (
     "arma_batch_generate", "arma_batch_generate_host", "arma_ar_filter_fp32c_noalloc",
     "arma_driver_open", "arma_driver_close", "arma_driver_generate",
     "arma_driver_compute_velocity", "arma_driver_write_all", "arma_driver_info",
-    "arma_driver_copy",
+    "arma_driver_copy", "arma_server_config_default", "arma_server_create",
+    "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
+    "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
 )
 
 
@@ -72,6 +74,48 @@ class Surface(C.Structure):
         ("phi", C.POINTER(C.c_double)), ("var_wn", C.c_double),
         ("acf0", C.c_double), ("mt", MtParams), ("seed", C.c_uint32),
         ("d_zeta", C.c_void_p), ("scale", C.c_double),
+    ]
+
+
+class ServerConfig(C.Structure):
+    """``arma_server_config``."""
+
+    _fields_ = [
+        ("chunk_slices", C.c_int), ("max_inflight", C.c_int), ("max_batch", C.c_int),
+        ("max_batch_points", C.c_longlong), ("hbm_budget", C.c_size_t), ("velocity", C.c_int),
+        ("depth", C.c_double), ("nz", C.c_int), ("z_levels", C.c_double * 8),
+        ("noise_margin", C.c_double),
+    ]
+
+
+class StreamSpec(C.Structure):
+    """``arma_stream_spec``."""
+
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("order", C.c_int * 3),
+        ("phi", C.POINTER(C.c_double)), ("var_wn", C.c_double), ("acf0", C.c_double),
+        ("mt", MtParams), ("seed", C.c_uint32), ("delta", C.c_double * 3),
+    ]
+
+
+class Completion(C.Structure):
+    """``arma_completion``."""
+
+    _fields_ = [
+        ("request", C.c_uint64), ("stream", C.c_uint64), ("chunk", C.c_uint64),
+        ("status", C.c_int), ("batch_size", C.c_int), ("latency_ms", C.c_double),
+        ("queue_ms", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    """``arma_server_stats``."""
+
+    _fields_ = [
+        ("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+        ("redone", C.c_uint64), ("launches", C.c_uint64), ("points", C.c_uint64),
+        ("resident_bytes", C.c_size_t), ("budget_bytes", C.c_size_t), ("streams", C.c_int),
+        ("resident_streams", C.c_int), ("inflight", C.c_int), ("pending", C.c_int),
     ]
 
 
@@ -124,6 +168,15 @@ def lib():
             "arma_driver_write_all": (i, [vp, C.c_char_p]),
             "arma_driver_info": (i, [vp, ip, dp, ip, dp, ip, C.POINTER(C.c_uint)]),
             "arma_driver_copy": (i, [vp, i, dp]),
+            "arma_server_config_default": (i, [C.POINTER(ServerConfig)]),
+            "arma_server_create": (i, [i, C.POINTER(ServerConfig), C.POINTER(vp)]),
+            "arma_server_destroy": (i, [vp]),
+            "arma_stream_open": (i, [vp, C.POINTER(StreamSpec), C.POINTER(C.c_uint64)]),
+            "arma_stream_close": (i, [vp, C.c_uint64]),
+            "arma_stream_submit": (i, [vp, C.c_uint64, vp, vp, C.POINTER(C.c_uint64)]),
+            "arma_server_poll": (i, [vp, C.POINTER(Completion), i, i, ip]),
+            "arma_server_stats_get": (i, [vp, C.POINTER(ServerStats)]),
+            "arma_server_last_failure": (i, [vp, C.c_char_p, sz]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -394,3 +447,112 @@ class Driver:
 
     def velocity_potentials(self) -> np.ndarray:
         return self._copy(2, self.info()["velocity_shape"])
+
+
+def server_config(**kw) -> ServerConfig:
+    """Defaults of ``arma_server_config_default`` with keyword overrides
+    (``z_levels`` as a sequence sets ``nz`` too)."""
+    cfg = ServerConfig()
+    _check(lib().arma_server_config_default(C.byref(cfg)))
+    for k, v in kw.items():
+        if k == "z_levels":
+            cfg.nz = len(v)
+            for j, z in enumerate(v):
+                cfg.z_levels[j] = z
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+class Server:
+    """An ``arma_server``: device-resident surface streams served in chunks
+    with continuous batching."""
+
+    def __init__(self, device: int = 0, config: ServerConfig | None = None, **kw):
+        self.config = config if config is not None else server_config(**kw)
+        h = C.c_void_p()
+        _check(lib().arma_server_create(device, C.byref(self.config), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def close(self):
+        if self._h:
+            _check(lib().arma_server_destroy(self._h))
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def open_stream(self, nx, ny, phi, var_wn, acf0, mt: MtParams, seed: int,
+                    delta=(1.0, 1.0, 1.0)) -> int:
+        phi = np.ascontiguousarray(phi, np.float64)
+        spec = StreamSpec()
+        spec.nx, spec.ny = int(nx), int(ny)
+        spec.order = (C.c_int * 3)(*phi.shape)
+        spec.phi = _dp(phi)
+        spec.var_wn = var_wn
+        spec.acf0 = acf0
+        spec.mt = mt
+        spec.seed = seed
+        spec.delta = (C.c_double * 3)(*delta)
+        sid = C.c_uint64()
+        _check(lib().arma_stream_open(self._h, C.byref(spec), C.byref(sid)))
+        return sid.value
+
+    def close_stream(self, sid: int):
+        _check(lib().arma_stream_close(self._h, sid))
+
+    def submit(self, sid: int, zeta_ptr: int, velocity_ptr: int = 0, keep=None) -> int:
+        """Queue the next chunk; the pointers must stay valid until completion
+        (``keep`` holds Python references until then)."""
+        rid = C.c_uint64()
+        _check(lib().arma_stream_submit(self._h, sid, C.c_void_p(zeta_ptr),
+                                        C.c_void_p(velocity_ptr or None), C.byref(rid)))
+        if keep is not None:
+            self._keep[rid.value] = keep
+        return rid.value
+
+    def poll(self, max_n: int = 256, timeout_ms: int = 0):
+        buf = (Completion * max_n)()
+        n = C.c_int()
+        _check(lib().arma_server_poll(self._h, buf, max_n, timeout_ms, C.byref(n)))
+        out = []
+        for k in range(n.value):
+            c = buf[k]
+            self._keep.pop(c.request, None)
+            out.append({"request": c.request, "stream": c.stream, "chunk": c.chunk,
+                        "status": c.status, "batch_size": c.batch_size,
+                        "latency_ms": c.latency_ms, "queue_ms": c.queue_ms})
+        return out
+
+    def wait(self, count: int, timeout_ms: int = 60000):
+        """Poll until `count` completions arrived (raises on timeout)."""
+        import time
+        got = []
+        deadline = time.monotonic() + timeout_ms / 1000.0
+        while len(got) < count:
+            left = int((deadline - time.monotonic()) * 1000)
+            if left <= 0:
+                raise TimeoutError(f"{len(got)} of {count} completions")
+            got += self.poll(256, min(left, 1000))
+        return got
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().arma_server_stats_get(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def last_failure(self) -> str:
+        buf = C.create_string_buffer(1024)
+        lib().arma_server_last_failure(self._h, buf, len(buf))
+        return buf.value.decode(errors="replace")

@@ -48,6 +48,7 @@ constexpr long long kSpinLimit = 1ll << 24;
 
 struct Task {
 	int nt, nx, ny, pt, px, py;
+	int t0;  // slices [0, t0) are history: read, never written
 	int tiles_x, tiles_y;
 	int ticket_base;
 	float* zeta;
@@ -196,6 +197,17 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 	for (int q = tid; q < pt * slot_sz; q += NTHREADS) ring[q] = 0.0f;
 	for (int q = tid; q < TX * SW; q += NTHREADS) ss[q] = 0.0f;
 	__syncthreads();
+	// history slices (a stream's previous chunk): the whole ring slot, tile
+	// and halo, straight from global memory (zero outside the surface)
+	for (int tt = max(0, tk.t0 - pt + 1); tt < tk.t0; ++tt) {
+		float* slot = ring + (tt % pt) * slot_sz;
+		const float* zs = tk.zeta + tt * sst;
+		for (int q = tid; q < slot_sz; q += NTHREADS) {
+			const int x = x0 - hx + q / W, y = y0 - LH + q % W;
+			if (x >= 0 && x < tk.nx && y >= 0 && y < tk.ny) slot[q] = __ldcg(zs + (long long)x * tk.ny + y);
+		}
+	}
+	__syncthreads();
 
 	const int gx = x0 + xl;
 	// 16-byte halo chunks need 16-byte aligned rows in global memory
@@ -210,7 +222,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 	const int dx_lo = grp == 0 ? 0 : (half ? 8 : 4);
 	const int dx_hi = grp == 0 ? (half ? 8 : 4) : TX;
 
-	for (int t = 0; t < tk.nt; ++t) {
+	for (int t = tk.t0; t < tk.nt; ++t) {
 		float* cur = ring + (t % pt) * slot_sz;
 		float* zt = tk.zeta + t * sst;
 		// group 0 starts from the noise of its strip (own tile: written by an
@@ -428,6 +440,7 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 		Task t;
 		t.nt = s.nt; t.nx = s.nx; t.ny = s.ny;
 		t.pt = s.pt; t.px = s.px; t.py = s.py;
+		t.t0 = s.t0;
 		t.tiles_x = s.tiles_x; t.tiles_y = s.tiles_y;
 		t.ticket_base = total;
 		t.zeta = s.zeta; t.phi = s.phi; t.phi_lo = s.phi_lo; t.h = s.h; t.h_lo = s.h_lo;
@@ -562,6 +575,7 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 	Task t;
 	t.nt = shape[0]; t.nx = shape[1]; t.ny = shape[2];
 	t.pt = order[0]; t.px = order[1]; t.py = order[2];
+	t.t0 = 0;
 	t.tiles_x = tiles_x; t.tiles_y = tiles_y;
 	t.ticket_base = 0;
 	t.zeta = d_zeta;

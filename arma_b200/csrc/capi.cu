@@ -14,14 +14,6 @@
 #include "distributions.h"
 #include "internal.h"
 
-struct arma_ctx {
-	armab::Ctx c;
-	std::vector<std::pair<char*, size_t>> chunks;  // scratch chunks
-	size_t used = 0;                                // bytes used in the last chunk
-	size_t high_water = 0;                          // total bytes taken in one call
-	size_t taken = 0;
-};
-
 namespace armab {
 
 namespace {
@@ -29,23 +21,6 @@ thread_local std::string g_last_error;
 
 arma_ctx* outer(Ctx* c) {
 	return reinterpret_cast<arma_ctx*>(reinterpret_cast<char*>(c) - offsetof(arma_ctx, c));
-}
-
-template <class F>
-int guard(F&& f) {
-	try {
-		f();
-		return ARMA_OK;
-	} catch (const Error& e) {
-		g_last_error = e.msg;
-		return e.code;
-	} catch (const std::bad_alloc&) {
-		g_last_error = "host allocation failed";
-		return ARMA_ENOMEM;
-	} catch (const std::exception& e) {
-		g_last_error = e.what();
-		return ARMA_EINVAL;
-	}
 }
 
 void require_shape(const int s[3], const char* name) {
@@ -59,6 +34,8 @@ size_t elem_size(int precision) {
 	return precision == ARMA_FP64 ? sizeof(double) : sizeof(float);
 }
 
+}  // namespace
+
 // Host-side copy of sgenrand-independent validation of a parameter set.
 void require_mt(const arma_mt_params* p) {
 	ARMA_REQUIRE(p, ARMA_EINVAL, "null MT parameter set");
@@ -71,6 +48,8 @@ uint64_t noise_attempts(size_t n, double margin) {
 	const double pairs = std::ceil(n / 2.0);
 	return uint64_t((pairs * (4.0 / dist::kPi) + 8.0 * std::sqrt(pairs) + 256.0) * margin);
 }
+
+namespace {
 
 void white_noise(Ctx* c, const arma_mt_params& p, uint32_t seed, double stddev, size_t n,
                  int precision, void* d_out) {
@@ -244,8 +223,6 @@ int arma_ctx_destroy(arma_ctx* ctx) {
 			cudaEventDestroy(p.stop);
 		}
 		for (auto& kv : ctx->c.graphs) cudaGraphExecDestroy(kv.second);
-		for (auto& kv : ctx->c.mt_tables)
-			for (int32_t* d : kv.second.bits) cudaFree(d);
 		for (auto& ch : ctx->chunks) cudaFree(ch.first);
 		cudaFree(ctx->c.d_err);
 		if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
@@ -463,6 +440,34 @@ int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed, doub
 	});
 }
 
+}  // extern "C"
+
+namespace armab {
+
+size_t ar32_coefficient_count(const int order[3]) {
+	return 2 * size_t(order[0]) * order[1] * order[2] + 2 * size_t(ar32c_tile_x()) * ar32c_tile_y();
+}
+
+void ar32_coefficients(const double* phi, const int order[3], float* b) {
+	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
+	const size_t nh = size_t(tx) * ty;
+	const int P = order[0] * order[1] * order[2];
+	std::vector<double> h(nh);
+	intra_slice_response(phi, order, tx, ty, h.data());
+	for (int i = 0; i < P; ++i) {
+		b[i] = float(phi[i]);
+		b[P + i] = float(phi[i] - double(b[i]));
+	}
+	for (size_t i = 0; i < nh; ++i) {
+		b[2 * P + i] = float(h[i]);
+		b[2 * P + nh + i] = float(h[i] - double(b[2 * P + i]));
+	}
+}
+
+}  // namespace armab
+
+extern "C" {
+
 namespace {
 
 // Device copies of the hi/lo float split of phi and of the intra-slice
@@ -476,20 +481,7 @@ std::vector<Ar32Surface> ar32_surfaces(Ctx* c, int n, const double* const* phis,
 	for (int k = 0; k < n; ++k)
 		off[k + 1] = off[k] + 2 * size_t(orders[k][0]) * orders[k][1] * orders[k][2] + 2 * nh;
 	std::vector<float> buf(off[n]);
-	std::vector<double> h(nh);
-	for (int k = 0; k < n; ++k) {
-		const int P = orders[k][0] * orders[k][1] * orders[k][2];
-		float* b = buf.data() + off[k];
-		intra_slice_response(phis[k], orders[k], tx, ty, h.data());
-		for (int i = 0; i < P; ++i) {
-			b[i] = float(phis[k][i]);
-			b[P + i] = float(phis[k][i] - double(b[i]));
-		}
-		for (size_t i = 0; i < nh; ++i) {
-			b[2 * P + i] = float(h[i]);
-			b[2 * P + nh + i] = float(h[i] - double(b[2 * P + i]));
-		}
-	}
+	for (int k = 0; k < n; ++k) ar32_coefficients(phis[k], orders[k], buf.data() + off[k]);
 	float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice,
 	                              c->stream));

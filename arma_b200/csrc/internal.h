@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <exception>
 #include <map>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -51,13 +53,6 @@ struct Ctx {
 	int num_sms = 148;
 	// cached CUDA graphs for the FP64 plane sweep, keyed by a string
 	std::map<std::string, cudaGraphExec_t> graphs;
-	// MT jump tables per parameter set: set-bit lists of t^(J 2^l) mod phi
-	struct MtTable {
-		bool ok = false;
-		std::vector<int32_t*> bits;  // device arrays, one per level
-		std::vector<int> nbits;
-	};
-	std::map<std::vector<uint32_t>, MtTable> mt_tables;
 	// optional per-kernel-class timing with CUDA events on `stream`
 	bool profiling = false;
 	struct Pending {
@@ -91,17 +86,34 @@ void* scratch_take(Ctx* c, size_t bytes);
 void check_device_error(Ctx* c);
 
 // ------------------------------------------------------------- launchers
-// MT: tempered words [offset, offset+n) of stream (p, seed) into d_out.
+// MT: tempered words [offset, offset+n) of stream (p, seed) into d_out.  A job
+// with `state` set starts from that raw window of nn words instead of the
+// seeded state (offset must then be 0).
 struct MtJob {
 	arma_mt_params p;
 	uint32_t seed;
 	unsigned long long offset, count;
 	uint32_t* out;
+	const uint32_t* state = nullptr;
 };
 void launch_mt_generate(Ctx* c, const arma_mt_params& p, uint32_t seed,
                         uint64_t offset, uint64_t n, uint32_t* d_out);
-// One launch generating every job's stream (one CTA per job).
-void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs);
+// Every job's stream in a few launches: streams longer than one segment of
+// 2^log2_seg words are split by jump-ahead into one CTA per segment.
+constexpr int kMtLog2Seg = 20;
+void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs,
+                              int log2_seg = kMtLog2Seg);
+// After a chunk consumed 4 * *attempts words of `words`: the raw window in
+// front of the next word (untempered copies of the nn words before it), and
+// *position += 4 * *attempts.  All on the device.
+struct MtWindowSpec {
+	arma_mt_params p;
+	const uint32_t* words;
+	const unsigned long long* attempts;
+	uint32_t* window;
+	unsigned long long* position;
+};
+void launch_mt_window_update(Ctx* c, const std::vector<MtWindowSpec>& specs);
 
 // White noise: n normals from the word stream d_words (n_words words).
 // enqueue_white_noise writes the number of accepted pairs to *d_pairs and does
@@ -114,12 +126,15 @@ bool launch_white_noise(Ctx* c, const uint32_t* d_words, uint64_t n_words,
                         double stddev, uint64_t n, int precision, void* d_out);
 // All surfaces of a batch in three launches; d_pairs[k] receives surface k's
 // number of accepted pairs (no synchronisation).
+// With `attempts` set (n even), the index + 1 of the polar attempt that gave
+// the last pair is written there: the words the noise consumed are 4 times it.
 struct NoiseSpec {
 	const uint32_t* words;
 	uint64_t n_words;
 	uint64_t n;
 	double stddev;
 	void* out;
+	unsigned long long* attempts = nullptr;
 };
 void enqueue_white_noise_batch(Ctx* c, const std::vector<NoiseSpec>& specs, int precision,
                                long long* d_pairs);
@@ -138,6 +153,7 @@ struct Ar32Surface {
 	const float* h;        // device, intra-slice impulse response (TX*TY), hi
 	const float* h_lo;     // device, lo part of h
 	int tiles_x, tiles_y;  // spatial tile grid
+	int t0 = 0;            // slices [0, t0) hold a finished history (streams)
 };
 void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx,
                   int ty, int tt);
@@ -153,7 +169,9 @@ struct RenormSpec {
 	double acf0;
 	double* d_scale;
 };
-void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int precision);
+// apply = false only computes the scales.
+void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int precision,
+                         bool apply = true);
 
 // NIT.
 void launch_nit_bisection(Ctx* c, int dist, const double params[3], double stdev,
@@ -201,4 +219,41 @@ const double* driver_velocity_data(const Driver* d);
 void nit_build_lut(int dist, const double params[3], double stdev, int nodes,
                    double range, double* x0, double* dx, std::vector<double>& y);
 
+// Polar attempts generated for n normals: the expected count plus 8 sigma,
+// times `margin` (capi.cu).
+uint64_t noise_attempts(size_t n, double margin);
+void require_mt(const arma_mt_params* p);
+// The FP32 tile kernel's coefficient block of one surface: phi hi, phi lo,
+// H hi, H lo (ar32_coefficient_count floats).
+size_t ar32_coefficient_count(const int order[3]);
+void ar32_coefficients(const double* phi, const int order[3], float* out);
+
+// Runs f, mapping library exceptions to status codes and the thread's last
+// error message.
+template <class F>
+int guard(F&& f) {
+	try {
+		f();
+		return ARMA_OK;
+	} catch (const Error& e) {
+		set_error(e.msg);
+		return e.code;
+	} catch (const std::bad_alloc&) {
+		set_error("host allocation failed");
+		return ARMA_ENOMEM;
+	} catch (const std::exception& e) {
+		set_error(e.what());
+		return ARMA_EINVAL;
+	}
+}
+
 }  // namespace armab
+
+// The context behind the opaque arma_ctx handle.
+struct arma_ctx {
+	armab::Ctx c;
+	std::vector<std::pair<char*, size_t>> chunks;  // scratch chunks
+	size_t used = 0;                                // bytes used in the last chunk
+	size_t high_water = 0;                          // total bytes taken in one call
+	size_t taken = 0;
+};

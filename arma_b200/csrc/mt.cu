@@ -19,6 +19,8 @@
 // k*2^(l+1) + 2^l.  All of it is bit-identical to the sequential generator.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "internal.h"
@@ -34,7 +36,6 @@ namespace {
 constexpr int kRingBits = 12;
 constexpr int kRing = 1 << kRingBits;  // ring of raw words, >= nn + (nn-mm)
 constexpr int kThreads = 256;
-constexpr int kLog2Seg = 20;           // segment length J = 2^20 words
 constexpr int kLevels = 16;            // jump tables for J * 2^l, l < 16
 
 struct SegJob {
@@ -114,9 +115,56 @@ mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	}
 }
 
+// Window of segment 0 of each jumped job: the seeded state, or a copy of the
+// job's own window.
 __global__ void mt_seed_kernel(const arma_mt_params* __restrict__ ps,
-                               const uint32_t* __restrict__ seeds, uint32_t* const* dst) {
-	if (threadIdx.x == 0) seed_state(dst[blockIdx.x], seeds[blockIdx.x], ps[blockIdx.x]);
+                               const uint32_t* __restrict__ seeds,
+                               const uint32_t* const* __restrict__ src, uint32_t* const* dst) {
+	const uint32_t* s = src[blockIdx.x];
+	if (s) {
+		for (int k = threadIdx.x; k < ps[blockIdx.x].nn; k += blockDim.x) dst[blockIdx.x][k] = s[k];
+	} else if (threadIdx.x == 0) {
+		seed_state(dst[blockIdx.x], seeds[blockIdx.x], ps[blockIdx.x]);
+	}
+}
+
+// Inverse of temper(): each xor-shift step y ^= (y >> s) (or (y << s) & mask)
+// is undone by the fixed-point iteration x <- y ^ (x >> s), which settles s
+// more bits per pass.
+__device__ __forceinline__ uint32_t undo_right(uint32_t y, int s) {
+	uint32_t x = y;
+	for (int k = 0; k < 32; k += s) x = y ^ (x >> s);
+	return x;
+}
+__device__ __forceinline__ uint32_t undo_left(uint32_t y, int s, uint32_t mask) {
+	uint32_t x = y;
+	for (int k = 0; k < 32; k += s) x = y ^ ((x << s) & mask);
+	return x;
+}
+__device__ __forceinline__ uint32_t untemper(uint32_t y, const arma_mt_params& p) {
+	y = undo_right(y, p.shift1);
+	y = undo_left(y, p.shiftC, p.maskC);
+	y = undo_left(y, p.shiftB, p.maskB);
+	return undo_right(y, p.shift0);
+}
+
+struct WindowJob {
+	arma_mt_params p;
+	const uint32_t* words;               // tempered words of the last chunk
+	const unsigned long long* attempts;  // polar attempts the chunk consumed
+	uint32_t* window;                    // raw window at the next word
+	unsigned long long* position;        // running word position (may be null)
+};
+
+// The raw window in front of word 4*attempts: untempered copies of the nn
+// words before it.
+__global__ void mt_window_kernel(const WindowJob* __restrict__ jobs) {
+	const WindowJob& jb = jobs[blockIdx.x];
+	const unsigned long long used = 4ull * *jb.attempts;
+	const int n = jb.p.nn;
+	for (int k = threadIdx.x; k < n; k += blockDim.x)
+		jb.window[k] = untemper(jb.words[used - n + k], jb.p);
+	if (threadIdx.x == 0 && jb.position) *jb.position += used;
 }
 
 // One CTA per jump: raw words y[0 .. p+n-2] from the source window in shared
@@ -164,14 +212,27 @@ std::vector<uint32_t> params_key(const arma_mt_params& p) {
 	return k;
 }
 
-const Ctx::MtTable& jump_table(Ctx* c, const arma_mt_params& p) {
+// Jump tables are cached per (device, parameter set, segment length) for the
+// life of the process; every context on the device shares them.
+struct MtTable {
+	bool ok = false;
+	std::vector<int32_t*> bits;  // device arrays, one per level
+	std::vector<int> nbits;
+};
+std::mutex g_table_mutex;
+std::map<std::vector<uint32_t>, MtTable> g_tables;
+
+const MtTable& jump_table(Ctx* c, const arma_mt_params& p, int log2_seg) {
 	auto key = params_key(p);
-	auto it = c->mt_tables.find(key);
-	if (it != c->mt_tables.end()) return it->second;
-	Ctx::MtTable t;
+	key.push_back(uint32_t(c->device));
+	key.push_back(uint32_t(log2_seg));
+	std::lock_guard<std::mutex> lock(g_table_mutex);
+	auto it = g_tables.find(key);
+	if (it != g_tables.end()) return it->second;
+	MtTable t;
 	std::vector<std::vector<int32_t>> bits;
 	int deg = 0;
-	t.ok = mt_jump_tables(p, kLog2Seg, kLevels, &bits, &deg);
+	t.ok = mt_jump_tables(p, log2_seg, kLevels, &bits, &deg);
 	if (t.ok) {
 		for (auto& b : bits) {
 			// pad to a multiple of 4 for vector loads (pads are never read)
@@ -184,24 +245,27 @@ const Ctx::MtTable& jump_table(Ctx* c, const arma_mt_params& p) {
 			t.nbits.push_back(int(b.size()));
 		}
 	}
-	return c->mt_tables.emplace(key, std::move(t)).first->second;
+	return g_tables.emplace(key, std::move(t)).first->second;
 }
 
 }  // namespace
 
-void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs) {
+void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_seg) {
 	ProfScope prof_(c, "mt");
+	ARMA_REQUIRE(log2_seg >= 12 && log2_seg <= 24, ARMA_EINVAL, "bad MT segment length");
 	for (const MtJob& j : jobs) {
+		ARMA_REQUIRE(!j.state || j.offset == 0, ARMA_EINVAL,
+		             "an MT job started from a window has no offset");
 		ARMA_REQUIRE(j.p.nn > 1 && j.p.mm > 0 && j.p.mm < j.p.nn && j.p.ww == 32, ARMA_EINVAL,
 		             "bad MT parameter set");
 		ARMA_REQUIRE(j.p.nn + (j.p.nn - j.p.mm) <= kRing, ARMA_EINVAL,
 		             "MT state too large for the device generator");
 	}
 	if (jobs.empty()) return;
-	const unsigned long long J = 1ull << kLog2Seg;
+	const unsigned long long J = 1ull << log2_seg;
 	// segments per job; jobs with more than one segment need jump tables
 	std::vector<int> K(jobs.size());
-	std::vector<const Ctx::MtTable*> tab(jobs.size(), nullptr);
+	std::vector<const MtTable*> tab(jobs.size(), nullptr);
 	int Kmax = 1;
 	size_t nstates = 0;
 	for (size_t q = 0; q < jobs.size(); ++q) {
@@ -209,7 +273,7 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs) {
 		ARMA_REQUIRE((total + J - 1) / J <= (1ull << kLevels), ARMA_EINVAL, "MT stream too long");
 		K[q] = int(std::max(1ull, (total + J - 1) / J));
 		if (K[q] > 1) {
-			tab[q] = &jump_table(c, jobs[q].p);
+			tab[q] = &jump_table(c, jobs[q].p, log2_seg);
 			if (!tab[q]->ok) K[q] = 1;  // not a full-period set: one sequential segment
 		}
 		if (K[q] > 1) nstates += size_t(K[q]) * jobs[q].p.nn;
@@ -221,6 +285,7 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs) {
 		size_t off = 0;
 		std::vector<arma_mt_params> ps;
 		std::vector<uint32_t> seeds;
+		std::vector<const uint32_t*> src;
 		std::vector<uint32_t*> dst;
 		for (size_t q = 0; q < jobs.size(); ++q) {
 			if (K[q] <= 1) continue;
@@ -228,18 +293,22 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs) {
 			off += size_t(K[q]) * jobs[q].p.nn;
 			ps.push_back(jobs[q].p);
 			seeds.push_back(jobs[q].seed);
+			src.push_back(jobs[q].state);
 			dst.push_back(state0[q]);
 		}
 		auto* d_ps = static_cast<arma_mt_params*>(scratch_take(c, sizeof(arma_mt_params) * ps.size()));
 		auto* d_seeds = static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * seeds.size()));
+		auto* d_src = static_cast<const uint32_t**>(scratch_take(c, sizeof(uint32_t*) * src.size()));
 		auto* d_dst = static_cast<uint32_t**>(scratch_take(c, sizeof(uint32_t*) * dst.size()));
 		ARMA_CUDA_TRY(cudaMemcpyAsync(d_ps, ps.data(), sizeof(arma_mt_params) * ps.size(),
 		                              cudaMemcpyHostToDevice, c->stream));
 		ARMA_CUDA_TRY(cudaMemcpyAsync(d_seeds, seeds.data(), sizeof(uint32_t) * seeds.size(),
 		                              cudaMemcpyHostToDevice, c->stream));
+		ARMA_CUDA_TRY(cudaMemcpyAsync(d_src, src.data(), sizeof(uint32_t*) * src.size(),
+		                              cudaMemcpyHostToDevice, c->stream));
 		ARMA_CUDA_TRY(cudaMemcpyAsync(d_dst, dst.data(), sizeof(uint32_t*) * dst.size(),
 		                              cudaMemcpyHostToDevice, c->stream));
-		mt_seed_kernel<<<int(ps.size()), 32, 0, c->stream>>>(d_ps, d_seeds, d_dst);
+		mt_seed_kernel<<<int(ps.size()), 32, 0, c->stream>>>(d_ps, d_seeds, d_src, d_dst);
 		c->launches += 1;
 		// binary tree of jumps, widest stride first
 		int levels = 0;
@@ -281,7 +350,7 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs) {
 			SegJob s;
 			s.p = jobs[q].p;
 			s.seed = jobs[q].seed;
-			s.state = K[q] > 1 ? state0[q] + size_t(k) * jobs[q].p.nn : nullptr;
+			s.state = K[q] > 1 ? state0[q] + size_t(k) * jobs[q].p.nn : jobs[q].state;
 			s.first = first;
 			s.count = K[q] > 1 ? std::min(J, total - first) : total;
 			s.offset = jobs[q].offset;
@@ -293,6 +362,21 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs) {
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d_seg, seg.data(), sizeof(SegJob) * seg.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
 	mt_generate_kernel<<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg);
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 1;
+}
+
+void launch_mt_window_update(Ctx* c, const std::vector<MtWindowSpec>& specs) {
+	if (specs.empty()) return;
+	ProfScope prof_(c, "mt");
+	std::vector<WindowJob> jobs(specs.size());
+	for (size_t k = 0; k < specs.size(); ++k)
+		jobs[k] = WindowJob{specs[k].p, specs[k].words, specs[k].attempts, specs[k].window,
+		                    specs[k].position};
+	auto* d_jobs = static_cast<WindowJob*>(scratch_take(c, sizeof(WindowJob) * jobs.size()));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(WindowJob) * jobs.size(),
+	                              cudaMemcpyHostToDevice, c->stream));
+	mt_window_kernel<<<int(jobs.size()), 256, 0, c->stream>>>(d_jobs);
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 }

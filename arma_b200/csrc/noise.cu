@@ -193,6 +193,7 @@ struct NoiseJob {
 	unsigned long long n;
 	double stddev;
 	void* out;
+	unsigned long long* attempts;
 	int block_base;
 	int nblocks;
 };
@@ -273,6 +274,7 @@ noise_scatter_batch_kernel(const NoiseJob* __restrict__ jobs, int njobs,
 			out[i0] = T(__dadd_rn(__dmul_rn(__dmul_rn(at[k].y, m), jb.stddev), 0.0));
 			if (i0 + 1 < jb.n)
 				out[i0 + 1] = T(__dadd_rn(__dmul_rn(__dmul_rn(at[k].x, m), jb.stddev), 0.0));
+			if (jb.attempts && i0 + 2 == jb.n) *jb.attempts = a0 + k + 1;
 		}
 		++rank;
 	}
@@ -288,8 +290,11 @@ void enqueue_white_noise_batch(Ctx* c, const std::vector<NoiseSpec>& specs, int 
 	for (size_t k = 0; k < specs.size(); ++k) {
 		const uint64_t na = specs[k].n_words / 4;
 		const long long nb = (long long)std::max<uint64_t>(1, (na + kPerBlock - 1) / kPerBlock);
+		ARMA_REQUIRE(!specs[k].attempts || specs[k].n % 2 == 0, ARMA_EINVAL,
+		             "a noise chunk that continues a stream needs an even count");
 		jobs[k] = NoiseJob{reinterpret_cast<const uint4*>(specs[k].words), na, specs[k].n,
-		                   specs[k].stddev, specs[k].out, int(total_blocks), int(nb)};
+		                   specs[k].stddev, specs[k].out, specs[k].attempts, int(total_blocks),
+		                   int(nb)};
 		total_blocks += nb;
 	}
 	ARMA_REQUIRE(total_blocks < (1ll << 31), ARMA_EINVAL, "white noise batch too large");

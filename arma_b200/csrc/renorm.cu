@@ -171,7 +171,8 @@ scale_batch_kernel(const RenormJob* __restrict__ jobs, int blocks_per_job) {
 
 }  // namespace
 
-void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int precision) {
+void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int precision,
+                         bool apply) {
 	ProfScope prof_(c, "renorm");
 	if (specs.empty()) return;
 	std::vector<RenormJob> jobs(specs.size());
@@ -198,16 +199,16 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 0, means);
 		partial_batch_kernel<double><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
-		scale_batch_kernel<double><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
+		if (apply) scale_batch_kernel<double><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
 	} else {
 		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, nullptr, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 0, means);
 		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
-		scale_batch_kernel<float><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
+		if (apply) scale_batch_kernel<float><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
-	c->launches += 5;
+	c->launches += apply ? 5 : 4;
 }
 
 }  // namespace armab

@@ -233,6 +233,76 @@ int arma_driver_info(arma_driver* drv, int shape[3], double delta[3], int order[
 /* Copies zeta (what = 0), phi coefficients (1) or velocity potentials (2). */
 int arma_driver_copy(arma_driver* drv, int what, double* out);
 
+/* ------------------------------------------------ serving */
+/* No counterpart in the reference.  A server owns device-resident surface
+ * streams: each stream is an unbounded surface of fixed nx x ny with one AR
+ * model (FP32 compensated filter) and one dcmt stream, generated in chunks of
+ * chunk_slices time slices.  A stream's chunks concatenated equal one surface
+ * generated in a single call with the same seed; with acf0 > 0 every chunk is
+ * scaled by the renormalisation factor of the first chunk.  Requests for the
+ * next chunk of any stream are batched continuously by a host thread (up to
+ * max_inflight device batches overlap) and admitted by the HBM footprint of
+ * the stream state (two slice buffers of pt-1+chunk_slices slices, the MT
+ * window, velocity and output staging). */
+typedef struct arma_server arma_server;
+typedef struct {
+	int chunk_slices;           /* T, even (default 64) */
+	int max_inflight;           /* device batches in flight, 1..8 (default 3) */
+	int max_batch;              /* requests per batch (default 64) */
+	long long max_batch_points; /* surface points per batch (default 2^26) */
+	size_t hbm_budget;          /* bytes of stream state (0: half the free memory) */
+	int velocity;               /* 1: velocity potentials of every chunk slice */
+	double depth;               /* velocity solver depth (INFINITY allowed) */
+	int nz;                     /* number of z levels, 1..8 */
+	double z_levels[8];
+	double noise_margin;        /* multiplier of the polar-attempt estimate (1) */
+} arma_server_config;
+
+typedef struct {
+	int nx, ny;
+	int order[3];          /* pt, px, py */
+	const double* phi;     /* FP64 coefficients, copied at open */
+	double var_wn;
+	double acf0;           /* > 0: renormalise by the first chunk */
+	arma_mt_params mt;
+	uint32_t seed;
+	double delta[3];       /* grid steps (t, x, y) for the velocity solver */
+} arma_stream_spec;
+
+typedef struct {
+	uint64_t request, stream, chunk;
+	int status;            /* ARMA_OK or an error code */
+	int batch_size;        /* requests in the device batch that ran it */
+	double latency_ms;     /* submit -> outputs in place */
+	double queue_ms;       /* submit -> launch */
+} arma_completion;
+
+typedef struct {
+	uint64_t submitted, completed, batches, redone, launches;
+	uint64_t points;       /* surface points delivered */
+	size_t resident_bytes, budget_bytes;
+	int streams, resident_streams, inflight, pending;
+} arma_server_stats;
+
+int arma_server_config_default(arma_server_config* cfg);
+int arma_server_create(int device, const arma_server_config* cfg, arma_server** out);
+/* Finishes every queued request, then frees everything. */
+int arma_server_destroy(arma_server* srv);
+int arma_stream_open(arma_server* srv, const arma_stream_spec* spec, uint64_t* stream_id);
+/* The stream's memory is released once its queued requests are done. */
+int arma_stream_close(arma_server* srv, uint64_t stream_id);
+/* Queues the stream's next chunk.  zeta_out: chunk_slices*nx*ny floats;
+ * velocity_out: chunk_slices*nz*nx*ny floats (t, z, x, y) or NULL.  Both must
+ * be device memory or page-locked host memory and stay valid until the
+ * request completes. */
+int arma_stream_submit(arma_server* srv, uint64_t stream_id, float* zeta_out,
+                       float* velocity_out, uint64_t* request_id);
+/* Up to max completions; waits up to timeout_ms (-1: forever) for the first. */
+int arma_server_poll(arma_server* srv, arma_completion* out, int max, int timeout_ms, int* n);
+int arma_server_stats_get(arma_server* srv, arma_server_stats* out);
+/* The last failure the serving thread saw (empty if none). */
+int arma_server_last_failure(arma_server* srv, char* buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif
