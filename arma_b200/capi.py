@@ -42,6 +42,7 @@ EXPORTS = (
     "arma_driver_copy", "arma_server_config_default", "arma_server_create",
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
+    "arma_server_profile",
 )
 
 
@@ -84,7 +85,7 @@ class ServerConfig(C.Structure):
         ("chunk_slices", C.c_int), ("max_inflight", C.c_int), ("max_batch", C.c_int),
         ("max_batch_points", C.c_longlong), ("hbm_budget", C.c_size_t), ("velocity", C.c_int),
         ("depth", C.c_double), ("nz", C.c_int), ("z_levels", C.c_double * 8),
-        ("noise_margin", C.c_double),
+        ("noise_margin", C.c_double), ("profile", C.c_int),
     ]
 
 
@@ -177,6 +178,7 @@ def lib():
             "arma_server_poll": (i, [vp, C.POINTER(Completion), i, i, ip]),
             "arma_server_stats_get": (i, [vp, C.POINTER(ServerStats)]),
             "arma_server_last_failure": (i, [vp, C.c_char_p, sz]),
+            "arma_server_profile": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_uint64)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -551,6 +553,13 @@ class Server:
         st = ServerStats()
         _check(lib().arma_server_stats_get(self._h, C.byref(st)))
         return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def profile(self, name: str):
+        """(milliseconds, scopes) of one kernel class when profiling is on."""
+        ms = C.c_double()
+        n = C.c_uint64()
+        _check(lib().arma_server_profile(self._h, name.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def last_failure(self) -> str:
         buf = C.create_string_buffer(1024)

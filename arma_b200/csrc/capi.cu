@@ -4,7 +4,9 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <new>
 #include <stdexcept>
@@ -105,15 +107,45 @@ void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
 void set_error(const std::string& msg) { g_last_error = msg; }
 const std::string& last_error() { return g_last_error; }
 
+cudaMemPool_t library_pool(int device) {
+	static std::mutex m;
+	static std::map<int, cudaMemPool_t> pools;
+	std::lock_guard<std::mutex> lk(m);
+	auto it = pools.find(device);
+	if (it != pools.end()) return it->second;
+	cudaMemPoolProps props{};
+	props.allocType = cudaMemAllocationTypePinned;
+	props.location.type = cudaMemLocationTypeDevice;
+	props.location.id = device;
+	cudaMemPool_t pool;
+	ARMA_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+	uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool for reuse
+	ARMA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+	pools.emplace(device, pool);
+	return pool;
+}
+
+void* pool_alloc(Ctx* c, size_t bytes) {
+	void* p = nullptr;
+	if (cudaMallocFromPoolAsync(&p, bytes, library_pool(c->device), c->stream) != cudaSuccess) {
+		cudaGetLastError();
+		throw Error{ARMA_ENOMEM, "device allocation failed"};
+	}
+	return p;
+}
+
+void pool_free(Ctx* c, void* p) {
+	if (p) cudaFreeAsync(p, c->stream);
+}
+
+// Chunks come from the library's stream-ordered pool, so growing or merging
+// the arena never synchronises the device.
 void scratch_begin(Ctx* c, size_t) {
 	arma_ctx* o = outer(c);
 	if (o->chunks.size() > 1 || (o->chunks.size() == 1 && o->chunks[0].second < o->high_water)) {
-		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
-		for (auto& ch : o->chunks) cudaFree(ch.first);
+		for (auto& ch : o->chunks) pool_free(c, ch.first);
 		o->chunks.clear();
-		char* p = nullptr;
-		if (cudaMalloc(&p, o->high_water) != cudaSuccess)
-			throw Error{ARMA_ENOMEM, "device scratch allocation failed"};
+		char* p = static_cast<char*>(pool_alloc(c, o->high_water));
 		o->chunks.emplace_back(p, o->high_water);
 	}
 	o->used = 0;
@@ -125,9 +157,7 @@ void* scratch_take(Ctx* c, size_t bytes) {
 	bytes = (bytes + 255) & ~size_t(255);
 	if (o->chunks.empty() || o->used + bytes > o->chunks.back().second) {
 		const size_t sz = std::max(bytes, size_t(64) << 20);
-		char* p = nullptr;
-		if (cudaMalloc(&p, sz) != cudaSuccess)
-			throw Error{ARMA_ENOMEM, "device scratch allocation failed"};
+		char* p = static_cast<char*>(pool_alloc(c, sz));
 		o->chunks.emplace_back(p, sz);
 		o->used = 0;
 	}
@@ -136,6 +166,18 @@ void* scratch_take(Ctx* c, size_t bytes) {
 	o->taken += bytes;
 	o->high_water = std::max(o->high_water, o->taken);
 	return r;
+}
+
+ScratchMark scratch_mark(Ctx* c) {
+	arma_ctx* o = outer(c);
+	return ScratchMark{o->chunks.size(), o->used, o->taken};
+}
+
+void scratch_release(Ctx* c, const ScratchMark& m) {
+	arma_ctx* o = outer(c);
+	if (o->chunks.size() != m.chunks) return;  // grew meanwhile: keep going forward
+	o->used = m.used;
+	o->taken = m.taken;
 }
 
 ProfScope::ProfScope(Ctx* c, const char* name) : c_(c) {
@@ -223,7 +265,8 @@ int arma_ctx_destroy(arma_ctx* ctx) {
 			cudaEventDestroy(p.stop);
 		}
 		for (auto& kv : ctx->c.graphs) cudaGraphExecDestroy(kv.second);
-		for (auto& ch : ctx->chunks) cudaFree(ch.first);
+		for (auto& ch : ctx->chunks) pool_free(&ctx->c, ch.first);
+		cudaStreamSynchronize(ctx->c.stream);
 		cudaFree(ctx->c.d_err);
 		if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
 		delete ctx;
@@ -233,10 +276,10 @@ int arma_ctx_destroy(arma_ctx* ctx) {
 int arma_ctx_set_stream(arma_ctx* ctx, void* stream) {
 	return guard([&] {
 		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
-		if (ctx->c.own_stream) {
-			ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
-			ARMA_CUDA_TRY(cudaStreamDestroy(ctx->c.stream));
-		}
+		// scratch allocated in the old stream's order must be complete before
+		// the new stream uses it
+		ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+		if (ctx->c.own_stream) ARMA_CUDA_TRY(cudaStreamDestroy(ctx->c.stream));
 		ctx->c.stream = static_cast<cudaStream_t>(stream);
 		ctx->c.own_stream = false;
 	});

@@ -82,6 +82,17 @@ void resolve_profile(Ctx* c);
 // high-water size (synchronising the stream first).
 void scratch_begin(Ctx* c, size_t total_bytes);
 void* scratch_take(Ctx* c, size_t bytes);
+// Work enqueued in order on the context's stream may reuse scratch: take a
+// mark, enqueue, release back to the mark.
+struct ScratchMark {
+	size_t chunks, used, taken;
+};
+ScratchMark scratch_mark(Ctx* c);
+void scratch_release(Ctx* c, const ScratchMark& m);
+// The library's stream-ordered device memory pool (one per device; freed
+// blocks are kept for reuse).  Allocations are ordered on c->stream.
+void* pool_alloc(Ctx* c, size_t bytes);
+void pool_free(Ctx* c, void* p);
 
 void check_device_error(Ctx* c);
 

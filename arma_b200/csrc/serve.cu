@@ -44,7 +44,7 @@ using Clock = std::chrono::steady_clock;
 
 constexpr int kCopyThreads = 256;
 constexpr int kCopyBlocksPerJob = 64;
-constexpr int kStreamLog2Seg = 16;  // MT segments of 2^16 words: short chains per chunk
+constexpr int kStreamLog2Seg = 18;  // MT segments of 2^18 words per chunk job
 constexpr int kMaxSlots = 8;
 
 // ---------------------------------------------------------------- kernels
@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(kCopyThreads) copy_batch_kernel(const CopyJob*
 
 void launch_copies(Ctx* c, const std::vector<CopyJob>& jobs) {
 	if (jobs.empty()) return;
+	ProfScope prof_(c, "copy");
 	auto* d = static_cast<CopyJob*>(scratch_take(c, sizeof(CopyJob) * jobs.size()));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d, jobs.data(), sizeof(CopyJob) * jobs.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
@@ -176,8 +177,8 @@ struct arma_server {
 	void harvest();
 	bool form_and_launch(armab::Slot& sl, std::unique_lock<std::mutex>& lk);
 	uint64_t launch(armab::Slot& sl);
-	void make_resident(armab::StreamState* st, cudaStream_t s);
-	void release(armab::StreamState* st, cudaStream_t s);
+	void make_resident(armab::StreamState* st, armab::Ctx* c);
+	void release(armab::StreamState* st, armab::Ctx* c);
 	size_t footprint(const armab::StreamState& st) const;
 	void complete(armab::Slot& sl, size_t k, int status);
 };
@@ -198,15 +199,11 @@ size_t arma_server::footprint(const StreamState& st) const {
 	return b;
 }
 
-void arma_server::make_resident(StreamState* st, cudaStream_t s) {
+void arma_server::make_resident(StreamState* st, Ctx* c) {
 	const size_t T = size_t(cfg.chunk_slices);
 	const size_t nz = cfg.velocity ? size_t(cfg.nz) : 0;
-	void* p = nullptr;
-	if (cudaMallocAsync(&p, st->bytes, s) != cudaSuccess) {
-		cudaGetLastError();
-		throw Error{ARMA_ENOMEM, "stream state allocation failed"};
-	}
-	char* m = static_cast<char*>(p);
+	cudaStream_t s = c->stream;
+	char* m = static_cast<char*>(pool_alloc(c, st->bytes));
 	st->mem = m;
 	auto take = [&](size_t b) {
 		char* r = m;
@@ -229,8 +226,8 @@ void arma_server::make_resident(StreamState* st, cudaStream_t s) {
 	st->resident = true;
 }
 
-void arma_server::release(StreamState* st, cudaStream_t s) {
-	if (st->resident && st->mem) cudaFreeAsync(st->mem, s);
+void arma_server::release(StreamState* st, Ctx* c) {
+	if (st->resident && st->mem) pool_free(c, st->mem);
 	st->mem = nullptr;
 	st->resident = false;
 	resident_bytes -= st->bytes;
@@ -307,7 +304,7 @@ uint64_t arma_server::launch(Slot& sl) {
 	const size_t n = sl.reqs.size();
 	const int nz = cfg.velocity ? cfg.nz : 0;
 	for (Request& r : sl.reqs)
-		if (!r.st->resident) make_resident(r.st, s);
+		if (!r.st->resident) make_resident(r.st, c);
 	const uint64_t launches0 = c->launches;
 	// 1. history: the previous chunk's last H slices in front of this one
 	std::vector<CopyJob> hist;
@@ -404,8 +401,10 @@ uint64_t arma_server::launch(Slot& sl) {
 			std::vector<int> tidx(T);
 			for (int t = 0; t < T; ++t) tidx[t] = t0 + t;
 			const float* z = first ? st->buf[cur] + size_t(st->H) * st->n2 : st->buf[cur];
+			const ScratchMark mark = scratch_mark(c);  // streams run in order: share scratch
 			launch_velocity_linear(c, z, shape, ARMA_FP32C, st->delta, cfg.depth, cfg.z_levels, nz,
 			                       tidx.data(), T, st->vel);
+			scratch_release(c, mark);
 		}
 	}
 	// 8. outputs: scaled into the caller's device buffers or into staging
@@ -510,7 +509,7 @@ void arma_server::harvest() {
 	for (auto it = streams.begin(); it != streams.end();) {
 		StreamState* st = it->second.get();
 		if (st->closed && st->queued == 0 && !st->busy) {
-			if (st->resident) release(st, slots[0].ctx->c.stream);
+			if (st->resident) release(st, &slots[0].ctx->c);
 			it = streams.erase(it);
 			any = true;
 		} else {
@@ -581,16 +580,11 @@ int arma_server_create(int device, const arma_server_config* cfg, arma_server** 
 		size_t free_b = 0, total_b = 0;
 		ARMA_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
 		srv->budget = cfg->hbm_budget ? cfg->hbm_budget : free_b / 2;
-		// keep freed stream state in the pool instead of returning it to the
-		// driver between streams
-		cudaMemPool_t pool;
-		ARMA_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, device));
-		uint64_t keep = UINT64_MAX;
-		ARMA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
 		srv->slots.resize(cfg->max_inflight);
 		for (Slot& sl : srv->slots) {
 			const int rc = arma_ctx_create(device, &sl.ctx);
 			if (rc != ARMA_OK) throw Error{rc, last_error()};
+			sl.ctx->c.profiling = cfg->profile != 0;
 			ARMA_CUDA_TRY(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
 			ARMA_CUDA_TRY(cudaHostAlloc(&sl.h_pairs, sizeof(long long) * (cfg->max_batch + 1),
 			                            cudaHostAllocDefault));
@@ -613,7 +607,7 @@ int arma_server_destroy(arma_server* srv) {
 		if (srv->thread.joinable()) srv->thread.join();
 		cudaSetDevice(srv->device);
 		for (auto& kv : srv->streams)
-			if (kv.second->resident) srv->release(kv.second.get(), srv->slots[0].ctx->c.stream);
+			if (kv.second->resident) srv->release(kv.second.get(), &srv->slots[0].ctx->c);
 		for (Slot& sl : srv->slots) {
 			if (sl.ctx) cudaStreamSynchronize(sl.ctx->c.stream);
 			if (sl.done) cudaEventDestroy(sl.done);
@@ -756,6 +750,25 @@ int arma_server_stats_get(arma_server* srv, arma_server_stats* out) {
 		out->resident_streams = res;
 		out->inflight = infl;
 		out->pending = int(srv->pending.size());
+	});
+}
+
+int arma_server_profile(arma_server* srv, const char* name, double* ms, uint64_t* launches) {
+	return guard([&] {
+		ARMA_REQUIRE(srv && name && ms && launches, ARMA_EINVAL, "null argument");
+		std::lock_guard<std::mutex> lk(srv->mu);
+		*ms = 0.0;
+		*launches = 0;
+		ARMA_CUDA_TRY(cudaSetDevice(srv->device));
+		for (Slot& sl : srv->slots) {
+			if (sl.busy) continue;  // its events may not have fired yet
+			resolve_profile(&sl.ctx->c);
+			auto it = sl.ctx->c.prof_ms.find(name);
+			if (it != sl.ctx->c.prof_ms.end()) {
+				*ms += it->second;
+				*launches += uint64_t(sl.ctx->c.prof_count[name]);
+			}
+		}
 	});
 }
 

@@ -339,6 +339,10 @@ def gpu_arm(args):
                "sample": f"{len(sample)} smallest surfaces of the batch ({points(sample)} points), "
                          f"OpenMP block wavefront restatement, {t:.1f} s"}
 
+    serving = None
+    if world == 1 and not args.skip_serve:
+        serving = serve_bench(A, args.serve_seconds)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
@@ -367,6 +371,10 @@ def gpu_arm(args):
                                  "time; peak = 148 SMs x 128 FP32 lanes x 2 x max SM clock "
                                  "(MEASURED_PEAKS.json has no FP32 figure)"},
             "cpu_baseline": cpu,
+            "latency": ({"p50_ms": serving["p50_ms_at_50pct"], "p99_ms": serving["p99_ms_at_50pct"],
+                         "p99_128x128x64_ms": serving["p99_128x128x64_ms_at_50pct"],
+                         "load": 0.5, "source": "serving"} if serving else None),
+            "serving": serving,
             "clocks": clk.summary(),
             "wall_s_timed": wall,
         }
@@ -374,6 +382,120 @@ def gpu_arm(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------- serving
+SERVE_SIDES = (64, 128, 256)
+SERVE_T = 64
+
+
+def serve_bench(A, seconds_per_load: float, seed: int = 42):
+    """Serving workload: streams of x = y in {64, 128, 256}, AR order 8^3
+    (standing / propagating ACFs alternating), FP32 filter with the velocity
+    potential at z = 0, chunks of 64 slices delivered into pinned host memory.
+    Capacity is measured closed-loop (four chunks queued for each of 48
+    streams); then Poisson arrivals at 10-90 % of it, each a request for the
+    next chunk of a random stream or, with probability 0.1, a new stream that
+    replaces a random one of the same size.  Latency = submit -> chunk and
+    velocity in host memory (the server's clock)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    mt = A.mt19937_params()
+    fits = [A.ar_fit_analytic(A.ACF_STANDING, (8, 8, 8), 1.5, 0.8, [0.05] * 3, [0.5, 0.5]),
+            A.ar_fit_analytic(A.ACF_PROPAGATING, (8, 8, 8), 1.0, 0.6, [0.04] * 3, [0.3, 0.2])]
+    srv = A.Server(chunk_slices=SERVE_T, velocity=1, z_levels=[0.0], max_inflight=3)
+    next_seed = [1000]
+
+    def open_stream(k, side):
+        phi, var = fits[k % 2]
+        next_seed[0] += 1
+        return srv.open_stream(side, side, phi, var, 1.0, mt, next_seed[0])
+
+    streams = [(open_stream(k, SERVE_SIDES[k % 3]), SERVE_SIDES[k % 3]) for k in range(48)]
+    pool = {side: [(torch.empty((SERVE_T, side, side), dtype=torch.float32).pin_memory(),
+                    torch.empty((SERVE_T, 1, side, side), dtype=torch.float32).pin_memory())
+                   for _ in range(68)] for side in SERVE_SIDES}
+    inflight = {}
+
+    def submit(i):
+        sid, side = streams[i]
+        b = pool[side].pop()
+        inflight[srv.submit(sid, b[0].data_ptr(), b[1].data_ptr())] = (b, side)
+
+    def collect(done):
+        for d in done:
+            b, side = inflight.pop(d["request"])
+            pool[side].append(b)
+            if d["status"] != 0:
+                raise RuntimeError(f"serving request failed: {d} {srv.last_failure()}")
+            d["side"] = side
+        return done
+
+    try:
+        for _ in range(2):  # warm-up: every stream's first chunks, scratch growth
+            for i in range(len(streams)):
+                submit(i)
+            collect(srv.wait(len(streams), 120000))
+        zero = {}
+        for i in range(3):
+            lat = []
+            for _ in range(15):
+                submit(i)
+                lat.append(collect(srv.wait(1))[0]["latency_ms"])
+            zero[f"{streams[i][1]}x{streams[i][1]}x{SERVE_T}"] = float(np.median(lat))
+        npts = 0
+        t0 = time.perf_counter()
+        for _ in range(4):
+            for i in range(len(streams)):
+                submit(i)
+                npts += SERVE_T * streams[i][1] ** 2
+        collect(srv.wait(4 * len(streams), 120000))
+        dt = time.perf_counter() - t0
+        cap = 4 * len(streams) / dt
+        loads = []
+        for load in (0.1, 0.3, 0.5, 0.7, 0.9):
+            lam = load * cap
+            n = max(50, int(lam * seconds_per_load))
+            arrivals = np.cumsum(rng.exponential(1.0 / lam, n))
+            picks = rng.integers(0, len(streams), n)
+            fresh = rng.random(n) < 0.1
+            res = []
+            start = time.perf_counter()
+            for a, i, new in zip(arrivals, picks, fresh):
+                while time.perf_counter() - start < a:
+                    res += collect(srv.poll(256, 0))
+                while not pool[streams[i][1]]:
+                    res += collect(srv.poll(256, 1))
+                if new:
+                    side = streams[i][1]
+                    srv.close_stream(streams[i][0])
+                    streams[i] = (open_stream(int(i), side), side)
+                submit(i)
+            res += collect(srv.wait(n - len(res), 120000))
+            span = time.perf_counter() - start
+            lat = np.array([r["latency_ms"] for r in res])
+            l128 = np.array([r["latency_ms"] for r in res if r["side"] == 128])
+            loads.append({"load": load, "rate_per_s": lam, "requests": n,
+                          "achieved_per_s": n / span,
+                          "p50_ms": float(np.percentile(lat, 50)),
+                          "p99_ms": float(np.percentile(lat, 99)),
+                          "p50_128_ms": float(np.percentile(l128, 50)) if l128.size else None,
+                          "p99_128_ms": float(np.percentile(l128, 99)) if l128.size else None,
+                          "mean_batch": float(np.mean([r["batch_size"] for r in res]))})
+        st = srv.stats()
+    finally:
+        srv.close()
+    half = next(x for x in loads if x["load"] == 0.5)
+    return {
+        "workload": "serving: 48 streams x,y in {64,128,256}, order 8^3, chunks of 64 slices, "
+                    "fp32c + velocity at z=0, outputs to pinned host memory, Poisson arrivals, "
+                    "10% new streams",
+        "capacity_chunks_per_s": cap, "capacity_points_per_s": npts / dt,
+        "zero_load_p50_ms": zero, "loads": loads,
+        "p50_ms_at_50pct": half["p50_ms"], "p99_ms_at_50pct": half["p99_ms"],
+        "p99_128x128x64_ms_at_50pct": half["p99_128_ms"],
+        "server": {k: st[k] for k in ("batches", "completed", "redone", "launches")},
+    }
 
 
 def main():
@@ -388,6 +510,9 @@ def main():
     ap.add_argument("--surfaces", type=int, default=N_SURFACES,
                     help="use the first N surfaces of the batch (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-serve", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=1.5,
+                    help="Poisson phase length per load level")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

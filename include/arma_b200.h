@@ -256,6 +256,7 @@ typedef struct {
 	int nz;                     /* number of z levels, 1..8 */
 	double z_levels[8];
 	double noise_margin;        /* multiplier of the polar-attempt estimate (1) */
+	int profile;                /* 1: time kernel classes with CUDA events */
 } arma_server_config;
 
 typedef struct {
@@ -300,6 +301,9 @@ int arma_stream_submit(arma_server* srv, uint64_t stream_id, float* zeta_out,
 /* Up to max completions; waits up to timeout_ms (-1: forever) for the first. */
 int arma_server_poll(arma_server* srv, arma_completion* out, int max, int timeout_ms, int* n);
 int arma_server_stats_get(arma_server* srv, arma_server_stats* out);
+/* With profile = 1: device milliseconds and scopes of one kernel class
+ * ("mt", "noise", "ar32c", "renorm", "velocity", "copy") over idle slots. */
+int arma_server_profile(arma_server* srv, const char* name, double* ms, uint64_t* launches);
 /* The last failure the serving thread saw (empty if none). */
 int arma_server_last_failure(arma_server* srv, char* buf, size_t len);
 
