@@ -105,7 +105,7 @@ class Completion(C.Structure):
     _fields_ = [
         ("request", C.c_uint64), ("stream", C.c_uint64), ("chunk", C.c_uint64),
         ("status", C.c_int), ("batch_size", C.c_int), ("latency_ms", C.c_double),
-        ("queue_ms", C.c_double),
+        ("queue_ms", C.c_double), ("device_ms", C.c_double),
     ]
 
 
@@ -117,6 +117,7 @@ class ServerStats(C.Structure):
         ("redone", C.c_uint64), ("launches", C.c_uint64), ("points", C.c_uint64),
         ("resident_bytes", C.c_size_t), ("budget_bytes", C.c_size_t), ("streams", C.c_int),
         ("resident_streams", C.c_int), ("inflight", C.c_int), ("pending", C.c_int),
+        ("launch_ms_total", C.c_double), ("launch_ms_max", C.c_double),
     ]
 
 
@@ -534,7 +535,8 @@ class Server:
             self._keep.pop(c.request, None)
             out.append({"request": c.request, "stream": c.stream, "chunk": c.chunk,
                         "status": c.status, "batch_size": c.batch_size,
-                        "latency_ms": c.latency_ms, "queue_ms": c.queue_ms})
+                        "latency_ms": c.latency_ms, "queue_ms": c.queue_ms,
+                        "device_ms": c.device_ms})
         return out
 
     def wait(self, count: int, timeout_ms: int = 60000):

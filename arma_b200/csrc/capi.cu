@@ -121,6 +121,11 @@ cudaMemPool_t library_pool(int device) {
 	ARMA_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
 	uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool for reuse
 	ARMA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+	// never make an allocation on one stream wait for a free still queued on
+	// another (concurrent serving batches would serialise); reuse only
+	// blocks whose free has completed, else grow the pool
+	int no = 0;
+	ARMA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
 	pools.emplace(device, pool);
 	return pool;
 }
@@ -166,6 +171,16 @@ void* scratch_take(Ctx* c, size_t bytes) {
 	o->taken += bytes;
 	o->high_water = std::max(o->high_water, o->taken);
 	return r;
+}
+
+void scratch_reserve(Ctx* c, size_t bytes) {
+	arma_ctx* o = outer(c);
+	o->high_water = std::max(o->high_water, bytes);
+	scratch_begin(c, 0);
+	if (o->chunks.empty()) {
+		char* p = static_cast<char*>(pool_alloc(c, o->high_water));
+		o->chunks.emplace_back(p, o->high_water);
+	}
 }
 
 ScratchMark scratch_mark(Ctx* c) {

@@ -88,6 +88,9 @@ struct ScratchMark {
 	size_t chunks, used, taken;
 };
 ScratchMark scratch_mark(Ctx* c);
+// Grows the arena to at least `bytes` in one chunk now, so that later calls
+// of up to that size never allocate.
+void scratch_reserve(Ctx* c, size_t bytes);
 void scratch_release(Ctx* c, const ScratchMark& m);
 // The library's stream-ordered device memory pool (one per device; freed
 // blocks are kept for reuse).  Allocations are ordered on c->stream.
@@ -114,12 +117,14 @@ void launch_mt_generate(Ctx* c, const arma_mt_params& p, uint32_t seed,
 constexpr int kMtLog2Seg = 20;
 void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs,
                               int log2_seg = kMtLog2Seg);
-// After a chunk consumed 4 * *attempts words of `words`: the raw window in
-// front of the next word (untempered copies of the nn words before it), and
-// *position += 4 * *attempts.  All on the device.
+// After a chunk consumed 4 * *attempts words of `words` (n_words long): the
+// raw window in front of the next word (untempered copies of the nn words
+// before it), and *position += 4 * *attempts.  All on the device; an attempt
+// count outside [nn/4, n_words/4] (0: the noise ran short) changes nothing.
 struct MtWindowSpec {
 	arma_mt_params p;
 	const uint32_t* words;
+	unsigned long long n_words;
 	const unsigned long long* attempts;
 	uint32_t* window;
 	unsigned long long* position;
@@ -196,6 +201,19 @@ void launch_velocity_linear(Ctx* c, const void* d_zeta, const int shape[3],
                             int precision, const double delta[3], double depth,
                             const double* z, int nz, const int* t_idx, int ntd,
                             void* d_out);
+// Many surfaces of one slice shape nx x ny in one set of launches: surface k
+// has nt slices at zeta, its slices t_idx[0..ntd) go to out as (ntd, nz, nx,
+// ny); dt is its time step.
+struct VelocitySurface {
+	const void* zeta;
+	void* out;
+	int nt;
+	const int* t_idx;
+	int ntd;
+	double dt;
+};
+void launch_velocity_linear_batch(Ctx* c, const VelocitySurface* v, int n, int nx, int ny,
+                                  int precision, double depth, const double* z, int nz);
 
 // Host math shared by the ABI (fit.cc).
 int fit_gauss_table(const double* acf, const int acf_shape[3], const int order[3],

@@ -37,6 +37,7 @@ constexpr int kRingBits = 12;
 constexpr int kRing = 1 << kRingBits;  // ring of raw words, >= nn + (nn-mm)
 constexpr int kThreads = 256;
 constexpr int kLevels = 16;            // jump tables for J * 2^l, l < 16
+constexpr int kJumpThreads = 640;
 
 struct SegJob {
 	arma_mt_params p;
@@ -151,30 +152,40 @@ __device__ __forceinline__ uint32_t untemper(uint32_t y, const arma_mt_params& p
 struct WindowJob {
 	arma_mt_params p;
 	const uint32_t* words;               // tempered words of the last chunk
+	unsigned long long n_words;          // words generated for it
 	const unsigned long long* attempts;  // polar attempts the chunk consumed
 	uint32_t* window;                    // raw window at the next word
 	unsigned long long* position;        // running word position (may be null)
 };
 
 // The raw window in front of word 4*attempts: untempered copies of the nn
-// words before it.
+// words before it.  A chunk whose noise ran short reports no attempt count
+// (0): the window is left as it was and the chunk is generated again.
 __global__ void mt_window_kernel(const WindowJob* __restrict__ jobs) {
 	const WindowJob& jb = jobs[blockIdx.x];
 	const unsigned long long used = 4ull * *jb.attempts;
 	const int n = jb.p.nn;
+	if (used < (unsigned long long)n || used > jb.n_words) return;
 	for (int k = threadIdx.x; k < n; k += blockDim.x)
 		jb.window[k] = untemper(jb.words[used - n + k], jb.p);
 	if (threadIdx.x == 0 && jb.position) *jb.position += used;
 }
 
-// One CTA per jump: raw words y[0 .. p+n-2] from the source window in shared
-// memory, then dst[w] = XOR over the set bits i of y[i + w].
-__global__ void __launch_bounds__(1024)
-mt_jump_kernel(const JumpJob* __restrict__ jobs) {
+// `parts` CTAs per jump: each computes the raw words y[0 .. p+n-2] from the
+// source window in shared memory, then its share of the destination window,
+// dst[w] = XOR over the set bits i of y[i + w], with the bit list split among
+// several threads per word and the partial XORs combined in shared memory.
+// More parts shorten a jump when few jumps run at once.
+__global__ void __launch_bounds__(kJumpThreads)
+mt_jump_kernel(const JumpJob* __restrict__ jobs, int parts) {
 	extern __shared__ uint32_t y[];
-	const JumpJob& jb = jobs[blockIdx.x];
+	const JumpJob& jb = jobs[blockIdx.x / parts];
 	const arma_mt_params p = jb.p;
 	const int n = p.nn, m = p.mm, chunk = n - m;
+	const int per = (n + parts - 1) / parts;
+	const int w0 = (blockIdx.x % parts) * per;
+	if (w0 >= n) return;  // uniform over the CTA
+	const int cnt = min(n, w0 + per) - w0;
 	const int deg = 32 * n - p.rr;
 	const int len = deg + n - 1;
 	for (int k = threadIdx.x; k < n; k += blockDim.x) y[k] = jb.src[k];
@@ -189,19 +200,31 @@ mt_jump_kernel(const JumpJob* __restrict__ jobs) {
 		}
 		__syncthreads();
 	}
-	for (int w = threadIdx.x; w < n; w += blockDim.x) {
+	uint32_t* acc = y + len;  // lanes * cnt <= blockDim.x partial XORs
+	const int lanes = max(1, int(blockDim.x) / cnt);
+	const int wl = threadIdx.x % cnt, lane = threadIdx.x / cnt;
+	if (lane < lanes) {
+		const int nb = jb.nbits;
+		const int span = ((nb + lanes - 1) / lanes + 3) & ~3;  // multiple of 4: aligned int4 loads
+		const int b0 = min(nb, lane * span), b1 = min(nb, b0 + span);
+		const int w = w0 + wl;
 		uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0;
-		int it = 0;
-		const int nb4 = jb.nbits & ~3;
-		for (; it < nb4; it += 4) {
+		int it = b0;
+		for (; it + 4 <= b1; it += 4) {
 			const int4 b = *reinterpret_cast<const int4*>(jb.bits + it);
 			r0 ^= y[b.x + w];
 			r1 ^= y[b.y + w];
 			r2 ^= y[b.z + w];
 			r3 ^= y[b.w + w];
 		}
-		for (; it < jb.nbits; ++it) r0 ^= y[jb.bits[it] + w];
-		jb.dst[w] = r0 ^ r1 ^ r2 ^ r3;
+		for (; it < b1; ++it) r0 ^= y[jb.bits[it] + w];
+		acc[lane * cnt + wl] = r0 ^ r1 ^ r2 ^ r3;
+	}
+	__syncthreads();
+	for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+		uint32_t r = 0;
+		for (int l = 0; l < lanes; ++l) r ^= acc[l * cnt + t];
+		jb.dst[w0 + t] = r;
 	}
 }
 
@@ -317,7 +340,7 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		for (size_t q = 0; q < jobs.size(); ++q)
 			if (K[q] > 1)
 				smem = std::max(smem, sizeof(uint32_t) * size_t(32 * jobs[q].p.nn - jobs[q].p.rr +
-				                                                jobs[q].p.nn));
+				                                                jobs[q].p.nn + kJumpThreads));
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(mt_jump_kernel,
 		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
 		for (int lv = levels - 1; lv >= 0; --lv) {
@@ -335,7 +358,12 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 			auto* d_jj = static_cast<JumpJob*>(scratch_take(c, sizeof(JumpJob) * jj.size()));
 			ARMA_CUDA_TRY(cudaMemcpyAsync(d_jj, jj.data(), sizeof(JumpJob) * jj.size(),
 			                              cudaMemcpyHostToDevice, c->stream));
-			mt_jump_kernel<<<int(jj.size()), 640, smem, c->stream>>>(d_jj);
+			// few jumps at this level: split each over several CTAs
+			int parts = int(std::min<size_t>(8, std::max<size_t>(1, (2 * size_t(c->num_sms) +
+			                                                         jj.size() - 1) / jj.size())));
+			for (const JumpJob& j : jj)  // every CTA's share must fit one word per thread
+				parts = std::max(parts, (j.p.nn + kJumpThreads - 1) / kJumpThreads);
+			mt_jump_kernel<<<int(jj.size()) * parts, kJumpThreads, smem, c->stream>>>(d_jj, parts);
 			ARMA_CUDA_TRY(cudaGetLastError());
 			c->launches += 1;
 		}
@@ -371,8 +399,8 @@ void launch_mt_window_update(Ctx* c, const std::vector<MtWindowSpec>& specs) {
 	ProfScope prof_(c, "mt");
 	std::vector<WindowJob> jobs(specs.size());
 	for (size_t k = 0; k < specs.size(); ++k)
-		jobs[k] = WindowJob{specs[k].p, specs[k].words, specs[k].attempts, specs[k].window,
-		                    specs[k].position};
+		jobs[k] = WindowJob{specs[k].p, specs[k].words, specs[k].n_words, specs[k].attempts,
+		                    specs[k].window, specs[k].position};
 	auto* d_jobs = static_cast<WindowJob*>(scratch_take(c, sizeof(WindowJob) * jobs.size()));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(WindowJob) * jobs.size(),
 	                              cudaMemcpyHostToDevice, c->stream));

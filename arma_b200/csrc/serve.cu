@@ -29,6 +29,7 @@
 #include <condition_variable>
 #include <cstdio>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -44,7 +45,7 @@ using Clock = std::chrono::steady_clock;
 
 constexpr int kCopyThreads = 256;
 constexpr int kCopyBlocksPerJob = 64;
-constexpr int kStreamLog2Seg = 18;  // MT segments of 2^18 words per chunk job
+constexpr int kStreamLog2Seg = 16;  // MT segments of 2^16 words: short generation chains
 constexpr int kMaxSlots = 8;
 
 // ---------------------------------------------------------------- kernels
@@ -140,6 +141,7 @@ struct Request {
 
 struct Slot {
 	arma_ctx* ctx = nullptr;
+	cudaEvent_t begin = nullptr;  // batch start on the device
 	cudaEvent_t done = nullptr;
 	long long* h_pairs = nullptr;  // pinned: pairs per request, then the error word
 	bool busy = false;
@@ -269,6 +271,7 @@ bool arma_server::form_and_launch(Slot& sl, std::unique_lock<std::mutex>& lk) {
 	int code = ARMA_OK;
 	std::string msg;
 	uint64_t nl = 0;
+	const auto t_launch = Clock::now();
 	try {
 		nl = launch(sl);
 	} catch (const Error& e) {
@@ -293,6 +296,9 @@ bool arma_server::form_and_launch(Slot& sl, std::unique_lock<std::mutex>& lk) {
 	}
 	stats.batches += 1;
 	stats.launches += nl;
+	const double lms = ms_between(t_launch, Clock::now());
+	stats.launch_ms_total += lms;
+	stats.launch_ms_max = std::max(stats.launch_ms_max, lms);
 	return true;
 }
 
@@ -306,6 +312,7 @@ uint64_t arma_server::launch(Slot& sl) {
 	for (Request& r : sl.reqs)
 		if (!r.st->resident) make_resident(r.st, c);
 	const uint64_t launches0 = c->launches;
+	ARMA_CUDA_TRY(cudaEventRecord(sl.begin, s));
 	// 1. history: the previous chunk's last H slices in front of this one
 	std::vector<CopyJob> hist;
 	for (Request& r : sl.reqs) {
@@ -319,6 +326,8 @@ uint64_t arma_server::launch(Slot& sl) {
 	// 2. MT words: from the seed (first chunk) or from the stream's window
 	auto* d_att = static_cast<unsigned long long*>(scratch_take(c, sizeof(unsigned long long) * n));
 	auto* d_pairs = static_cast<long long*>(scratch_take(c, sizeof(long long) * n));
+	// a chunk whose noise runs short writes no attempt count: 0 marks it
+	ARMA_CUDA_TRY(cudaMemsetAsync(d_att, 0, sizeof(unsigned long long) * n, s));
 	std::vector<MtJob> mj(n);
 	std::vector<uint64_t> att(n);
 	for (size_t k = 0; k < n; ++k) {
@@ -345,7 +354,7 @@ uint64_t arma_server::launch(Slot& sl) {
 	for (size_t k = 0; k < n; ++k) {
 		StreamState* st = sl.reqs[k].st;
 		const int cur = int(sl.reqs[k].chunk & 1);
-		ws[k] = MtWindowSpec{st->mt, mj[k].out, d_att + k, st->window[cur ^ 1], nullptr};
+		ws[k] = MtWindowSpec{st->mt, mj[k].out, 4 * att[k], d_att + k, st->window[cur ^ 1], nullptr};
 	}
 	launch_mt_window_update(c, ws);
 	// 5. the AR filter of every chunk in one launch
@@ -390,20 +399,32 @@ uint64_t arma_server::launch(Slot& sl) {
 		}
 	}
 	launch_renorm_batch(c, rs, ARMA_FP32C, false);
-	// 7. velocity potentials of the chunk slices
+	// 7. velocity potentials of the chunk slices: one set of launches per
+	//    slice shape
 	if (nz > 0) {
+		std::map<std::pair<int, int>, std::vector<VelocitySurface>> groups;
+		std::vector<std::vector<int>> tidx_keep;
+		tidx_keep.reserve(sl.reqs.size());
 		for (Request& r : sl.reqs) {
 			StreamState* st = r.st;
 			const int cur = int(r.chunk & 1);
 			const bool first = r.chunk == 0;
 			const int t0 = first ? 0 : st->H;
-			const int shape[3] = {t0 + T, st->nx, st->ny};
-			std::vector<int> tidx(T);
-			for (int t = 0; t < T; ++t) tidx[t] = t0 + t;
-			const float* z = first ? st->buf[cur] + size_t(st->H) * st->n2 : st->buf[cur];
-			const ScratchMark mark = scratch_mark(c);  // streams run in order: share scratch
-			launch_velocity_linear(c, z, shape, ARMA_FP32C, st->delta, cfg.depth, cfg.z_levels, nz,
-			                       tidx.data(), T, st->vel);
+			tidx_keep.emplace_back(T);
+			for (int t = 0; t < T; ++t) tidx_keep.back()[t] = t0 + t;
+			VelocitySurface v;
+			v.zeta = first ? st->buf[cur] + size_t(st->H) * st->n2 : st->buf[cur];
+			v.out = st->vel;
+			v.nt = t0 + T;
+			v.t_idx = tidx_keep.back().data();
+			v.ntd = T;
+			v.dt = st->delta[0];
+			groups[{st->nx, st->ny}].push_back(v);
+		}
+		for (auto& g : groups) {
+			const ScratchMark mark = scratch_mark(c);  // groups run in order: share scratch
+			launch_velocity_linear_batch(c, g.second.data(), int(g.second.size()), g.first.first,
+			                             g.first.second, ARMA_FP32C, cfg.depth, cfg.z_levels, nz);
 			scratch_release(c, mark);
 		}
 	}
@@ -450,6 +471,11 @@ void arma_server::complete(Slot& sl, size_t k, int status) {
 	cpl.latency_ms = ms_between(r.submit, now);
 	cpl.queue_ms = ms_between(r.submit, r.launch);
 	cpl.batch_size = int(sl.reqs.size());
+	float dev_ms = 0.0f;
+	if (!sl.failed && cudaEventElapsedTime(&dev_ms, sl.begin, sl.done) == cudaSuccess)
+		cpl.device_ms = dev_ms;
+	else
+		cudaGetLastError();
 	done.push_back(cpl);
 	st->busy = false;
 	st->queued -= 1;
@@ -585,7 +611,12 @@ int arma_server_create(int device, const arma_server_config* cfg, arma_server** 
 			const int rc = arma_ctx_create(device, &sl.ctx);
 			if (rc != ARMA_OK) throw Error{rc, last_error()};
 			sl.ctx->c.profiling = cfg->profile != 0;
-			ARMA_CUDA_TRY(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+			// scratch of a full batch, reserved up front: MT words (~10.2 bytes
+			// a point), spectra for several depths, velocity work buffers
+			const size_t per_point = 11 + (cfg->velocity && cfg->nz > 1 ? 8 * size_t(cfg->nz) : 0);
+			scratch_reserve(&sl.ctx->c, size_t(cfg->max_batch_points) * per_point + (640u << 20));
+			ARMA_CUDA_TRY(cudaEventCreate(&sl.begin));
+			ARMA_CUDA_TRY(cudaEventCreate(&sl.done));
 			ARMA_CUDA_TRY(cudaHostAlloc(&sl.h_pairs, sizeof(long long) * (cfg->max_batch + 1),
 			                            cudaHostAllocDefault));
 		}
@@ -610,6 +641,7 @@ int arma_server_destroy(arma_server* srv) {
 			if (kv.second->resident) srv->release(kv.second.get(), &srv->slots[0].ctx->c);
 		for (Slot& sl : srv->slots) {
 			if (sl.ctx) cudaStreamSynchronize(sl.ctx->c.stream);
+			if (sl.begin) cudaEventDestroy(sl.begin);
 			if (sl.done) cudaEventDestroy(sl.done);
 			if (sl.h_pairs) cudaFreeHost(sl.h_pairs);
 			if (sl.ctx) arma_ctx_destroy(sl.ctx);

@@ -276,6 +276,7 @@ typedef struct {
 	int batch_size;        /* requests in the device batch that ran it */
 	double latency_ms;     /* submit -> outputs in place */
 	double queue_ms;       /* submit -> launch */
+	double device_ms;      /* the batch's time on the GPU */
 } arma_completion;
 
 typedef struct {
@@ -283,6 +284,7 @@ typedef struct {
 	uint64_t points;       /* surface points delivered */
 	size_t resident_bytes, budget_bytes;
 	int streams, resident_streams, inflight, pending;
+	double launch_ms_total, launch_ms_max;  /* host time spent enqueueing batches */
 } arma_server_stats;
 
 int arma_server_config_default(arma_server_config* cfg);
