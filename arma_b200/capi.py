@@ -42,7 +42,7 @@ EXPORTS = (
     "arma_driver_copy", "arma_server_config_default", "arma_server_create",
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
-    "arma_server_profile",
+    "arma_server_profile", "arma_velocity_linear_batch",
 )
 
 
@@ -75,6 +75,15 @@ class Surface(C.Structure):
         ("phi", C.POINTER(C.c_double)), ("var_wn", C.c_double),
         ("acf0", C.c_double), ("mt", MtParams), ("seed", C.c_uint32),
         ("d_zeta", C.c_void_p), ("scale", C.c_double),
+    ]
+
+
+class VelocityJob(C.Structure):
+    """``arma_velocity_job``."""
+
+    _fields_ = [
+        ("d_zeta", C.c_void_p), ("d_out", C.c_void_p), ("nt", C.c_int),
+        ("t_idx", C.POINTER(C.c_int)), ("ntd", C.c_int), ("dt", C.c_double),
     ]
 
 
@@ -180,6 +189,7 @@ def lib():
             "arma_server_stats_get": (i, [vp, C.POINTER(ServerStats)]),
             "arma_server_last_failure": (i, [vp, C.c_char_p, sz]),
             "arma_server_profile": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_uint64)]),
+            "arma_velocity_linear_batch": (i, [vp, C.POINTER(VelocityJob), i, i, i, i, d, dp, i]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -351,6 +361,20 @@ class Context:
                                           dlp, depth, zsp, len(zs),
                                           ti.ctypes.data_as(C.POINTER(C.c_int)), len(ti),
                                           C.c_void_p(d_out)))
+
+    def velocity_linear_batch(self, jobs, nx: int, ny: int, precision: int, depth: float,
+                              z_levels):
+        """jobs: (d_zeta, d_out, nt, t_idx, dt) per surface of slice shape nx x ny."""
+        arr = (VelocityJob * len(jobs))()
+        keep = []
+        for k, (dz, do, nt, tidx, dt) in enumerate(jobs):
+            ti = np.ascontiguousarray(tidx, np.int32)
+            keep.append(ti)
+            arr[k] = VelocityJob(C.c_void_p(dz), C.c_void_p(do), int(nt),
+                                 ti.ctypes.data_as(C.POINTER(C.c_int)), len(ti), float(dt))
+        zs, zsp = _d(z_levels)
+        _check(lib().arma_velocity_linear_batch(self._h, arr, len(jobs), nx, ny, precision, depth,
+                                                zsp, len(zs)))
 
     def batch_generate(self, surfaces, precision: int, host: bool = False):
         arr = (Surface * len(surfaces))(*surfaces)

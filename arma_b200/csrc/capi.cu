@@ -677,6 +677,31 @@ int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3], 
 	});
 }
 
+int arma_velocity_linear_batch(arma_ctx* ctx, const arma_velocity_job* jobs, int n, int nx, int ny,
+                               int precision, double depth, const double* z, int nz) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && jobs && z && n >= 0, ARMA_EINVAL, "null argument");
+		ARMA_REQUIRE(nx > 0 && ny > 0 && nz > 0, ARMA_EINVAL, "Bad \"domain\": empty");
+		for (int j = 0; j < nz; ++j)
+			ARMA_REQUIRE(!(z[j] < -depth), ARMA_EINVAL, "min(z) is less than -h");
+		elem_size(precision);
+		std::vector<VelocitySurface> v(n);
+		for (int k = 0; k < n; ++k) {
+			const arma_velocity_job& j = jobs[k];
+			ARMA_REQUIRE(j.d_zeta && j.d_out && j.t_idx && j.nt > 0 && j.ntd > 0, ARMA_EINVAL,
+			             "bad velocity job");
+			for (int i = 0; i < j.ntd; ++i)
+				ARMA_REQUIRE(j.t_idx[i] >= 0 && j.t_idx[i] < j.nt, ARMA_EINVAL,
+				             "Bad \"domain\": t outside the surface");
+			v[k] = VelocitySurface{j.d_zeta, j.d_out, j.nt, j.t_idx, j.ntd, j.dt > 0 ? j.dt : 1.0};
+		}
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		launch_velocity_linear_batch(&ctx->c, v.data(), n, nx, ny, precision, depth, z, nz);
+		ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
+	});
+}
+
 // ---------------------------------------------------------------- batches
 namespace {
 

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <map>
 #include <memory>
@@ -173,6 +174,10 @@ struct arma_server {
 	std::vector<armab::Slot> slots;
 	arma_server_stats stats{};
 	size_t resident_bytes = 0;
+	// state blocks of closed streams kept for reuse by new streams of the
+	// same footprint (allocating fresh device memory can take tens of ms)
+	std::multimap<size_t, char*> spare;
+	size_t spare_bytes = 0;
 	std::string fatal;  // loop-thread failure outside any request
 
 	void loop();
@@ -181,6 +186,7 @@ struct arma_server {
 	uint64_t launch(armab::Slot& sl);
 	void make_resident(armab::StreamState* st, armab::Ctx* c);
 	void release(armab::StreamState* st, armab::Ctx* c);
+	void reserve_block(armab::StreamState* st, armab::Ctx* c);
 	size_t footprint(const armab::StreamState& st) const;
 	void complete(armab::Slot& sl, size_t k, int status);
 };
@@ -205,8 +211,8 @@ void arma_server::make_resident(StreamState* st, Ctx* c) {
 	const size_t T = size_t(cfg.chunk_slices);
 	const size_t nz = cfg.velocity ? size_t(cfg.nz) : 0;
 	cudaStream_t s = c->stream;
-	char* m = static_cast<char*>(pool_alloc(c, st->bytes));
-	st->mem = m;
+	if (!st->mem) st->mem = static_cast<char*>(pool_alloc(c, st->bytes));
+	char* m = st->mem;
 	auto take = [&](size_t b) {
 		char* r = m;
 		m += align256(b);
@@ -228,11 +234,33 @@ void arma_server::make_resident(StreamState* st, Ctx* c) {
 	st->resident = true;
 }
 
-void arma_server::release(StreamState* st, Ctx* c) {
-	if (st->resident && st->mem) pool_free(c, st->mem);
+void arma_server::release(StreamState* st, Ctx*) {
+	if (st->resident && st->mem) {
+		spare.emplace(st->bytes, st->mem);
+		spare_bytes += st->bytes;
+	}
 	st->mem = nullptr;
 	st->resident = false;
 	resident_bytes -= st->bytes;
+}
+
+// A block for a stream being admitted: a spare one of the same size, else
+// room is made in the budget by freeing spare blocks (the allocation itself
+// happens in launch()).
+void arma_server::reserve_block(StreamState* st, Ctx* c) {
+	auto it = spare.find(st->bytes);
+	if (it != spare.end()) {
+		st->mem = it->second;
+		spare_bytes -= it->first;
+		spare.erase(it);
+		return;
+	}
+	while (!spare.empty() && resident_bytes + spare_bytes > budget) {
+		auto big = std::prev(spare.end());
+		pool_free(c, big->second);
+		spare_bytes -= big->first;
+		spare.erase(big);
+	}
 }
 
 // Requests are taken in arrival order; a request waits while its stream has a
@@ -248,7 +276,10 @@ bool arma_server::form_and_launch(Slot& sl, std::unique_lock<std::mutex>& lk) {
 		bool ok = !st->busy && (take.empty() || points + np <= cfg.max_batch_points);
 		if (ok && !st->resident) {
 			ok = resident_bytes + st->bytes <= budget;
-			if (ok) resident_bytes += st->bytes;  // reserved; allocated in launch()
+			if (ok) {
+				resident_bytes += st->bytes;  // reserved; allocated in launch()
+				reserve_block(st, &sl.ctx->c);
+			}
 		}
 		if (!ok) {
 			++it;
@@ -291,8 +322,15 @@ bool arma_server::form_and_launch(Slot& sl, std::unique_lock<std::mutex>& lk) {
 		sl.failed = true;
 		sl.fail_code = code;
 		fatal = msg;
-		for (Request& r : sl.reqs)  // reservations that were never allocated
-			if (!r.st->resident) resident_bytes -= r.st->bytes;
+		for (Request& r : sl.reqs)  // reservations that were never made resident
+			if (!r.st->resident) {
+				resident_bytes -= r.st->bytes;
+				if (r.st->mem) {
+					spare.emplace(r.st->bytes, r.st->mem);
+					spare_bytes += r.st->bytes;
+					r.st->mem = nullptr;
+				}
+			}
 	}
 	stats.batches += 1;
 	stats.launches += nl;
@@ -303,6 +341,16 @@ bool arma_server::form_and_launch(Slot& sl, std::unique_lock<std::mutex>& lk) {
 }
 
 uint64_t arma_server::launch(Slot& sl) {
+	// host time per phase, reported on stderr for slow launches when the
+	// ARMA_SERVE_TRACE environment variable is set
+	static const bool trace = std::getenv("ARMA_SERVE_TRACE") != nullptr;
+	double ph[10] = {0};
+	auto tp = Clock::now();
+	auto mark = [&](int k) {
+		const auto now = Clock::now();
+		ph[k] = ms_between(tp, now);
+		tp = now;
+	};
 	Ctx* c = &sl.ctx->c;
 	cudaStream_t s = c->stream;
 	scratch_begin(c, 0);
@@ -313,6 +361,7 @@ uint64_t arma_server::launch(Slot& sl) {
 		if (!r.st->resident) make_resident(r.st, c);
 	const uint64_t launches0 = c->launches;
 	ARMA_CUDA_TRY(cudaEventRecord(sl.begin, s));
+	mark(0);
 	// 1. history: the previous chunk's last H slices in front of this one
 	std::vector<CopyJob> hist;
 	for (Request& r : sl.reqs) {
@@ -323,6 +372,7 @@ uint64_t arma_server::launch(Slot& sl) {
 			                       size_t(st->H) * st->n2, nullptr});
 	}
 	launch_copies(c, hist);
+	mark(1);
 	// 2. MT words: from the seed (first chunk) or from the stream's window
 	auto* d_att = static_cast<unsigned long long*>(scratch_take(c, sizeof(unsigned long long) * n));
 	auto* d_pairs = static_cast<long long*>(scratch_take(c, sizeof(long long) * n));
@@ -340,6 +390,7 @@ uint64_t arma_server::launch(Slot& sl) {
 		              sl.reqs[k].chunk > 0 ? st->window[cur] : nullptr};
 	}
 	launch_mt_generate_batch(c, mj, kStreamLog2Seg);
+	mark(2);
 	// 3. polar noise into the chunk slices, counting the attempts consumed
 	std::vector<NoiseSpec> ns(n);
 	for (size_t k = 0; k < n; ++k) {
@@ -349,6 +400,7 @@ uint64_t arma_server::launch(Slot& sl) {
 		                  st->buf[cur] + size_t(st->H) * st->n2, d_att + k};
 	}
 	enqueue_white_noise_batch(c, ns, ARMA_FP32C, d_pairs);
+	mark(3);
 	// 4. the MT window for the next chunk
 	std::vector<MtWindowSpec> ws(n);
 	for (size_t k = 0; k < n; ++k) {
@@ -357,6 +409,7 @@ uint64_t arma_server::launch(Slot& sl) {
 		ws[k] = MtWindowSpec{st->mt, mj[k].out, 4 * att[k], d_att + k, st->window[cur ^ 1], nullptr};
 	}
 	launch_mt_window_update(c, ws);
+	mark(4);
 	// 5. the AR filter of every chunk in one launch
 	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
 	std::vector<Ar32Surface> as(n);
@@ -383,6 +436,7 @@ uint64_t arma_server::launch(Slot& sl) {
 		a.tiles_y = (st->ny + ty - 1) / ty;
 	}
 	launch_ar32c(c, as, tx, ty, 0);
+	mark(5);
 	// 6. the stream's scale from its first chunk
 	std::vector<RenormSpec> rs;
 	for (Request& r : sl.reqs) {
@@ -399,6 +453,7 @@ uint64_t arma_server::launch(Slot& sl) {
 		}
 	}
 	launch_renorm_batch(c, rs, ARMA_FP32C, false);
+	mark(6);
 	// 7. velocity potentials of the chunk slices: one set of launches per
 	//    slice shape
 	if (nz > 0) {
@@ -428,6 +483,7 @@ uint64_t arma_server::launch(Slot& sl) {
 			scratch_release(c, mark);
 		}
 	}
+	mark(7);
 	// 8. outputs: scaled into the caller's device buffers or into staging
 	std::vector<CopyJob> outs;
 	for (Request& r : sl.reqs) {
@@ -451,11 +507,23 @@ uint64_t arma_server::launch(Slot& sl) {
 			ARMA_CUDA_TRY(cudaMemcpyAsync(r.vel_out, st->stage_v, sizeof(float) * nzeta * nz,
 			                              cudaMemcpyDeviceToHost, s));
 	}
+	mark(8);
 	// 9. status words back to pinned memory, then the completion event
 	ARMA_CUDA_TRY(cudaMemcpyAsync(sl.h_pairs, d_pairs, sizeof(long long) * n, cudaMemcpyDeviceToHost, s));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<int*>(sl.h_pairs + cfg.max_batch), c->d_err,
 	                              sizeof(int), cudaMemcpyDeviceToHost, s));
 	ARMA_CUDA_TRY(cudaEventRecord(sl.done, s));
+	mark(9);
+	if (trace) {
+		double tot = 0;
+		for (double v : ph) tot += v;
+		if (tot > 5.0)
+			std::fprintf(stderr,
+			             "[arma serve] slow launch %.1f ms (%zu requests): resident %.1f hist %.1f "
+			             "mt %.1f noise %.1f window %.1f ar %.1f renorm %.1f velocity %.1f out %.1f "
+			             "status %.1f\n",
+			             tot, n, ph[0], ph[1], ph[2], ph[3], ph[4], ph[5], ph[6], ph[7], ph[8], ph[9]);
+	}
 	return c->launches - launches0;
 }
 
@@ -620,6 +688,15 @@ int arma_server_create(int device, const arma_server_config* cfg, arma_server** 
 			ARMA_CUDA_TRY(cudaHostAlloc(&sl.h_pairs, sizeof(long long) * (cfg->max_batch + 1),
 			                            cudaHostAllocDefault));
 		}
+		// back the library pool with physical memory for stream state now, so
+		// that admitting a stream does not wait for the driver to map memory
+		{
+			Ctx* c0 = &srv->slots[0].ctx->c;
+			const size_t warm = std::min(srv->budget, size_t(4) << 30);
+			void* p = pool_alloc(c0, warm);
+			pool_free(c0, p);
+			ARMA_CUDA_TRY(cudaStreamSynchronize(c0->stream));
+		}
 		arma_server* raw = srv.get();
 		srv->thread = std::thread([raw] { raw->loop(); });
 		*out = srv.release();
@@ -639,6 +716,8 @@ int arma_server_destroy(arma_server* srv) {
 		cudaSetDevice(srv->device);
 		for (auto& kv : srv->streams)
 			if (kv.second->resident) srv->release(kv.second.get(), &srv->slots[0].ctx->c);
+		for (auto& kv : srv->spare) pool_free(&srv->slots[0].ctx->c, kv.second);
+		srv->spare.clear();
 		for (Slot& sl : srv->slots) {
 			if (sl.ctx) cudaStreamSynchronize(sl.ctx->c.stream);
 			if (sl.begin) cudaEventDestroy(sl.begin);

@@ -339,6 +339,15 @@ def gpu_arm(args):
                "sample": f"{len(sample)} smallest surfaces of the batch ({points(sample)} points), "
                          f"OpenMP block wavefront restatement, {t:.1f} s"}
 
+    full = None
+    if not args.skip_full:
+        full = full_path(A, capi, ctx, batch, sets, 2, stream)
+        full["value"] *= world  # every rank runs its own batch
+        full["ratio_over_plain_fp64_ar"] = (full["value"] / plain) if plain else None
+    prec = None
+    if rank == 0 and not args.skip_precision:
+        prec = precision_report(A, capi, ctx)
+
     serving = None
     if world == 1 and not args.skip_serve:
         serving = serve_bench(A, args.serve_seconds)
@@ -371,6 +380,8 @@ def gpu_arm(args):
                                  "time; peak = 148 SMs x 128 FP32 lanes x 2 x max SM clock "
                                  "(MEASURED_PEAKS.json has no FP32 figure)"},
             "cpu_baseline": cpu,
+            "full_path": full,
+            "precision_fp32c_vs_fp64": prec,
             "latency": ({"p50_ms": serving["p50_ms_at_50pct"], "p99_ms": serving["p99_ms_at_50pct"],
                          "p99_128x128x64_ms": serving["p99_128x128x64_ms_at_50pct"],
                          "load": 0.5, "source": "serving"} if serving else None),
@@ -382,6 +393,108 @@ def gpu_arm(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------- full path
+def full_path(A, capi, ctx, batch, sets, steps, stream):
+    """The batched FP32 compensated path end to end on the device: noise, AR
+    filter and renormalisation for every surface (one call), the skew-normal
+    NIT (skewness 0.3: alpha 1.499) through the 1024-node inverse-CDF table,
+    and the linear velocity potential at z = 0 on every slice of every surface
+    (infinite depth), batched by slice shape.  Returns points/s and the
+    per-stage device milliseconds of one step."""
+    import torch
+    order = sorted(range(len(batch)), key=lambda k: batch[k]["acf0"])
+    total = points(batch)
+    flat = torch.empty(total, dtype=torch.float32, device="cuda")
+    vel = torch.empty(total, dtype=torch.float32, device="cuda")
+    surfs, groups, nit_ranges, off = [], {}, {}, 0
+    for k in order:
+        s = batch[k]
+        n = int(np.prod(s["shape"]))
+        surfs.append(capi.make_surface(s["shape"], s["phi"], s["var"], s["acf0"],
+                                       sets[s["mtset"] % len(sets)], s["seed"],
+                                       flat[off:].data_ptr()))
+        lo, hi = nit_ranges.get(s["acf0"], (off, off))
+        nit_ranges[s["acf0"]] = (min(lo, off), off + n)
+        nt, nx, ny = s["shape"]
+        groups.setdefault((nx, ny), []).append(
+            (flat[off:].data_ptr(), vel[off:].data_ptr(), nt, list(range(nt)), 1.0))
+        off += n
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def step(record):
+        if record:
+            ev[0].record(stream)
+        ctx.batch_generate(surfs, A.FP32C)
+        if record:
+            ev[1].record(stream)
+        for acf0, (lo, hi) in nit_ranges.items():
+            ctx.nit_apply(A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499], float(np.sqrt(acf0)), A.NIT_LUT,
+                          hi - lo, A.FP32C, flat[lo:].data_ptr(), lut_nodes=1024, lut_range=5.0)
+        if record:
+            ev[2].record(stream)
+        for (nx, ny), jobs in groups.items():
+            ctx.velocity_linear_batch(jobs, nx, ny, A.FP32C, float("inf"), [0.0])
+        if record:
+            ev[3].record(stream)
+
+    step(False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    stage = np.zeros(3)
+    for _ in range(steps):
+        step(True)
+        torch.cuda.synchronize()
+        stage += [ev[i].elapsed_time(ev[i + 1]) for i in range(3)]
+    wall = time.perf_counter() - t0
+    dev_ms = float(stage.sum()) / steps
+    return {"value": total / (dev_ms / 1e3), "unit": "points/s", "steps": steps,
+            "ms_per_step": dev_ms, "wall_ms_per_step": wall / steps * 1e3,
+            "stage_ms": {"noise_ar_renorm": stage[0] / steps, "nit_lut": stage[1] / steps,
+                         "velocity_z0": stage[2] / steps},
+            "workload": "batched-256-surfaces + skew-normal NIT (LUT 1024 nodes) + velocity "
+                        "potential at z=0 on every slice (infinite depth)"}
+
+
+def precision_report(A, capi, ctx):
+    """FP32 compensated against FP64 on the 400 x 128 x 128 propagating model
+    of order 10^3 (zeta, variance, ACF, velocity at z in {0,-1,-2,-4}) and the
+    NIT moments of the 512 x 256 x 256 model (first 64 slices)."""
+    import torch
+    from arma_b200.precision import compare_surfaces, field_error
+    phi, var = A.ar_fit_analytic(A.ACF_PROPAGATING, (10, 10, 10), 1.0, 0.6, [0.04] * 3, [0.3, 0.2])
+    mt = A.mt19937_params()
+
+    def pair(shape):
+        z64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+        z32 = torch.empty(shape, dtype=torch.float32, device="cuda")
+        for z, prec in ((z64, A.FP64), (z32, A.FP32C)):
+            ctx.batch_generate([capi.make_surface(shape, phi, var, 1.0, mt, 42, z.data_ptr())], prec)
+        ctx.synchronize()
+        return z64, z32
+
+    z64, z32 = pair((400, 128, 128))
+    out = {"zeta_400x128x128": compare_surfaces(z64, z32)}
+    zs = [0.0, -1.0, -2.0, -4.0]
+    v64 = torch.empty((400, 4, 128, 128), dtype=torch.float64, device="cuda")
+    v32 = torch.empty((400, 4, 128, 128), dtype=torch.float32, device="cuda")
+    for z, v, prec in ((z64, v64, A.FP64), (z32, v32, A.FP32C)):
+        ctx.velocity_linear(z.data_ptr(), z.shape, prec, (1.0, 1.0, 1.0), float("inf"), zs,
+                            list(range(400)), v.data_ptr())
+    ctx.synchronize()
+    out["velocity_400x128x128_z4"] = field_error(v64, v32)
+    del z64, z32, v64, v32
+    z64, z32 = pair((512, 256, 256))
+    w64, w32 = z64[:64].contiguous(), z32[:64].contiguous()
+    del z64, z32
+    ctx.nit_apply(A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499], 1.0, A.NIT_BISECTION, w64.numel(), A.FP64,
+                  w64.data_ptr(), interval=(-10.0, 10.0), eps=1e-10, max_iter=100)
+    ctx.nit_apply(A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499], 1.0, A.NIT_LUT, w32.numel(), A.FP32C,
+                  w32.data_ptr(), lut_nodes=1024, lut_range=5.0)
+    ctx.synchronize()
+    out["nit_skew_normal_512x256x256_first64"] = compare_surfaces(w64, w32)
+    return out
 
 
 # --------------------------------------------------------------------- serving
@@ -511,6 +624,8 @@ def main():
                     help="use the first N surfaces of the batch (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-serve", action="store_true")
+    ap.add_argument("--skip-full", action="store_true")
+    ap.add_argument("--skip-precision", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=1.5,
                     help="Poisson phase length per load level")
     args = ap.parse_args()

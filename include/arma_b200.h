@@ -184,6 +184,21 @@ int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3],
                          const double* z, int nz, const int* t_idx, int ntd,
                          void* d_phi_out);
 
+/* Many surfaces of one slice shape nx x ny in one set of launches (no
+ * counterpart in the reference): job k reads nt slices at d_zeta and writes
+ * its slices t_idx[0..ntd) to d_out as (ntd, nz, nx, ny); dt is its time step
+ * (<= 0: 1). */
+typedef struct {
+	const void* d_zeta;
+	void* d_out;
+	int nt;
+	const int* t_idx;
+	int ntd;
+	double dt;
+} arma_velocity_job;
+int arma_velocity_linear_batch(arma_ctx* ctx, const arma_velocity_job* jobs, int n, int nx,
+                               int ny, int precision, double depth, const double* z, int nz);
+
 /* ------------------------------------------------ batched generation */
 /* One surface of a batch.  phi/var_wn come from a fit; the noise stream is
  * (mt, seed); zeta is a device buffer of shape[0]*shape[1]*shape[2] elements

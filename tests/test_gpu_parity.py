@@ -294,3 +294,27 @@ def test_white_noise_long_stream(ctx):
     ctx.white_noise(A.mt19937_params(), 77, 1.3, n, A.FP64, out.data_ptr())
     ctx.synchronize()
     assert_noise_close(out.cpu().numpy(), ref)
+
+
+def test_velocity_batch_equals_single_calls(ctx):
+    """The batched velocity entry point (several surfaces of one slice shape,
+    different lengths and slice lists) gives exactly the per-surface results,
+    in FP32 (fused kernel) and FP64 (FFT passes through global memory)."""
+    phi, var = A.ar_fit_analytic(A.ACF_STANDING, (4, 4, 4), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    specs = [((10, 32, 64), [0, 3, 9]), ((6, 32, 64), [5, 1]), ((3, 32, 64), [2])]
+    for prec, dt in [(A.FP32C, torch.float32), (A.FP64, torch.float64)]:
+        zs, outs, jobs = [], [], []
+        for k, (shape, tidx) in enumerate(specs):
+            eps = O.white_noise(O.mt19937_params(), 7 + k, np.sqrt(var), int(np.prod(shape)))
+            z = dev(O.ar_filter(eps.reshape(shape), phi), dt)
+            o = torch.zeros((len(tidx), 2) + shape[1:], dtype=dt, device="cuda")
+            zs.append(z)
+            outs.append(o)
+            jobs.append((z.data_ptr(), o.data_ptr(), shape[0], tidx, 1.0))
+        ctx.velocity_linear_batch(jobs, 32, 64, prec, 12.0, [0.0, -2.0])
+        for (shape, tidx), z, o in zip(specs, zs, outs):
+            ref = torch.zeros_like(o)
+            ctx.velocity_linear(z.data_ptr(), shape, prec, (1.0, 1.0, 1.0), 12.0, [0.0, -2.0], tidx,
+                                ref.data_ptr())
+            ctx.synchronize()
+            assert torch.equal(o, ref)

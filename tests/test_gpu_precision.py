@@ -1,0 +1,77 @@
+"""FP32 compensated path against the FP64 GPU path at the full sizes of the
+propagating-wave configurations.
+
+  * 400 x 128 x 128, order 10^3 (propagating a=1, b=0.04, c=0.6, d=0.3,
+    e=0.2): zeta RMS error <= 1e-5 relative to the FP64 surface; variance and
+    ACF (lags {0,1,2}^3) within 0.1 %; velocity potentials at z in
+    {0, -1, -2, -4}, infinite depth, on every slice: RMS error <= 1e-4 and
+    max-abs error <= 2e-4 of max |phi|.
+  * 512 x 256 x 256, same model, with the NIT (skew-normal with skewness 0.3,
+    i.e. alpha = 1.499, and Gram-Charlier with skewness 0.3, kurtosis 3.2):
+    the FP32 surface through the 1024-node inverse-CDF table over +-5 sigma
+    against the FP64 surface through the FP64 bisection (tolerance 1e-10) --
+    variance, skewness and ACF within 0.1 %.  The bisection oracle runs on the
+    first 64 slices (4.2 M points); the statistics compare that window.
+"""
+import numpy as np
+import pytest
+
+import arma_b200 as A
+from arma_b200 import capi
+from arma_b200.precision import compare_surfaces, field_error
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+PROP = dict(kind=A.ACF_PROPAGATING, amplitude=1.0, velocity=0.6, alpha=[0.04] * 3,
+            beta=[0.3, 0.2])
+
+
+def surfaces(ctx, shape, order, seed=42):
+    phi, var = A.ar_fit_analytic(PROP["kind"], order, PROP["amplitude"], PROP["velocity"],
+                                 PROP["alpha"], PROP["beta"])
+    mt = A.mt19937_params()
+    z64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+    z32 = torch.empty(shape, dtype=torch.float32, device="cuda")
+    for z, prec in ((z64, A.FP64), (z32, A.FP32C)):
+        s = capi.make_surface(shape, phi, var, 1.0, mt, seed, z.data_ptr())
+        ctx.batch_generate([s], prec)
+    ctx.synchronize()
+    return z64, z32
+
+
+def test_propagating_400x128x128_order10(ctx):
+    z64, z32 = surfaces(ctx, (400, 128, 128), (10, 10, 10))
+    st = compare_surfaces(z64, z32)
+    assert st["rms_rel"] <= 1e-5, st
+    assert st["variance_rel"] <= 1e-3 and st["acf_rel_max"] <= 1e-3, st
+    zs, tidx = [0.0, -1.0, -2.0, -4.0], list(range(400))
+    v64 = torch.empty((400, 4, 128, 128), dtype=torch.float64, device="cuda")
+    v32 = torch.empty((400, 4, 128, 128), dtype=torch.float32, device="cuda")
+    ctx.velocity_linear(z64.data_ptr(), z64.shape, A.FP64, (1.0, 1.0, 1.0), float("inf"), zs,
+                        tidx, v64.data_ptr())
+    ctx.velocity_linear(z32.data_ptr(), z32.shape, A.FP32C, (1.0, 1.0, 1.0), float("inf"), zs,
+                        tidx, v32.data_ptr())
+    ctx.synchronize()
+    ve = field_error(v64, v32)
+    assert ve["rms_rel"] <= 1e-4 and ve["max_abs"] <= 2e-4 * ve["max_ref"], ve
+
+
+@pytest.mark.parametrize("dist,params", [
+    (A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499]),
+    (A.NIT_GRAM_CHARLIER, [0.3, 3.2]),
+])
+def test_propagating_512x256x256_nit_moments(ctx, dist, params):
+    z64, z32 = surfaces(ctx, (512, 256, 256), (10, 10, 10))
+    w64 = z64[:64].contiguous()
+    w32 = z32[:64].contiguous()
+    del z64, z32
+    ctx.nit_apply(dist, params, 1.0, A.NIT_BISECTION, w64.numel(), A.FP64, w64.data_ptr(),
+                  interval=(-10.0, 10.0), eps=1e-10, max_iter=100)
+    ctx.nit_apply(dist, params, 1.0, A.NIT_LUT, w32.numel(), A.FP32C, w32.data_ptr(),
+                  lut_nodes=1024, lut_range=5.0)
+    ctx.synchronize()
+    st = compare_surfaces(w64, w32)
+    assert st["variance_rel"] <= 1e-3, st
+    assert st["skewness_rel"] <= 1e-3, st
+    assert st["acf_rel_max"] <= 1e-3, st
