@@ -214,6 +214,8 @@ struct VelocitySurface {
 };
 void launch_velocity_linear_batch(Ctx* c, const VelocitySurface* v, int n, int nx, int ny,
                                   int precision, double depth, const double* z, int nz);
+// Slice shapes the solver's FFTs take: sides in [4, 1024], prime factors <= 64.
+bool velocity_supported(int nx, int ny);
 
 // Host math shared by the ABI (fit.cc).
 int fit_gauss_table(const double* acf, const int acf_shape[3], const int order[3],

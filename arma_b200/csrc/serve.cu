@@ -744,11 +744,9 @@ int arma_stream_open(arma_server* srv, const arma_stream_spec* spec, uint64_t* s
 		             "variance is less than zero");
 		ARMA_REQUIRE((long long)srv->cfg.chunk_slices * spec->nx * spec->ny % 2 == 0, ARMA_EINVAL,
 		             "chunk point count must be even");
-		if (srv->cfg.velocity) {
-			auto pow2 = [](int v) { return v >= 4 && v <= 1024 && (v & (v - 1)) == 0; };
-			ARMA_REQUIRE(pow2(spec->nx) && pow2(spec->ny), ARMA_ENOTSUP,
-			             "velocity solver: slice sides must be powers of two in [4, 1024]");
-		}
+		if (srv->cfg.velocity)
+			ARMA_REQUIRE(velocity_supported(spec->nx, spec->ny), ARMA_ENOTSUP,
+			             "velocity solver: slice sides must be in [4, 1024] with prime factors <= 64");
 		std::unique_ptr<StreamState> st(new StreamState());
 		st->nx = spec->nx;
 		st->ny = spec->ny;

@@ -11,25 +11,26 @@
 // The work is a list of slices (surface pointer, its length, slice index,
 // time step, output pointer), so one set of launches serves any number of
 // surfaces of one slice shape:
-//   1. factor_waves_kernel one CTA per (slice, axis), streaming: extrema
-//                          events of a tile of positions are compacted in
-//                          loop order with a block scan, then warp 0 walks
-//                          them 32 at a time with ballots and a segmented
-//                          first-maximum scan, carrying the open sign run
-//                          across tiles; min/max k over consecutive closed
-//                          runs give wnmax.  No per-event global memory.
+//   1. factor_waves_kernel one CTA per (slice, axis): the positions are cut
+//                          into one segment per warp; each warp compacts the
+//                          extrema events of 32 positions at a time with a
+//                          ballot and walks them with a segmented first-
+//                          maximum scan, summarising its segment; warp 0
+//                          merges the summaries in order.  No per-event
+//                          global memory.
 //   2a. FP32, nx*ny <= 16384: velocity_fused_kernel, one CTA per slice:
-//                          zeta_t into shared memory, in-place radix-2 FFT2
-//                          (decimation in frequency: natural in, bit-reversed
-//                          out), the spectrum kept in registers, and per depth
-//                          the window product in the bit-reversed domain, the
-//                          inverse FFT2 (decimation in time: bit-reversed in,
-//                          natural out), Re / N and the edge extrapolation,
-//                          stored once.
-//   2b. otherwise (FP64, larger slices), in passes of bounded scratch:
-//                          deriv_kernel -> batched Stockham FFTs through
-//                          global memory (rows, then columns) ->
-//                          window_mul_kernel -> inverse FFTs -> finish_kernel.
+//                          zeta_t into shared memory, in-place mixed-radix
+//                          FFT2 (decimation in frequency: natural in, digit-
+//                          reversed out), and per depth the window product in
+//                          the digit-reversed domain, the inverse FFT2
+//                          (decimation in time: digit-reversed in, natural
+//                          out), Re / N and the edge extrapolation, stored
+//                          once.
+//   2b. otherwise (FP64, larger slices), in passes of bounded scratch: the
+//                          same radix-2 FFTs on bands of rows and columns
+//                          held in shared memory, spectra through global
+//                          memory between three launches (vel_rows_fwd,
+//                          vel_cols with the window, vel_rows_inv).
 // The window is always evaluated in FP64 with the reference's edge fixes and
 // blitz::rotate permutation.
 #include <algorithm>
@@ -50,13 +51,6 @@ template <class T> struct C2;
 template <> struct C2<float> { using type = float2; };
 template <> struct C2<double> { using type = double2; };
 
-template <class V>
-__device__ __forceinline__ V cmul(V a, V b) {
-	V r;
-	r.x = a.x * b.x - a.y * b.y;
-	r.y = a.x * b.y + a.y * b.x;
-	return r;
-}
 
 // One slice of the work list.
 template <class T>
@@ -89,58 +83,39 @@ __device__ __forceinline__ double zeta_t(const VelSlice<T>& s, long long n2, lon
 	return -r;
 }
 
-template <class T>
-__global__ void deriv_kernel(const VelSlice<T>* __restrict__ sl, int ns, int nx, int ny,
-                             typename C2<T>::type* __restrict__ a) {
-	const long long n2 = (long long)nx * ny;
-	const long long total = n2 * ns;
-	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-	     q += (long long)gridDim.x * blockDim.x) {
-		typename C2<T>::type v;
-		v.x = T(zeta_t(sl[q / n2], n2, q % n2));
-		v.y = T(0);
-		a[q] = v;
-	}
-}
-
 // ---------------------------------------------------------------- 2. wnmax
-constexpr int kFwThreads = 256;
+// factor_waves walks the extrema events of one axis in loop order, splits
+// them into maximal same-sign runs, takes each run's first event of largest
+// |elevation| as its representative, and forms k = (2 pi / |2 (p_r -
+// p_{r-1})|)^2 / g for every run r >= 1 that closes (the last run never
+// closes); wnmax comes from the smallest k.
+//
+// On the device one CTA of kFwWarps warps handles one (slice, axis): the
+// positions are cut into kFwWarps contiguous segments, each warp walks its
+// segment 32 positions at a time (ballot compaction of the events, a
+// segmented first-maximum scan over the runs) and summarises it; warp 0 then
+// merges the summaries in order.  A segment's first run may continue the
+// previous segment's last run, so pairs that involve its first run are
+// completed during the merge.
+constexpr int kFwWarps = 8;
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ int block_scan_excl(int v, int* total, int* sh) {
-	// sh: kFwThreads/32 ints
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	int incl = v;
-	for (int o = 1; o < 32; o <<= 1) {
-		const int t = __shfl_up_sync(kFull, incl, o);
-		if (lane >= o) incl += t;
-	}
-	if (lane == 31) sh[warp] = incl;
-	__syncthreads();
-	if (warp == 0) {
-		int s = lane < kFwThreads / 32 ? sh[lane] : 0;
-		for (int o = 1; o < 32; o <<= 1) {
-			const int t = __shfl_up_sync(kFull, s, o);
-			if (lane >= o) s += t;
-		}
-		if (lane < kFwThreads / 32) sh[lane] = s;
-	}
-	__syncthreads();
-	const int base = warp ? sh[warp - 1] : 0;
-	*total = sh[kFwThreads / 32 - 1];
-	__syncthreads();
-	return base + incl - v;
-}
+struct Run {
+	int sign;       // elevation > 0
+	double best_e;  // |elevation| of the first maximum
+	double best_p;  // its period
+};
 
-// The open sign run carried from one group of events to the next (warp 0).
-struct RunState {
-	bool open = false;     // a run has started
-	int sign = 0;          // elevation > 0 of the open run
-	double best_e = 0.0;   // |elevation| of the open run's first maximum
-	double best_p = 0.0;   // its period
-	double prev_p = 0.0;   // first-maximum period of the run before it
-	int index = -1;        // index of the open run
-	double mn = DBL_MAX, mx = DBL_MIN;
+// Walk state of one segment (uniform over the warp).  Local run indices
+// start at 0 with the segment's first run.
+struct SegWalk {
+	int m = 0;              // runs started so far
+	Run open{0, 0.0, 0.0};  // run m-1
+	double prev_p = 0.0;    // representative period of run m-2
+	Run r0{0, 0.0, 0.0};    // run 0 once closed
+	double r1_p = 0.0;      // run 1 once closed
+	double mn = DBL_MAX, mx = DBL_MIN;  // pairs (r-1, r) with r >= 2, closed (per lane
+	                                    // until the warp reduces them)
 };
 
 __device__ __forceinline__ void pair_k(double p0, double p1, double& mn, double& mx) {
@@ -150,25 +125,20 @@ __device__ __forceinline__ void pair_k(double p0, double p1, double& mn, double&
 	if (k > mx) mx = k;
 }
 
-// Events e[0..g) (g <= 32, in loop order) continue the sequence of runs.
-// Runs are maximal same-sign stretches; each run's representative is its
-// first event of largest |elevation|; every run that closes with index >= 1
-// pairs with the run before it (the last run never closes), exactly as the
-// reference walks the events one by one.
-__device__ void walk_group(const double* ev_p, const double* ev_e, int g, RunState& st) {
+// The first g lanes hold consecutive events (e: elevation, p: period).
+__device__ void walk_events(double e, double p, int g, SegWalk& st) {
 	const int lane = threadIdx.x & 31;
 	const bool valid = lane < g;
-	const double e = valid ? ev_e[lane] : 0.0;
-	const double p = valid ? ev_p[lane] : 0.0;
 	const int s = e > 0.0 ? 1 : 0;
 	const int sprev = __shfl_up_sync(kFull, s, 1);
-	bool b = lane == 0 ? (!st.open || s != st.sign) : (s != sprev);
+	const bool open = st.m > 0;
+	bool b = lane == 0 ? (!open || s != st.open.sign) : (s != sprev);
 	b = b && valid;
 	const unsigned B = __ballot_sync(kFull, b);
 	const unsigned upto = B & (lane == 31 ? kFull : ((2u << lane) - 1u));
 	const int start = upto ? 31 - __clz(upto) : 0;  // first lane of this lane's run
 	// segmented inclusive scan: first maximum of |elevation| within the run
-	double bv = fabs(e), bp = p;
+	double bv = valid ? fabs(e) : 0.0, bp = p;
 	for (int o = 1; o < 32; o <<= 1) {
 		const double ov = __shfl_up_sync(kFull, bv, o);
 		const double op = __shfl_up_sync(kFull, bp, o);
@@ -178,46 +148,96 @@ __device__ void walk_group(const double* ev_p, const double* ev_e, int g, RunSta
 		}
 	}
 	const bool lead = (B & 1u) != 0;  // lane 0 starts a new run
-	if (st.open && !lead && upto == 0 && !(bv > st.best_e)) {
-		bv = st.best_e;  // the carried run continues: it came first
-		bp = st.best_p;
+	if (open && !lead && upto == 0 && !(bv > st.open.best_e)) {
+		bv = st.open.best_e;  // the open run continues: it came first
+		bp = st.open.best_p;
 	}
-	const int first_index = lead ? (st.open ? st.index + 1 : 0) : st.index;
+	const int first_index = lead ? st.m : st.m - 1;
 	const int run = first_index + __popc(upto & ~1u);
-	// the previous run's representative for this lane's run
 	const double before = __shfl_sync(kFull, bp, start > 0 ? start - 1 : 0);
-	const double prev = start > 0 ? before : (lead ? st.best_p : st.prev_p);
-	// runs that close inside the group: the carried one (if a new run starts
-	// at lane 0) and every run followed by a boundary
-	if (lane == 0 && st.open && lead && st.index >= 1) pair_k(st.prev_p, st.best_p, st.mn, st.mx);
+	const double prev = start > 0 ? before : (lead ? st.open.best_p : st.prev_p);
+	// runs closing here: the open one (a new run starts at lane 0) and every
+	// run followed by a boundary inside the group
 	const bool closes = valid && lane + 1 < g && ((B >> (lane + 1)) & 1u);
-	if (closes && run >= 1) pair_k(prev, bp, st.mn, st.mx);
+	if (open && lead) {
+		const int r = st.m - 1;
+		if (r == 0) st.r0 = st.open;
+		else if (r == 1) st.r1_p = st.open.best_p;
+		else if (lane == 0) pair_k(st.prev_p, st.open.best_p, st.mn, st.mx);
+	}
+	if (closes && run >= 2) pair_k(prev, bp, st.mn, st.mx);
+	const unsigned c0 = __ballot_sync(kFull, closes && run == 0);
+	if (c0) {
+		const int src = __ffs(c0) - 1;
+		st.r0.sign = __shfl_sync(kFull, s, src);
+		st.r0.best_e = __shfl_sync(kFull, bv, src);
+		st.r0.best_p = __shfl_sync(kFull, bp, src);
+	}
+	const unsigned c1 = __ballot_sync(kFull, closes && run == 1);
+	if (c1) st.r1_p = __shfl_sync(kFull, bp, __ffs(c1) - 1);
 	// the run open after the group
 	const int last = g - 1;
-	const double nbv = __shfl_sync(kFull, bv, last);
-	const double nbp = __shfl_sync(kFull, bp, last);
 	const int lstart = __shfl_sync(kFull, start, last);
-	const int lsign = __shfl_sync(kFull, s, last);
-	const int lrun = __shfl_sync(kFull, run, last);
 	const double lbefore = __shfl_sync(kFull, bp, lstart > 0 ? lstart - 1 : 0);
-	st.prev_p = lstart > 0 ? lbefore : (lead ? st.best_p : st.prev_p);
-	st.open = true;
-	st.sign = lsign;
-	st.best_e = nbv;
-	st.best_p = nbp;
-	st.index = lrun;
+	st.prev_p = lstart > 0 ? lbefore : (lead ? st.open.best_p : st.prev_p);
+	st.open.sign = __shfl_sync(kFull, s, last);
+	st.open.best_e = __shfl_sync(kFull, bv, last);
+	st.open.best_p = __shfl_sync(kFull, bp, last);
+	st.m = __shfl_sync(kFull, run, last) + 1;
+}
+
+// The global walk, continued by one segment summary (lane-uniform).
+struct GlobalWalk {
+	bool open = false;
+	Run cur{0, 0.0, 0.0};
+	double prev_p = 0.0;
+	int index = -1;
+	double mn = DBL_MAX, mx = DBL_MIN;
+};
+
+__device__ void merge_segment(GlobalWalk& G, const SegWalk& S) {
+	if (S.m == 0) return;
+	if (S.mn < G.mn) G.mn = S.mn;
+	if (S.mx > G.mx) G.mx = S.mx;
+	const Run r0 = S.m == 1 ? S.open : S.r0;
+	Run merged;
+	int idx0;
+	double prev0;
+	if (G.open && r0.sign == G.cur.sign) {  // the open run continues
+		merged = r0.best_e > G.cur.best_e ? r0 : G.cur;
+		merged.sign = G.cur.sign;
+		idx0 = G.index;
+		prev0 = G.prev_p;
+	} else {
+		if (G.open && G.index >= 1) pair_k(G.prev_p, G.cur.best_p, G.mn, G.mx);
+		merged = r0;
+		idx0 = G.open ? G.index + 1 : 0;
+		prev0 = G.cur.best_p;
+	}
+	if (S.m == 1) {
+		G.open = true;
+		G.cur = merged;
+		G.prev_p = prev0;
+		G.index = idx0;
+		return;
+	}
+	if (idx0 >= 1) pair_k(prev0, merged.best_p, G.mn, G.mx);
+	if (S.m >= 3) pair_k(merged.best_p, S.r1_p, G.mn, G.mx);
+	G.open = true;
+	G.cur = S.open;
+	G.prev_p = S.m == 2 ? merged.best_p : S.prev_p;
+	G.index = idx0 + S.m - 1;
 }
 
 // One CTA per (slice, axis).  axis 0 loops y outer, x inner over z(x,y);
 // axis 1 (the reference's transposed call) x outer, y inner.  Writes min_k,
 // max_k of the axis.
 template <class T>
-__global__ void __launch_bounds__(kFwThreads)
+__global__ void __launch_bounds__(kFwWarps * 32)
 factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* __restrict__ kout) {
-	__shared__ int sh[kFwThreads / 32];
-	__shared__ double s_p[kFwThreads], s_e[kFwThreads];
-	__shared__ int s_m;
+	__shared__ SegWalk seg[kFwWarps];
 	const int slice = blockIdx.x >> 1, axis = blockIdx.x & 1;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const VelSlice<T> S = sl[slice];
 	const long long n2 = (long long)nx * ny;
 	const T* z = S.zeta + S.d * n2;
@@ -229,12 +249,14 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 	auto at = [&](int a, int b) -> double {  // a: inner index, b: outer index
 		return axis == 0 ? double(z[(long long)a * ny + b]) : double(z[(long long)b * ny + a]);
 	};
-	RunState st;
-	for (long long base = 0; base < L; base += kFwThreads) {
-		const long long q = base + threadIdx.x;
+	const long long per = (L + kFwWarps - 1) / kFwWarps;
+	const long long q0 = min(L, warp * per), q1 = min(L, q0 + per);
+	SegWalk st;
+	for (long long base = q0; base < q1; base += 32) {
+		const long long q = base + lane;
 		int flag = 0;
 		double period = 0.0, elevation = 0.0;
-		if (q < L) {
+		if (q < q1) {
 			const int b = int(q / inner), a = int(q % inner) + 1;
 			const double z0 = at(a, b), z1 = at(a - 1, b), z2 = at(a + 1, b);
 			const double dw1 = z0 - z1, dw2 = z0 - z2;
@@ -248,97 +270,26 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 				flag = 1;
 			}
 		}
-		int tot;
-		const int off = block_scan_excl(flag, &tot, sh);
-		if (flag) {
-			s_p[off] = period;
-			s_e[off] = elevation;
-		}
-		if (threadIdx.x == 0) s_m = tot;
-		__syncthreads();
-		if (threadIdx.x < 32) {
-			const int m = s_m;
-			for (int g0 = 0; g0 < m; g0 += 32) walk_group(s_p + g0, s_e + g0, min(32, m - g0), st);
-		}
-		__syncthreads();
+		const unsigned mask = __ballot_sync(kFull, flag);
+		if (!mask) continue;
+		const int g = __popc(mask);
+		const int src = lane < g ? int(__fns(mask, 0, lane + 1)) : 0;
+		const double e = __shfl_sync(kFull, elevation, src);
+		const double pp = __shfl_sync(kFull, period, src);
+		walk_events(e, pp, g, st);
 	}
-	if (threadIdx.x < 32) {
-		double mn = st.mn, mx = st.mx;
-		for (int o = 16; o > 0; o >>= 1) {
-			mn = fmin(mn, __shfl_down_sync(kFull, mn, o));
-			mx = fmax(mx, __shfl_down_sync(kFull, mx, o));
-		}
-		if (threadIdx.x == 0) {
-			kout[slice * 4 + axis] = mn;      // min_k for this axis
-			kout[slice * 4 + 2 + axis] = mx;  // max_k
-		}
+	// pairs were accumulated by the lanes that closed them
+	for (int o = 16; o > 0; o >>= 1) {
+		st.mn = fmin(st.mn, __shfl_down_sync(kFull, st.mn, o));
+		st.mx = fmax(st.mx, __shfl_down_sync(kFull, st.mx, o));
 	}
-}
-
-// ---------------------------------------------------------------- 3/5. FFT
-// Batched radix-2 Stockham FFT along lines of length n (power of two, <= 1024)
-// held in shared memory.  Line l, element k lives at data[line_off(l) +
-// k * estride]; a CTA transforms `lines` consecutive line indices whose first
-// element is at base + l * lstride within a group of `group` lines, and groups
-// are `gstride` apart.
-template <class T>
-__global__ void fft_lines_kernel(typename C2<T>::type* __restrict__ data, int n, int log2n,
-                                 long long nlines, int group, long long lstride,
-                                 long long gstride, long long estride, int lines, int sign) {
-	using V = typename C2<T>::type;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	V* buf0 = reinterpret_cast<V*>(smem_raw);
-	V* buf1 = buf0 + (size_t)lines * n;
-	V* tw = buf1 + (size_t)lines * n;  // n/2 twiddles
-	for (int k = threadIdx.x; k < n / 2; k += blockDim.x) {
-		double s, c;
-		sincospi(2.0 * k / n, &s, &c);
-		V w;
-		w.x = T(c);
-		w.y = T(sign * s);
-		tw[k] = w;
-	}
-	const long long l0 = (long long)blockIdx.x * lines;
-	auto addr = [&](long long l, int k) -> long long {
-		const long long g = l / group, r = l % group;
-		return g * gstride + r * lstride + (long long)k * estride;
-	};
-	// load: consecutive threads take consecutive lines first when lines are
-	// adjacent in memory (column FFTs), else consecutive elements
-	const int tot = lines * n;
-	for (int q = threadIdx.x; q < tot; q += blockDim.x) {
-		int li, k;
-		if (lstride == 1) { li = q % lines; k = q / lines; } else { li = q / n; k = q % n; }
-		const long long l = l0 + li;
-		if (l < nlines) buf0[li * n + k] = data[addr(l, k)];
-	}
+	if (lane == 0) seg[warp] = st;
 	__syncthreads();
-	V* in = buf0;
-	V* out = buf1;
-	const int half = n / 2;
-	for (int s = 0; s < log2n; ++s) {
-		const int Ns = 1 << s;
-		for (int q = threadIdx.x; q < lines * half; q += blockDim.x) {
-			const int li = q / half, j = q % half;
-			const int k = j & (Ns - 1);
-			const V a = in[li * n + j];
-			V b = in[li * n + j + half];
-			b = cmul(b, tw[k * (half / Ns)]);  // exp(sign 2 pi i k / (2 Ns))
-			const int o = ((j >> s) << (s + 1)) + k;
-			V u, v;
-			u.x = a.x + b.x; u.y = a.y + b.y;
-			v.x = a.x - b.x; v.y = a.y - b.y;
-			out[li * n + o] = u;
-			out[li * n + o + Ns] = v;
-		}
-		__syncthreads();
-		V* tmp = in; in = out; out = tmp;
-	}
-	for (int q = threadIdx.x; q < tot; q += blockDim.x) {
-		int li, k;
-		if (lstride == 1) { li = q % lines; k = q / lines; } else { li = q / n; k = q % n; }
-		const long long l = l0 + li;
-		if (l < nlines) data[addr(l, k)] = in[li * n + k];
+	if (threadIdx.x == 0) {
+		GlobalWalk G;
+		for (int w = 0; w < kFwWarps; ++w) merge_segment(G, seg[w]);
+		kout[slice * 4 + axis] = G.mn;      // min_k for this axis
+		kout[slice * 4 + 2 + axis] = G.mx;  // max_k
 	}
 }
 
@@ -408,31 +359,6 @@ __device__ double window_fixed(int i, int j, int nx, int ny, double dkx, double 
 	return isfinite(r) ? r : 0.0;
 }
 
-template <class T>
-__global__ void window_mul_kernel(const typename C2<T>::type* __restrict__ a, int nx, int ny,
-                                  int ntd, const double* __restrict__ kinfo,
-                                  const double* __restrict__ zs, int nz, double depth,
-                                  typename C2<T>::type* __restrict__ b) {
-	const long long n2 = (long long)nx * ny;
-	const long long total = n2 * ntd * nz;
-	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-	     q += (long long)gridDim.x * blockDim.x) {
-		const long long p = q % n2;
-		const long long iz = q / n2;
-		const int j = int(iz % nz), i = int(iz / nz);
-		const int x = int(p / ny), y = int(p % ny);
-		// wnmax = 1 / min_k per axis; grid step ub / (n-1)
-		const double wx = 1.0 / kinfo[i * 4 + 0], wy = 1.0 / kinfo[i * 4 + 1];
-		const double dkx = wx / max(nx - 1, 1), dky = wy / max(ny - 1, 1);
-		const double w = window_fixed(rotate_src(x, nx), rotate_src(y, ny), nx, ny, dkx, dky,
-		                              zs[j], depth);
-		typename C2<T>::type v = a[i * n2 + p];
-		v.x = T(v.x * w);
-		v.y = T(v.y * w);
-		b[q] = v;
-	}
-}
-
 // ---------------------------------------------------------------- 6. finish
 // Re / N with the reference's edge extrapolation (src/velocity/basic_solver.cc:
 // 62-68): column 0 (rows >= 1) from columns 1-2, then row 0 from rows 1-2
@@ -453,129 +379,213 @@ __device__ __forceinline__ double finish_at(int x, int y, int nx, int ny, F f) {
 	return f(x, y);
 }
 
-template <class T>
-__global__ void finish_kernel(const typename C2<T>::type* __restrict__ b, int nx, int ny,
-                              long long narr, int nz, const VelSlice<T>* __restrict__ sl) {
-	const long long n2 = (long long)nx * ny;
-	const double inv = 1.0 / double(n2);
-	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < narr * n2;
-	     q += (long long)gridDim.x * blockDim.x) {
-		const long long arr = q / n2, p = q % n2;
-		const int x = int(p / ny), y = int(p % ny);
-		const typename C2<T>::type* s = b + arr * n2;
-		auto f = [&](int a, int c) -> double { return double(s[(long long)a * ny + c].x) * inv; };
-		sl[arr / nz].out[(arr % nz) * n2 + p] = T(finish_at(x, y, nx, ny, f));
-	}
-}
-
 // ---------------------------------------------------------------- 2a. fused
 constexpr int kFuseThreads = 512;
 constexpr int kFuseMax = 16384;  // largest nx*ny of the fused path (128 KB of float2)
 
-__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
-	return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+__device__ __forceinline__ float2 cpx(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ double2 cpx(double x, double y) { return make_double2(x, y); }
+template <class V>
+__device__ __forceinline__ V c_add(V a, V b) { return cpx(a.x + b.x, a.y + b.y); }
+template <class V>
+__device__ __forceinline__ V c_sub(V a, V b) { return cpx(a.x - b.x, a.y - b.y); }
+template <class V>
+__device__ __forceinline__ V c_mul(V a, V b) {
+	return cpx(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+template <class V>
+__device__ __forceinline__ V c_conj(V a) { return cpx(a.x, -a.y); }
 
-// In-place radix-2 FFTs of every row (len ny, stride 1) or every column (len
-// nx, stride ny) of the nx x ny array in shared memory.  tw[k] =
-// exp(-2 pi i k / n), k < n/2.  Forward: decimation in frequency (natural in,
-// bit-reversed out); inverse: decimation in time with conjugate twiddles
-// (bit-reversed in, natural out).  Unnormalised both ways.
-__device__ void fft_rows_dif(float2* a, int nx, int ny, const float2* tw) {
-	const int half = ny / 2;
-	for (int h = half; h >= 1; h >>= 1) {
-		const int tstep = half / h;
-		for (int q = threadIdx.x; q < nx * half; q += blockDim.x) {
-			const int r = q / half, m = q % half;
-			const int j = m & (h - 1);
-			const int i0 = r * ny + ((m - j) << 1) + j;
-			const float2 u = a[i0], v = a[i0 + h];
-			a[i0] = c_add(u, v);
-			a[i0 + h] = c_mul(c_sub(u, v), tw[j * tstep]);
+// ---------------------------------------------------------------- FFT
+// In-place mixed-radix FFTs of lines held in shared memory (any length <=
+// 1024 whose prime factors are <= kMaxRadix; GSL's mixed-radix transform in
+// the reference takes any length).  A plan lists the radices of the forward
+// stages.  Forward: decimation in frequency -- stage s splits each block of
+// L_s points into r_s interleaved sub-blocks of h_s = L_s / r_s, applies the
+// r_s-point DFT across them and the twiddles W_{L_s}^{q j}; the output is in
+// digit-reversed order (position sum q_s h_s holds frequency sum q_s
+// r_0...r_{s-1}).  Inverse: the mirror stages in reverse order (conjugate
+// twiddles, then the conjugate r_s-point DFT), digit-reversed in, natural out.
+// Unnormalised both ways.  tw[k] = exp(-2 pi i k / n), k < n, from FP64
+// sincospi.
+constexpr int kMaxStages = 12;
+constexpr int kMaxRadix = 64;
+
+struct FftPlan {
+	int n, m;
+	int r[kMaxStages];
+};
+
+template <class V>
+__device__ void make_twiddles(V* tw, int n) {
+	for (int k = threadIdx.x; k < n; k += blockDim.x) {
+		double sn, cs;
+		sincospi(2.0 * k / n, &sn, &cs);
+		tw[k] = cpx(decltype(tw[0].x)(cs), decltype(tw[0].x)(-sn));
+	}
+}
+
+// Frequency held at position p after the forward stages.
+__device__ __forceinline__ int plan_freq(const FftPlan& P, int p) {
+	int h = P.n, w = 1, f = 0;
+	for (int s = 0; s < P.m; ++s) {
+		h /= P.r[s];
+		f += ((p / h) % P.r[s]) * w;
+		w *= P.r[s];
+	}
+	return f;
+}
+
+// R-point DFT of v[0..R) in place: forward roots exp(-2 pi i t / R) (= tw[t
+// n/R], rs = n/R), conjugated for the inverse.  Fixed R: registers.
+template <class V, bool INV, int R>
+__device__ __forceinline__ void dft_fixed(V* v, int rs, const V* tw) {
+	using T = decltype(v[0].x);
+	if constexpr (R == 2) {
+		const V a = v[0], b = v[1];
+		v[0] = c_add(a, b);
+		v[1] = c_sub(a, b);
+	} else if constexpr (R == 4) {
+		const V t0 = c_add(v[0], v[2]), t1 = c_sub(v[0], v[2]);
+		const V t2 = c_add(v[1], v[3]);
+		const V d = c_sub(v[1], v[3]);
+		const V t3 = INV ? cpx(-d.y, d.x) : cpx(d.y, -d.x);  // (+-i) d
+		v[0] = c_add(t0, t2);
+		v[1] = c_add(t1, t3);
+		v[2] = c_sub(t0, t2);
+		v[3] = c_sub(t1, t3);
+	} else if constexpr (R == 3) {
+		const T c = T(-0.5), sn = INV ? T(0.86602540378443864676) : T(-0.86602540378443864676);
+		const V t1 = c_add(v[1], v[2]), t2 = c_sub(v[1], v[2]);
+		const V m = cpx(v[0].x + c * t1.x, v[0].y + c * t1.y);
+		const V it = cpx(-sn * t2.y, sn * t2.x);  // i sn t2
+		v[0] = c_add(v[0], t1);
+		v[1] = c_add(m, it);
+		v[2] = c_sub(m, it);
+	} else {
+		V y[R];
+#pragma unroll
+		for (int q = 0; q < R; ++q) {
+			V acc = v[0];
+#pragma unroll
+			for (int k = 1; k < R; ++k) {
+				const V w = tw[((q * k) % R) * rs];
+				acc = c_add(acc, c_mul(v[k], INV ? c_conj(w) : w));
+			}
+			y[q] = acc;
+		}
+#pragma unroll
+		for (int q = 0; q < R; ++q) v[q] = y[q];
+	}
+}
+
+// One radix-R butterfly of a stage: elements x[k hs], k < R, of sub-block
+// offset j; twiddles W_L^{k j} = tw[k j tws].
+template <class V, bool INV, int R>
+__device__ __forceinline__ void butterfly(V* x, int hs, int j, int tws, int rs, const V* tw) {
+	V v[R];
+#pragma unroll
+	for (int k = 0; k < R; ++k) v[k] = x[k * hs];
+	if (INV) {
+#pragma unroll
+		for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], c_conj(tw[k * j * tws]));
+	}
+	dft_fixed<V, INV, R>(v, rs, tw);
+	if (!INV) {
+#pragma unroll
+		for (int k = 1; k < R; ++k) v[k] = c_mul(v[k], tw[k * j * tws]);
+	}
+#pragma unroll
+	for (int k = 0; k < R; ++k) x[k * hs] = v[k];
+}
+
+// Any other radix (a prime <= kMaxRadix): the DFT by direct summation.
+template <class V, bool INV>
+__device__ __noinline__ void butterfly_any(V* x, int hs, int r, int j, int tws, int rs,
+                                           const V* tw) {
+	V v[kMaxRadix], y[kMaxRadix];
+	for (int k = 0; k < r; ++k) {
+		v[k] = x[k * hs];
+		if (INV && k > 0) v[k] = c_mul(v[k], c_conj(tw[k * j * tws]));
+	}
+	for (int q = 0; q < r; ++q) {
+		V acc = v[0];
+		for (int k = 1; k < r; ++k) {
+			const V w = tw[((q * k) % r) * rs];
+			acc = c_add(acc, c_mul(v[k], INV ? c_conj(w) : w));
+		}
+		y[q] = (!INV && q > 0) ? c_mul(acc, tw[q * j * tws]) : acc;
+	}
+	for (int q = 0; q < r; ++q) x[q * hs] = y[q];
+}
+
+// Every stage over `nlines` lines: line l, element e at a[l * lstride + e *
+// estride].  lines_fastest puts consecutive threads on consecutive lines
+// (column transforms), else on consecutive elements (row transforms).
+template <class V, bool INV>
+__device__ void fft_lines(V* a, int nlines, int lstride, int estride, const FftPlan& P,
+                          const V* tw, bool lines_fastest) {
+	const int n = P.n;
+	for (int si = 0; si < P.m; ++si) {
+		const int s = INV ? P.m - 1 - si : si;
+		int L = n;
+		for (int t = 0; t < s; ++t) L /= P.r[t];
+		const int r = P.r[s], h = L / r, per = (n / L) * h;
+		const int tws = n / L, rs = n / r;
+		for (int q = threadIdx.x; q < nlines * per; q += blockDim.x) {
+			int line, bj;
+			if (lines_fastest) {
+				line = q % nlines;
+				bj = q / nlines;
+			} else {
+				line = q / per;
+				bj = q % per;
+			}
+			const int b = bj / h, j = bj % h;
+			V* x = a + line * lstride + (b * L + j) * estride;
+			const int hs = h * estride;
+			switch (r) {
+				case 4: butterfly<V, INV, 4>(x, hs, j, tws, rs, tw); break;
+				case 2: butterfly<V, INV, 2>(x, hs, j, tws, rs, tw); break;
+				case 3: butterfly<V, INV, 3>(x, hs, j, tws, rs, tw); break;
+				case 5: butterfly<V, INV, 5>(x, hs, j, tws, rs, tw); break;
+				case 7: butterfly<V, INV, 7>(x, hs, j, tws, rs, tw); break;
+				default: butterfly_any<V, INV>(x, hs, r, j, tws, rs, tw); break;
+			}
 		}
 		__syncthreads();
 	}
 }
 
-__device__ void fft_cols_dif(float2* a, int nx, int ny, const float2* tw) {
-	const int half = nx / 2;
-	for (int h = half; h >= 1; h >>= 1) {
-		const int tstep = half / h;
-		for (int q = threadIdx.x; q < half * ny; q += blockDim.x) {
-			const int c = q % ny, m = q / ny;
-			const int j = m & (h - 1);
-			const int i0 = (((m - j) << 1) + j) * ny + c;
-			const float2 u = a[i0], v = a[i0 + h * ny];
-			a[i0] = c_add(u, v);
-			a[i0 + h * ny] = c_mul(c_sub(u, v), tw[j * tstep]);
-		}
-		__syncthreads();
-	}
-}
-
-__device__ void fft_rows_dit_inv(float2* a, int nx, int ny, const float2* tw) {
-	const int half = ny / 2;
-	for (int h = 1; h <= half; h <<= 1) {
-		const int tstep = half / h;
-		for (int q = threadIdx.x; q < nx * half; q += blockDim.x) {
-			const int r = q / half, m = q % half;
-			const int j = m & (h - 1);
-			const int i0 = r * ny + ((m - j) << 1) + j;
-			const float2 u = a[i0];
-			const float2 v = c_mul(a[i0 + h], c_conj(tw[j * tstep]));
-			a[i0] = c_add(u, v);
-			a[i0 + h] = c_sub(u, v);
-		}
-		__syncthreads();
-	}
-}
-
-__device__ void fft_cols_dit_inv(float2* a, int nx, int ny, const float2* tw) {
-	const int half = nx / 2;
-	for (int h = 1; h <= half; h <<= 1) {
-		const int tstep = half / h;
-		for (int q = threadIdx.x; q < half * ny; q += blockDim.x) {
-			const int c = q % ny, m = q / ny;
-			const int j = m & (h - 1);
-			const int i0 = (((m - j) << 1) + j) * ny + c;
-			const float2 u = a[i0];
-			const float2 v = c_mul(a[i0 + h * ny], c_conj(tw[j * tstep]));
-			a[i0] = c_add(u, v);
-			a[i0 + h * ny] = c_sub(u, v);
-		}
-		__syncthreads();
-	}
+// Window row/column indices of the spectrum positions: position p along an
+// axis of length n holds frequency plan_freq(p), whose window index is its
+// blitz::rotate source.  Built once per CTA into shared memory.
+__device__ void make_window_index(int* idx, const FftPlan& P) {
+	for (int p = threadIdx.x; p < P.n; p += blockDim.x) idx[p] = rotate_src(plan_freq(P, p), P.n);
 }
 
 __global__ void __launch_bounds__(kFuseThreads, 1)
-velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, int lnx, int lny,
-                      const double* __restrict__ kinfo, const double* __restrict__ zs, int nz,
-                      double depth, float2* __restrict__ spectra) {
+velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, FftPlan px,
+                      FftPlan py, const double* __restrict__ kinfo, const double* __restrict__ zs,
+                      int nz, double depth, float2* __restrict__ spectra) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	float2* a = reinterpret_cast<float2*>(smem_raw);  // nx * ny
-	float2* twx = a + nx * ny;                         // nx / 2
-	float2* twy = twx + nx / 2;                        // ny / 2
+	float2* twx = a + nx * ny;                         // nx
+	float2* twy = twx + nx;                            // ny
+	int* wix = reinterpret_cast<int*>(twy + ny);       // nx window row indices
+	int* wiy = wix + nx;                               // ny window column indices
 	const int s = blockIdx.x;
 	const VelSlice<float> S = sl[s];
 	const int n2 = nx * ny;
-	for (int k = threadIdx.x; k < nx / 2; k += blockDim.x) {
-		double sn, cs;
-		sincospi(2.0 * k / nx, &sn, &cs);
-		twx[k] = make_float2(float(cs), float(-sn));
-	}
-	for (int k = threadIdx.x; k < ny / 2; k += blockDim.x) {
-		double sn, cs;
-		sincospi(2.0 * k / ny, &sn, &cs);
-		twy[k] = make_float2(float(cs), float(-sn));
-	}
+	make_twiddles(twx, nx);
+	make_twiddles(twy, ny);
+	make_window_index(wix, px);
+	make_window_index(wiy, py);
 	for (int q = threadIdx.x; q < n2; q += blockDim.x)
 		a[q] = make_float2(float(zeta_t(S, n2, q)), 0.0f);
 	__syncthreads();
-	fft_rows_dif(a, nx, ny, twy);
-	fft_cols_dif(a, nx, ny, twx);
+	fft_lines<float2, false>(a, nx, ny, 1, py, twy, false);  // rows
+	fft_lines<float2, false>(a, ny, 1, ny, px, twx, true);   // columns
 	// with several depths the spectrum is kept in global memory (L2) and
 	// reloaded per depth; the first depth works on it in place
 	float2* spec = spectra ? spectra + (long long)s * n2 : nullptr;
@@ -588,17 +598,13 @@ velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, in
 	for (int iz = 0; iz < nz; ++iz) {
 		__syncthreads();  // the previous depth's output read a[]
 		for (int q = threadIdx.x; q < n2; q += blockDim.x) {
-			// position (i, j) holds frequency (brev i, brev j)
-			const int fi = int(__brev(unsigned(q / ny)) >> (32 - lnx));
-			const int fj = int(__brev(unsigned(q % ny)) >> (32 - lny));
-			const double w = window_fixed(rotate_src(fi, nx), rotate_src(fj, ny), nx, ny, dkx, dky,
-			                              zs[iz], depth);
+			const double w = window_fixed(wix[q / ny], wiy[q % ny], nx, ny, dkx, dky, zs[iz], depth);
 			const float2 x = iz == 0 ? a[q] : spec[q];
 			a[q] = make_float2(float(x.x * w), float(x.y * w));
 		}
 		__syncthreads();
-		fft_cols_dit_inv(a, nx, ny, twx);
-		fft_rows_dit_inv(a, nx, ny, twy);
+		fft_lines<float2, true>(a, ny, 1, ny, px, twx, true);
+		fft_lines<float2, true>(a, nx, ny, 1, py, twy, false);
 		float* out = S.out + (long long)iz * n2;
 		auto f = [&](int r, int c) -> double { return double(a[r * ny + c].x) * inv; };
 		for (int q = threadIdx.x; q < n2; q += blockDim.x)
@@ -606,64 +612,162 @@ velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, in
 	}
 }
 
-int ilog2(int n) {
-	int l = 0;
-	while ((1 << l) < n) ++l;
-	return l;
+// Radices of the forward stages: 4s first, then 2, 3, 5, 7, ... (at most
+// kMaxRadix); false when n has a larger prime factor.
+bool make_plan(int n, FftPlan* P) {
+	P->n = n;
+	P->m = 0;
+	int rest = n;
+	auto push = [&](int r) {
+		if (P->m >= kMaxStages) return false;
+		P->r[P->m++] = r;
+		rest /= r;
+		return true;
+	};
+	while (rest % 4 == 0)
+		if (!push(4)) return false;
+	while (rest % 2 == 0)
+		if (!push(2)) return false;
+	for (int f = 3; rest > 1 && f <= kMaxRadix; f += 2)
+		while (rest % f == 0)
+			if (!push(f)) return false;
+	return rest == 1;
+}
+
+// ---------------------------------------------------------------- 2b. banded
+// Slices larger than the fused kernel's shared memory go through three
+// banded passes with the spectra in global memory (A: one per slice, B: one
+// per slice and depth), each band sized to ~64 KB of shared memory:
+//   vel_rows_fwd   R rows of zeta_t, forward row FFTs        -> A
+//   vel_cols       CB columns of A, forward column FFTs, then per depth the
+//                  window product and inverse column FFTs     -> B
+//   vel_rows_inv   R rows (+ the row above) of B, inverse row FFTs, Re / N
+//                  and the edge extrapolation                  -> output
+template <class T>
+__global__ void __launch_bounds__(256)
+vel_rows_fwd(const VelSlice<T>* __restrict__ sl, int nx, int ny, int R, FftPlan py,
+             typename C2<T>::type* __restrict__ A) {
+	using V = typename C2<T>::type;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	V* a = reinterpret_cast<V*>(smem_raw);  // R x ny
+	V* tw = a + R * ny;                     // ny
+	const long long n2 = (long long)nx * ny;
+	const VelSlice<T> S = sl[blockIdx.y];
+	const int r0 = blockIdx.x * R, rows = min(R, nx - r0);
+	make_twiddles(tw, ny);
+	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x)
+		a[q] = cpx(T(zeta_t(S, n2, (long long)r0 * ny + q)), T(0));
+	__syncthreads();
+	fft_lines<V, false>(a, rows, ny, 1, py, tw, false);
+	V* dst = A + blockIdx.y * n2 + (long long)r0 * ny;
+	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x) dst[q] = a[q];
 }
 
 template <class T>
-void fft2(Ctx* c, typename C2<T>::type* d, long long narr, int nx, int ny, int sign) {
+__global__ void __launch_bounds__(256)
+vel_cols(int nx, int ny, FftPlan px, FftPlan py, int CB, const double* __restrict__ kinfo,
+         const double* __restrict__ zs, int nz, double depth,
+         const typename C2<T>::type* __restrict__ A, typename C2<T>::type* __restrict__ B) {
 	using V = typename C2<T>::type;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	V* spec = reinterpret_cast<V*>(smem_raw);  // nx x cols
+	V* work = nz > 1 ? spec + nx * CB : spec;  // one buffer when there is one depth
+	V* tw = spec + (nz > 1 ? 2 : 1) * nx * CB;  // nx
+	int* wix = reinterpret_cast<int*>(tw + nx);  // nx window row indices
+	int* wiy = wix + nx;                         // ny window column indices
 	const long long n2 = (long long)nx * ny;
-	// rows: narr*nx lines of length ny, contiguous
-	{
-		const int lines = std::max(1, int((48 * 1024 / sizeof(V) - ny / 2) / (2 * ny)));
-		const size_t smem = sizeof(V) * (2 * size_t(lines) * ny + ny / 2);
-		const long long nlines = narr * nx;
-		const int grid = int((nlines + lines - 1) / lines);
-		fft_lines_kernel<T><<<grid, 256, smem, c->stream>>>(d, ny, ilog2(ny), nlines, nx, ny, n2, 1,
-		                                                      lines, sign);
+	const int s = blockIdx.y, c0 = blockIdx.x * CB, cols = min(CB, ny - c0);
+	make_twiddles(tw, nx);
+	make_window_index(wix, px);
+	make_window_index(wiy, py);
+	const V* src = A + s * n2 + c0;
+	for (int q = threadIdx.x; q < nx * cols; q += blockDim.x)
+		spec[q] = src[(long long)(q / cols) * ny + q % cols];
+	__syncthreads();
+	fft_lines<V, false>(spec, cols, 1, cols, px, tw, true);
+	const double wx = 1.0 / kinfo[s * 4 + 0], wy = 1.0 / kinfo[s * 4 + 1];
+	const double dkx = wx / max(nx - 1, 1), dky = wy / max(ny - 1, 1);
+	for (int iz = 0; iz < nz; ++iz) {
+		for (int q = threadIdx.x; q < nx * cols; q += blockDim.x) {
+			const double w = window_fixed(wix[q / cols], wiy[c0 + q % cols], nx, ny, dkx, dky,
+			                              zs[iz], depth);
+			const V x = spec[q];
+			work[q] = cpx(T(x.x * w), T(x.y * w));
+		}
+		__syncthreads();
+		fft_lines<V, true>(work, cols, 1, cols, px, tw, true);
+		V* dst = B + ((long long)s * nz + iz) * n2 + c0;
+		for (int q = threadIdx.x; q < nx * cols; q += blockDim.x)
+			dst[(long long)(q / cols) * ny + q % cols] = work[q];
+		__syncthreads();
 	}
-	// columns: narr*ny lines of length nx, element stride ny
-	{
-		const int lines = std::max(1, std::min(16, int((48 * 1024 / sizeof(V) - nx / 2) / (2 * nx))));
-		const size_t smem = sizeof(V) * (2 * size_t(lines) * nx + nx / 2);
-		const long long nlines = narr * ny;
-		const int grid = int((nlines + lines - 1) / lines);
-		fft_lines_kernel<T><<<grid, 256, smem, c->stream>>>(d, nx, ilog2(nx), nlines, ny, 1, n2, ny,
-		                                                      lines, sign);
-	}
-	ARMA_CUDA_TRY(cudaGetLastError());
-	c->launches += 2;
 }
 
-// The general path for one pass of slices: FFTs through global memory.
 template <class T>
-void velocity_general(Ctx* c, const VelSlice<T>* d_sl, int ns, int nx, int ny, const double* d_k,
-                      const double* d_z, int nz, double depth) {
+__global__ void __launch_bounds__(256)
+vel_rows_inv(const VelSlice<T>* __restrict__ sl, int nx, int ny, int R, int nz, FftPlan py,
+             const typename C2<T>::type* __restrict__ B) {
+	using V = typename C2<T>::type;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	V* a = reinterpret_cast<V*>(smem_raw);  // (R + 1) x ny: the row above the band first
+	V* tw = a + (R + 1) * ny;               // ny
+	const long long n2 = (long long)nx * ny;
+	const long long arr = blockIdx.y;  // slice * nz + depth
+	const int r0 = blockIdx.x * R, rows = min(R, nx - r0);
+	make_twiddles(tw, ny);
+	const V* src = B + arr * n2;
+	for (int q = threadIdx.x; q < (rows + 1) * ny; q += blockDim.x) {
+		const int row = r0 - 1 + q / ny;
+		a[q] = row >= 0 ? src[(long long)row * ny + q % ny] : cpx(T(0), T(0));
+	}
+	__syncthreads();
+	fft_lines<V, true>(a, rows + 1, ny, 1, py, tw, false);
+	const double inv = 1.0 / double(n2);
+	auto f = [&](int x, int y) -> double { return double(a[(x - r0 + 1) * ny + y].x) * inv; };
+	T* out = sl[arr / nz].out + (arr % nz) * n2 + (long long)r0 * ny;
+	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x)
+		out[q] = T(finish_at(r0 + q / ny, q % ny, nx, ny, f));
+}
+
+// The banded path for one pass of slices.
+template <class T>
+void velocity_general(Ctx* c, const VelSlice<T>* d_sl, int ns, int nx, int ny, const FftPlan& px,
+                      const FftPlan& py, const double* d_k, const double* d_z, int nz,
+                      double depth) {
 	using V = typename C2<T>::type;
 	const long long n2 = (long long)nx * ny;
-	V* a = static_cast<V*>(scratch_take(c, sizeof(V) * n2 * ns));
-	V* b = static_cast<V*>(scratch_take(c, sizeof(V) * n2 * ns * nz));
-	const int g = c->num_sms * 8;
-	deriv_kernel<T><<<g, 256, 0, c->stream>>>(d_sl, ns, nx, ny, a);
-	c->launches += 1;
-	fft2<T>(c, a, ns, nx, ny, -1);
-	window_mul_kernel<T><<<g, 256, 0, c->stream>>>(a, nx, ny, ns, d_k, d_z, nz, depth, b);
-	c->launches += 1;
-	fft2<T>(c, b, (long long)ns * nz, nx, ny, +1);
-	finish_kernel<T><<<g, 256, 0, c->stream>>>(b, nx, ny, (long long)ns * nz, nz, d_sl);
+	const int budget = int((64 << 10) / sizeof(V));  // elements of one 64 KB band
+	const int R = std::min(nx, std::max(4, budget / ny));
+	const int CB = std::min(ny, std::max(1, budget / nx));
+	V* A = static_cast<V*>(scratch_take(c, sizeof(V) * n2 * ns));
+	V* B = static_cast<V*>(scratch_take(c, sizeof(V) * n2 * ns * nz));
+	const size_t s1 = sizeof(V) * (size_t(R) * ny + ny);
+	const size_t s2 = sizeof(V) * ((nz > 1 ? 2 : 1) * size_t(nx) * CB + nx) +
+	                  sizeof(int) * (size_t(nx) + ny);
+	const size_t s3 = sizeof(V) * (size_t(R + 1) * ny + ny);
+	ARMA_CUDA_TRY(cudaFuncSetAttribute(vel_rows_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                   int(s1)));
+	ARMA_CUDA_TRY(cudaFuncSetAttribute(vel_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                   int(s2)));
+	ARMA_CUDA_TRY(cudaFuncSetAttribute(vel_rows_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                   int(s3)));
+	const int bands = (nx + R - 1) / R, cbands = (ny + CB - 1) / CB;
+	vel_rows_fwd<T><<<dim3(bands, ns), 256, s1, c->stream>>>(d_sl, nx, ny, R, py, A);
+	vel_cols<T><<<dim3(cbands, ns), 256, s2, c->stream>>>(nx, ny, px, py, CB, d_k, d_z, nz, depth,
+	                                                       A, B);
+	vel_rows_inv<T><<<dim3(bands, ns * nz), 256, s3, c->stream>>>(d_sl, nx, ny, R, nz, py, B);
 	ARMA_CUDA_TRY(cudaGetLastError());
-	c->launches += 1;
+	c->launches += 3;
 }
 
 template <class T>
 void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int ny, double depth,
                      const double* z, int nz) {
-	ARMA_REQUIRE((nx & (nx - 1)) == 0 && (ny & (ny - 1)) == 0 && nx >= 4 && ny >= 4 &&
-	                 nx <= 1024 && ny <= 1024,
-	             ARMA_ENOTSUP, "velocity solver: slice sides must be powers of two in [4, 1024]");
+	FftPlan px, py;
+	ARMA_REQUIRE(nx >= 4 && ny >= 4 && nx <= 1024 && ny <= 1024 && make_plan(nx, &px) &&
+	                 make_plan(ny, &py),
+	             ARMA_ENOTSUP,
+	             "velocity solver: slice sides must be in [4, 1024] with prime factors <= 64");
 	ARMA_REQUIRE(nz >= 1, ARMA_EINVAL, "no z levels");
 	const int ns = int(slices.size());
 	if (ns == 0) return;
@@ -674,18 +778,18 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d_sl, slices.data(), sizeof(VelSlice<T>) * ns,
 	                              cudaMemcpyHostToDevice, c->stream));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d_z, z, sizeof(double) * nz, cudaMemcpyHostToDevice, c->stream));
-	factor_waves_kernel<T><<<2 * ns, kFwThreads, 0, c->stream>>>(d_sl, nx, ny, d_k);
+	factor_waves_kernel<T><<<2 * ns, kFwWarps * 32, 0, c->stream>>>(d_sl, nx, ny, d_k);
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 	if (sizeof(T) == sizeof(float) && n2 <= kFuseMax) {
-		const size_t smem = sizeof(float2) * (size_t(n2) + nx / 2 + ny / 2);
+		const size_t smem = sizeof(float2) * (size_t(n2) + nx + ny) + sizeof(int) * (nx + ny);
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(velocity_fused_kernel,
 		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
 		float2* spectra =
 		    nz > 1 ? static_cast<float2*>(scratch_take(c, sizeof(float2) * n2 * ns)) : nullptr;
 		velocity_fused_kernel<<<ns, kFuseThreads, smem, c->stream>>>(
-		    reinterpret_cast<const VelSlice<float>*>(d_sl), int(nx), int(ny), ilog2(nx), ilog2(ny),
-		    d_k, d_z, nz, depth, spectra);
+		    reinterpret_cast<const VelSlice<float>*>(d_sl), int(nx), int(ny), px, py, d_k, d_z, nz,
+		    depth, spectra);
 		ARMA_CUDA_TRY(cudaGetLastError());
 		c->launches += 1;
 		return;
@@ -695,13 +799,18 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	const int pass = int(std::max<long long>(1, std::min<long long>(ns, (512ll << 20) / per_slice)));
 	for (int s0 = 0; s0 < ns; s0 += pass) {
 		const ScratchMark mark = scratch_mark(c);
-		velocity_general<T>(c, d_sl + s0, std::min(pass, ns - s0), nx, ny, d_k + 4 * s0, d_z, nz,
-		                    depth);
+		velocity_general<T>(c, d_sl + s0, std::min(pass, ns - s0), nx, ny, px, py, d_k + 4 * s0, d_z,
+		                    nz, depth);
 		scratch_release(c, mark);
 	}
 }
 
 }  // namespace
+
+bool velocity_supported(int nx, int ny) {
+	FftPlan p;
+	return nx >= 4 && ny >= 4 && nx <= 1024 && ny <= 1024 && make_plan(nx, &p) && make_plan(ny, &p);
+}
 
 void launch_velocity_linear(Ctx* c, const void* d_zeta, const int shape[3], int precision,
                             const double delta[3], double depth, const double* z, int nz,

@@ -30,7 +30,7 @@ def write_mt(path):
 
 def config(mt, output="surface,csv,blitz,binary", extra=""):
     return f"""model = AR {{
-	out_grid = (40,32,32)
+	out_grid = (40,24,24)
 	acf = {{
 		func = standing_wave
 		grid = (10,10,10) : (2.5,5,5)
@@ -63,7 +63,7 @@ def oracle_fit():
 def oracle_surface(phi, var, acf0, seed=1234):
     """The oracle chain on the driver's own coefficients, so that the surface
     check isolates noise + filter + renormalisation."""
-    shape = (40, 32, 32)
+    shape = (40, 24, 24)
     eps = O.white_noise(O.mt19937_params(), seed, math.sqrt(var),
                         int(np.prod(shape))).reshape(shape)
     zeta, _ = O.variance_renorm(O.ar_filter(eps, phi), acf0)
@@ -85,7 +85,7 @@ def test_driver_generate_velocity_write(ctx, tmp_path):
 
     d.compute_velocity_potentials(ctx)
     info = d.info()
-    assert info["velocity_shape"] == (3, 4, 32, 32)
+    assert info["velocity_shape"] == (3, 4, 24, 24)
     vel = d.velocity_potentials()
     t_idx = [10, 20, 30]
     z = [-6.0, -4.0, -2.0, 0.0]
@@ -101,9 +101,9 @@ def test_driver_generate_velocity_write(ctx, tmp_path):
     O.write_zeta_csv(str(tmp_path / "ref.csv"), zeta, info["delta"])
     assert (out / "zeta.csv").read_text() == (tmp_path / "ref.csv").read_text()
     head = (out / "zeta").read_text().split("\n", 1)[0]
-    assert head == "(0,39) x (0,31) x (0,31)"
+    assert head == "(0,39) x (0,23) x (0,23)"
     rows = (out / "phi.csv").read_text().splitlines()
-    assert rows[0] == "t,z,x,y,phi" and len(rows) == 1 + 3 * 4 * 32 * 32
+    assert rows[0] == "t,z,x,y,phi" and len(rows) == 1 + 3 * 4 * 24 * 24
 
 
 def test_driver_fp32c_and_nit(ctx, tmp_path):
@@ -140,4 +140,4 @@ def test_cli_runs(tmp_path):
     out = tmp_path / "o"
     out.mkdir()
     assert main(["-C", str(out), str(cfg)]) == 0
-    assert (out / "zeta.bin").stat().st_size == 40 * 32 * 32 * 8
+    assert (out / "zeta.bin").stat().st_size == 40 * 24 * 24 * 8

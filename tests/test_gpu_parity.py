@@ -318,3 +318,30 @@ def test_velocity_batch_equals_single_calls(ctx):
                                 ref.data_ptr())
             ctx.synchronize()
             assert torch.equal(o, ref)
+
+
+@pytest.mark.parametrize("shape,depth,zs", [
+    ((8, 40, 24), 12.0, [0.0, -3.0]),     # 40 = 4.2.5, 24 = 4.2.3
+    ((6, 20, 30), np.inf, [0.0]),         # 30 = 2.3.5
+    ((5, 12, 100), np.inf, [0.0, -1.0]),  # 100 = 4.5.5
+    ((4, 28, 36), 12.0, [0.0]),           # 28 = 4.7, 36 = 4.3.3
+    ((4, 13, 16), np.inf, [0.0]),         # 13: direct-summation radix
+    ((3, 200, 100), np.inf, [0.0]),       # FP32 over 16384 points: banded passes
+])
+def test_velocity_mixed_radix_vs_oracle(ctx, shape, depth, zs):
+    """Slice sides that are not powers of two (the reference's GSL mixed-radix
+    FFT takes any length): FP64 within 1e-9 and FP32 within 2e-4 of max|phi|
+    against the oracle's direct DFT."""
+    phi, var = A.ar_fit_analytic(A.ACF_STANDING, (3, 3, 3), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    eps = O.white_noise(O.mt19937_params(), 5, np.sqrt(var), int(np.prod(shape))).reshape(shape)
+    zeta = O.ar_filter(eps, phi)
+    tidx = list(range(shape[0]))
+    ref = O.velocity_linear(zeta, (1.0, 1.0, 1.0), depth, zs, tidx)
+    scale = np.abs(ref).max()
+    for prec, dt, tol in [(A.FP64, torch.float64, 1e-9), (A.FP32C, torch.float32, 2e-4)]:
+        z = dev(zeta, dt)
+        out = torch.zeros(ref.shape, dtype=dt, device="cuda")
+        ctx.velocity_linear(z.data_ptr(), shape, prec, (1.0, 1.0, 1.0), depth, zs, tidx,
+                            out.data_ptr())
+        got = out.cpu().numpy().astype(np.float64)
+        assert np.abs(got - ref).max() <= tol * scale, (prec, np.abs(got - ref).max() / scale)

@@ -208,7 +208,7 @@ def test_open_rejects_bad_streams():
     phi, var = model()
     with A.Server(chunk_slices=8, velocity=1) as srv:
         with pytest.raises(A.ArmaError) as e:
-            srv.open_stream(96, 64, phi, var, 0.0, mt(), 1)   # FFT sides
+            srv.open_stream(67, 64, phi, var, 0.0, mt(), 1)   # prime side > 64: no FFT plan
         assert e.value.code == -8
         big, bv = model((13, 4, 4))
         with pytest.raises(A.ArmaError) as e:
