@@ -94,6 +94,25 @@ def flops(batch):
     return float(sum(np.prod(s["shape"]) * 2 * (np.prod(s["order"]) - 1) for s in batch))
 
 
+def shard_value(points_per_rank: int, steps: int, elapsed_s: float, world: int) -> float:
+    """Whole-job points/s of a weakly scaled run: every rank processes its own
+    batch of `points_per_rank` points per step; `elapsed_s` is the max over
+    ranks of the timed region."""
+    return world * points_per_rank * steps / elapsed_s
+
+
+def reduce_max(x: float, device: str) -> float:
+    """Max of x over the ranks of the default process group (x itself when
+    there is none)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # --------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -240,11 +259,7 @@ def gpu_arm(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, "cuda")
 
     # ---- device-resident FP32 compensated batch
     for _ in range(args.warmup):
@@ -270,7 +285,7 @@ def gpu_arm(args):
     ar_ms, ar_n = ctx.profile("ar32c")
     prof = {k: ctx.profile(k) for k in ("mt", "noise", "ar32c", "renorm")}
     ctx.set_profiling(False)
-    value = world * npts * args.steps / elapsed
+    value = shard_value(npts, args.steps, elapsed, world)
 
     # ---- e2e: same call into pinned host buffers
     e2e = None
