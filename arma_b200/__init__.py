@@ -11,5 +11,5 @@ from .capi import (  # noqa: F401
     FP64, FP32C, ACF_STANDING, ACF_PROPAGATING,
     NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL, NIT_BISECTION, NIT_LUT,
     acf_eval, ar_fit, ar_fit_analytic, mt19937_params, mt_file_count,
-    mt_file_read, mt_file_write,
+    mt_file_read, mt_file_write, poly_roots, validate_process,
 )

@@ -42,7 +42,8 @@ EXPORTS = (
     "arma_driver_copy", "arma_server_config_default", "arma_server_create",
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
-    "arma_server_profile", "arma_velocity_linear_batch",
+    "arma_server_profile", "arma_velocity_linear_batch", "arma_validate_process",
+    "arma_poly_roots",
 )
 
 
@@ -190,6 +191,8 @@ def lib():
             "arma_server_last_failure": (i, [vp, C.c_char_p, sz]),
             "arma_server_profile": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_uint64)]),
             "arma_velocity_linear_batch": (i, [vp, C.POINTER(VelocityJob), i, i, i, i, d, dp, i]),
+            "arma_validate_process": (i, [dp, ip, ip]),
+            "arma_poly_roots": (i, [dp, i, dp, dp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -246,6 +249,30 @@ def ar_fit_analytic(kind, order, amplitude, velocity, alpha, beta, delta=(1.0, 1
     _check(lib().arma_ar_fit_analytic(kind, amplitude, velocity, ap, bp, dlp, _i3(order),
                                       _dp(phi), C.byref(var)))
     return phi, var.value
+
+
+def validate_process(phi) -> int:
+    """Raises ArmaError (ARMA_EINVAL) when the flattened AR polynomial has roots
+    inside or on the unit circle; returns the number of such roots (0)."""
+    phi = np.ascontiguousarray(phi, np.float64)
+    bad = C.c_int()
+    rc = lib().arma_validate_process(_dp(phi), _i3(phi.shape), C.byref(bad))
+    if rc != 0:
+        err = C.create_string_buffer(1024)
+        lib().arma_last_error(err, len(err))
+        e = ArmaError(rc, err.value.decode(errors="replace"))
+        e.bad_roots = bad.value
+        raise e
+    return bad.value
+
+
+def poly_roots(c):
+    """Complex roots of c[0] + c[1] x + ... + c[n-1] x^(n-1)."""
+    c = np.ascontiguousarray(c, np.float64)
+    re = np.empty(len(c) - 1)
+    im = np.empty(len(c) - 1)
+    _check(lib().arma_poly_roots(_dp(c), len(c), _dp(re), _dp(im)))
+    return re + 1j * im
 
 
 def mt19937_params() -> MtParams:

@@ -788,6 +788,36 @@ int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n, int p
 	});
 }
 
+// ---------------------------------------------------------------- A5
+int arma_poly_roots(const double* c, int n, double* re, double* im) {
+	return guard([&] {
+		ARMA_REQUIRE(c && re && im && n >= 2, ARMA_EINVAL, "null argument or n < 2");
+		std::vector<std::complex<double>> roots;
+		const int rc = poly_roots(c, n, roots);
+		if (rc == 1) throw Error{ARMA_ENUMERIC, "leading term of polynomial must be non-zero"};
+		if (rc == 2) throw Error{ARMA_ENUMERIC, "root solving qr method failed to converge"};
+		for (int i = 0; i < n - 1; ++i) {
+			re[i] = roots[i].real();
+			im[i] = roots[i].imag();
+		}
+	});
+}
+
+int arma_validate_process(const double* phi, const int order[3], int* bad_roots) {
+	return guard([&] {
+		ARMA_REQUIRE(phi && order && bad_roots, ARMA_EINVAL, "null argument");
+		require_order(order);
+		const int P = order[0] * order[1] * order[2];
+		const int rc = validate_ar_process(phi, P, bad_roots);
+		if (rc == 1) throw Error{ARMA_ENUMERIC, "leading term of polynomial must be non-zero"};
+		if (rc == 2) throw Error{ARMA_ENUMERIC, "root solving qr method failed to converge"};
+		if (rc == 3)
+			throw Error{ARMA_EINVAL,
+			            "AR/MA process is not stationary/invertible: some roots lie inside unit "
+			            "circle or on its borderline."};
+	});
+}
+
 // ---------------------------------------------------------------- driver
 struct arma_driver {
 	armab::Driver* d;

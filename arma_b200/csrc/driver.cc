@@ -471,6 +471,18 @@ void driver_generate(Ctx* c, Driver* d) {
 	                              a.order, d->phi.data(), &d->var_wn);
 	if (info != 0)
 		throw Error{ARMA_ENUMERIC, "Yule-Walker matrix is not positive definite"};
+	// validate_process on the fitted coefficients (src/generator/basic_arma_model.cc:
+	// 92-96, src/generator/ar_model.cc:64-68), before the noise
+	if (a.validate) {
+		int bad = 0;
+		const int rc = validate_ar_process(d->phi.data(), P, &bad);
+		if (rc == 1) throw Error{ARMA_ENUMERIC, "leading term of polynomial must be non-zero"};
+		if (rc == 2) throw Error{ARMA_ENUMERIC, "root solving qr method failed to converge"};
+		if (rc == 3)
+			throw Error{ARMA_EINVAL,
+			            "AR/MA process is not stationary/invertible: some roots lie inside unit "
+			            "circle or on its borderline."};
+	}
 	if (d->var_wn < 0.0) throw Error{ARMA_EINVAL, "variance is less than zero"};
 	arma_mt_params mt;
 	{

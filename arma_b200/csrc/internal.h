@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <complex>
 #include <cstdint>
 #include <exception>
 #include <map>
@@ -249,6 +250,14 @@ const double* driver_velocity_data(const Driver* d);
 // Inverse-CDF table for the NIT LUT path.
 void nit_build_lut(int dist, const double params[3], double stdev, int nodes,
                    double range, double* x0, double* dx, std::vector<double>& y);
+
+// Roots of c[0] + c[1] x + ... + c[n-1] x^(n-1) (validate.cc): 0, 1 when the
+// leading coefficient is zero or n < 2, 2 when the QR iteration does not
+// converge.
+int poly_roots(const double* c, int n, std::vector<std::complex<double>>& roots);
+// validate_process on the flattened phi (P coefficients): 0 stationary, 3 with
+// *bad_roots roots of modulus <= 1, or poly_roots' failure code.
+int validate_ar_process(const double* phi, int P, int* bad_roots);
 
 // Polar attempts generated for n normals: the expected count plus 8 sigma,
 // times `margin` (capi.cu).

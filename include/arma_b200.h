@@ -225,6 +225,18 @@ int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n,
 int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n,
                              int precision);
 
+/* ------------------------------------------------ A5: stationarity */
+/* validate_process (src/arma.cc:14-70): the roots of the flattened
+ * polynomial 1 - sum_k phi_k x^k, k = 1 .. P-1 (P = order product), by the
+ * balanced companion-matrix QR method of gsl_poly_complex_solve.  ARMA_OK when
+ * every root lies outside the unit circle; ARMA_EINVAL otherwise ("AR/MA
+ * process is not stationary/invertible..."), with *bad_roots set; ARMA_ENUMERIC
+ * when the leading coefficient is zero or the iteration fails. */
+int arma_validate_process(const double* phi, const int order[3], int* bad_roots);
+/* The root finder itself: roots of c[0] + c[1] x + ... + c[n-1] x^(n-1) into
+ * re/im (n-1 each), as gsl_poly_complex_solve. */
+int arma_poly_roots(const double* c, int n, double* re, double* im);
+
 /* ------------------------------------------------ programme layer */
 /* The reference's ARMA_driver (src/arma_driver.hh:43-150): parses a `.arma`
  * configuration (`model = AR {...}`, `velocity_potential_solver = linear
