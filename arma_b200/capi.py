@@ -43,7 +43,7 @@ EXPORTS = (
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
     "arma_server_profile", "arma_velocity_linear_batch", "arma_validate_process",
-    "arma_poly_roots",
+    "arma_poly_roots", "arma_ar_fit_choi",
 )
 
 
@@ -193,6 +193,7 @@ def lib():
             "arma_velocity_linear_batch": (i, [vp, C.POINTER(VelocityJob), i, i, i, i, d, dp, i]),
             "arma_validate_process": (i, [dp, ip, ip]),
             "arma_poly_roots": (i, [dp, i, dp, dp]),
+            "arma_ar_fit_choi": (i, [dp, i, i, i, d, i, dp, ip, dp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -249,6 +250,22 @@ def ar_fit_analytic(kind, order, amplitude, velocity, alpha, beta, delta=(1.0, 1
     _check(lib().arma_ar_fit_analytic(kind, amplitude, velocity, ap, bp, dlp, _i3(order),
                                       _dp(phi), C.byref(var)))
     return phi, var.value
+
+
+def ar_fit_choi(acf, max_order=None, determine_order=True, var_epsilon=1e-6, chop=True):
+    """Choi's order-recursive solver on a cubic ACF: (phi, var_wn)."""
+    acf = np.ascontiguousarray(acf, np.float64)
+    n = acf.shape[0]
+    if acf.shape != (n, n, n):
+        raise ValueError("ACF is not square")
+    mo = min(n - 1, max_order if max_order else n - 1)
+    buf = np.zeros(mo ** 3)
+    order = (C.c_int * 3)()
+    var = C.c_double()
+    _check(lib().arma_ar_fit_choi(_dp(acf), n, mo, 1 if determine_order else 0, var_epsilon,
+                                  1 if chop else 0, _dp(buf), order, C.byref(var)))
+    shape = tuple(order)
+    return buf[:int(np.prod(shape))].reshape(shape).copy(), var.value
 
 
 def validate_process(phi) -> int:

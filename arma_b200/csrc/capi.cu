@@ -1,5 +1,6 @@
 // C ABI: argument checking, error mapping, context and scratch management,
 // and the orchestration of the device kernels.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -785,6 +786,25 @@ int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n, int p
 		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
 		scratch_begin(&ctx->c, 0);
 		batch(&ctx->c, surfaces, n, precision, true);
+	});
+}
+
+// ---------------------------------------------------------------- A3'
+int arma_ar_fit_choi(const double* acf, int n, int max_order, int determine_order,
+                     double var_epsilon, int chop, double* phi_out, int order_out[3],
+                     double* var_wn) {
+	return guard([&] {
+		ARMA_REQUIRE(acf && phi_out && order_out && var_wn, ARMA_EINVAL, "null argument");
+		ARMA_REQUIRE(n >= 2 && max_order >= 1, ARMA_EINVAL, "bad ACF size or AR order");
+		std::vector<double> phi;
+		double solver_var = 0.0;
+		const int rc = fit_choi(acf, n, max_order, determine_order != 0, var_epsilon, chop != 0,
+		                        1e-10, &phi, order_out, &solver_var);
+		if (rc == 2) throw Error{ARMA_ENUMERIC, "singular Yule-Walker block"};
+		ARMA_REQUIRE(rc == 0, ARMA_EINVAL, "bad ACF size or AR order");
+		std::copy(phi.begin(), phi.end(), phi_out);
+		const int shape[3] = {n, n, n};
+		*var_wn = ar_white_noise_variance(acf, shape, phi.data(), order_out);
 	});
 }
 

@@ -465,12 +465,30 @@ void driver_generate(Ctx* c, Driver* d) {
 	         d->acf.data());
 	// The reference NIT-transforms a copy of the ACF and discards it
 	// (src/generator/basic_arma_model.cc:74-79): the fit uses the Gaussian ACF.
+	if (a.algorithm == "choi_recursive") {
+		// determine_coefficients_choi (src/generator/ar_model.cc:136-152): the
+		// order-recursive solver on the ACF table, maximum order max(order),
+		// variance tolerance 1e-6, chopped; the model's order replaces the
+		// configured one and var_wn is recomputed from phi
+		const int n = d->acf_shape[0];
+		if (d->acf_shape[1] != n || d->acf_shape[2] != n)
+			throw Error{ARMA_EINVAL, "ACF is not square"};
+		const int mo = std::max(a.order[0], std::max(a.order[1], a.order[2]));
+		double solver_var = 0.0;
+		const int rc = fit_choi(d->acf.data(), n, mo, true, 1e-6, true, 1e-10, &d->phi, a.order,
+		                        &solver_var);
+		if (rc == 2) throw Error{ARMA_ENUMERIC, "singular Yule-Walker block"};
+		if (rc != 0) throw Error{ARMA_EINVAL, "bad AR model order"};
+		d->var_wn = ar_white_noise_variance(d->acf.data(), d->acf_shape, d->phi.data(), a.order);
+	} else {
+		const int P0 = a.order[0] * a.order[1] * a.order[2];
+		d->phi.assign(P0, 0.0);
+		const int info = fit_analytic(a.acf_kind, a.amplitude, a.velocity, a.alpha, a.beta, adelta,
+		                              a.order, d->phi.data(), &d->var_wn);
+		if (info != 0)
+			throw Error{ARMA_ENUMERIC, "Yule-Walker matrix is not positive definite"};
+	}
 	const int P = a.order[0] * a.order[1] * a.order[2];
-	d->phi.assign(P, 0.0);
-	const int info = fit_analytic(a.acf_kind, a.amplitude, a.velocity, a.alpha, a.beta, adelta,
-	                              a.order, d->phi.data(), &d->var_wn);
-	if (info != 0)
-		throw Error{ARMA_ENUMERIC, "Yule-Walker matrix is not positive definite"};
 	// validate_process on the fitted coefficients (src/generator/basic_arma_model.cc:
 	// 92-96, src/generator/ar_model.cc:64-68), before the noise
 	if (a.validate) {

@@ -251,6 +251,16 @@ const double* driver_velocity_data(const Driver* d);
 void nit_build_lut(int dist, const double params[3], double stdev, int nodes,
                    double range, double* x0, double* dx, std::vector<double>& y);
 
+// Choi's order-recursive Yule-Walker solver (choi.cc) on a cubic n^3 ACF:
+// 0 with phi (order[0] x order[1] x order[2]) and the solver's variance, 1 bad
+// sizes, 2 singular block.
+int fit_choi(const double* acf, int n, int max_order, bool determine_order, double var_eps,
+             bool chop, double chop_eps, std::vector<double>* phi, int order[3], double* var_out);
+// white_noise_variance (src/generator/ar_model.cc:55-61): acf(0,0,0) minus the
+// sum of phi times the ACF over phi's box (acf is n0 x n1 x n2).
+double ar_white_noise_variance(const double* acf, const int acf_shape[3], const double* phi,
+                               const int order[3]);
+
 // Roots of c[0] + c[1] x + ... + c[n-1] x^(n-1) (validate.cc): 0, 1 when the
 // leading coefficient is zero or n < 2, 2 when the QR iteration does not
 // converge.

@@ -225,6 +225,20 @@ int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n,
 int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n,
                              int precision);
 
+/* ------------------------------------------------ A3': Choi solver */
+/* Yule_walker_solver::solve (src/yule_walker.cc:426-539) as called by
+ * AR_model::determine_coefficients_choi (src/generator/ar_model.cc:136-152):
+ * the order-recursive solver on a cubic acf of n^3 values (lags accessed by
+ * absolute value), up to max_order (clamped to n-1); with determine_order it
+ * stops when the white-noise variance changes by less than var_epsilon (the
+ * reference's AR model uses 1e-6); with chop it drops trailing planes whose
+ * values are all below 1e-10.  phi_out must hold max_order^3 doubles;
+ * order_out receives the model's shape; var_wn = acf(0,0,0) - sum(phi * acf
+ * over phi's box), as the reference recomputes it. */
+int arma_ar_fit_choi(const double* acf, int n, int max_order, int determine_order,
+                     double var_epsilon, int chop, double* phi_out, int order_out[3],
+                     double* var_wn);
+
 /* ------------------------------------------------ A5: stationarity */
 /* validate_process (src/arma.cc:14-70): the roots of the flattened
  * polynomial 1 - sum_k phi_k x^k, k = 1 .. P-1 (P = order product), by the

@@ -40,6 +40,7 @@ def config(mt, output="surface,csv,blitz,binary", extra=""):
 		beta = (0.8,0.8)
 	}}
 	order = (5,5,5)
+	algorithm = gauss_elimination
 	output = {output}
 	validate = 0
 	seed = 1234
@@ -141,3 +142,22 @@ def test_cli_runs(tmp_path):
     out.mkdir()
     assert main(["-C", str(out), str(cfg)]) == 0
     assert (out / "zeta.bin").stat().st_size == 40 * 24 * 24 * 8
+
+
+def test_driver_choi_default_algorithm(ctx, tmp_path):
+    """Without `algorithm`, the reference fits with Choi's recursive solver on
+    the ACF table: the driver's order and phi are the solver's, and the surface
+    is the oracle chain on those coefficients."""
+    mt = write_mt(tmp_path / "mt.dat")
+    text = config(mt, output="none").replace("\talgorithm = gauss_elimination\n", "")
+    text = text.replace("alpha = (0.06,0.06,0.06)", "alpha = (0.3,0.3,0.3)")
+    d = A.Driver(text)
+    d.generate_wavy_surface(ctx)
+    delta = [L / 9 for L in ACF_LEN]
+    acf = O.acf("standing_wave", (10, 10, 10), 1.5, 0.5, [0.3] * 3, [0.8, 0.8], delta)
+    phi, var = A.ar_fit_choi(acf, max_order=5)
+    assert d.info()["order"] == phi.shape == (5, 5, 5) and var > 0
+    np.testing.assert_array_equal(d.phi(), phi)
+    assert d.info()["var_wn"] == var
+    zeta_ref = oracle_surface(phi, var, acf[0, 0, 0])
+    assert np.abs(d.zeta() - zeta_ref).max() <= 1e-12 * np.abs(zeta_ref).max()
