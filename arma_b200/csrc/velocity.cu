@@ -521,10 +521,13 @@ __device__ __noinline__ void butterfly_any(V* x, int hs, int r, int j, int tws, 
 
 // Every stage over `nlines` lines: line l, element e at a[l * lstride + e *
 // estride].  lines_fastest puts consecutive threads on consecutive lines
-// (column transforms), else on consecutive elements (row transforms).
+// (column transforms), else on consecutive elements (row transforms); with
+// rows_padded (row transforms whose line stride is an odd number of
+// elements) stages of span h < 32 also go lines-first, which keeps their
+// butterflies free of shared-memory bank conflicts.
 template <class V, bool INV>
 __device__ void fft_lines(V* a, int nlines, int lstride, int estride, const FftPlan& P,
-                          const V* tw, bool lines_fastest) {
+                          const V* tw, bool lines_fastest, bool rows_padded = false) {
 	const int n = P.n;
 	for (int si = 0; si < P.m; ++si) {
 		const int s = INV ? P.m - 1 - si : si;
@@ -532,9 +535,10 @@ __device__ void fft_lines(V* a, int nlines, int lstride, int estride, const FftP
 		for (int t = 0; t < s; ++t) L /= P.r[t];
 		const int r = P.r[s], h = L / r, per = (n / L) * h;
 		const int tws = n / L, rs = n / r;
+		const bool lf = lines_fastest || (rows_padded && h < 32 && nlines >= 8);
 		for (int q = threadIdx.x; q < nlines * per; q += blockDim.x) {
 			int line, bj;
-			if (lines_fastest) {
+			if (lf) {
 				line = q % nlines;
 				bj = q / nlines;
 			} else {
@@ -569,8 +573,9 @@ velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, Ff
                       FftPlan py, const double* __restrict__ kinfo, const double* __restrict__ zs,
                       int nz, double depth, float2* __restrict__ spectra) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	float2* a = reinterpret_cast<float2*>(smem_raw);  // nx * ny
-	float2* twx = a + nx * ny;                         // nx
+	const int ld = ny + 1;                             // padded row stride
+	float2* a = reinterpret_cast<float2*>(smem_raw);  // nx rows of ld
+	float2* twx = a + nx * ld;                         // nx
 	float2* twy = twx + nx;                            // ny
 	int* wix = reinterpret_cast<int*>(twy + ny);       // nx window row indices
 	int* wiy = wix + nx;                               // ny window column indices
@@ -582,15 +587,15 @@ velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, Ff
 	make_window_index(wix, px);
 	make_window_index(wiy, py);
 	for (int q = threadIdx.x; q < n2; q += blockDim.x)
-		a[q] = make_float2(float(zeta_t(S, n2, q)), 0.0f);
+		a[(q / ny) * ld + q % ny] = make_float2(float(zeta_t(S, n2, q)), 0.0f);
 	__syncthreads();
-	fft_lines<float2, false>(a, nx, ny, 1, py, twy, false);  // rows
-	fft_lines<float2, false>(a, ny, 1, ny, px, twx, true);   // columns
+	fft_lines<float2, false>(a, nx, ld, 1, py, twy, false, true);  // rows
+	fft_lines<float2, false>(a, ny, 1, ld, px, twx, true);         // columns
 	// with several depths the spectrum is kept in global memory (L2) and
 	// reloaded per depth; the first depth works on it in place
 	float2* spec = spectra ? spectra + (long long)s * n2 : nullptr;
 	if (spec)
-		for (int q = threadIdx.x; q < n2; q += blockDim.x) spec[q] = a[q];
+		for (int q = threadIdx.x; q < n2; q += blockDim.x) spec[q] = a[(q / ny) * ld + q % ny];
 	// wnmax = 1 / min_k per axis; k-grid step ub / (n-1)
 	const double wx = 1.0 / kinfo[s * 4 + 0], wy = 1.0 / kinfo[s * 4 + 1];
 	const double dkx = wx / max(nx - 1, 1), dky = wy / max(ny - 1, 1);
@@ -599,14 +604,15 @@ velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, Ff
 		__syncthreads();  // the previous depth's output read a[]
 		for (int q = threadIdx.x; q < n2; q += blockDim.x) {
 			const double w = window_fixed(wix[q / ny], wiy[q % ny], nx, ny, dkx, dky, zs[iz], depth);
-			const float2 x = iz == 0 ? a[q] : spec[q];
-			a[q] = make_float2(float(x.x * w), float(x.y * w));
+			const int qa = (q / ny) * ld + q % ny;
+			const float2 x = iz == 0 ? a[qa] : spec[q];
+			a[qa] = make_float2(float(x.x * w), float(x.y * w));
 		}
 		__syncthreads();
-		fft_lines<float2, true>(a, ny, 1, ny, px, twx, true);
-		fft_lines<float2, true>(a, nx, ny, 1, py, twy, false);
+		fft_lines<float2, true>(a, ny, 1, ld, px, twx, true);
+		fft_lines<float2, true>(a, nx, ld, 1, py, twy, false, true);
 		float* out = S.out + (long long)iz * n2;
-		auto f = [&](int r, int c) -> double { return double(a[r * ny + c].x) * inv; };
+		auto f = [&](int r, int c) -> double { return double(a[r * ld + c].x) * inv; };
 		for (int q = threadIdx.x; q < n2; q += blockDim.x)
 			out[q] = float(finish_at(q / ny, q % ny, nx, ny, f));
 	}
@@ -649,18 +655,19 @@ vel_rows_fwd(const VelSlice<T>* __restrict__ sl, int nx, int ny, int R, FftPlan 
              typename C2<T>::type* __restrict__ A) {
 	using V = typename C2<T>::type;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	V* a = reinterpret_cast<V*>(smem_raw);  // R x ny
-	V* tw = a + R * ny;                     // ny
+	const int ld = ny + 1;                  // padded row stride
+	V* a = reinterpret_cast<V*>(smem_raw);  // R rows of ld
+	V* tw = a + R * ld;                     // ny
 	const long long n2 = (long long)nx * ny;
 	const VelSlice<T> S = sl[blockIdx.y];
 	const int r0 = blockIdx.x * R, rows = min(R, nx - r0);
 	make_twiddles(tw, ny);
 	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x)
-		a[q] = cpx(T(zeta_t(S, n2, (long long)r0 * ny + q)), T(0));
+		a[(q / ny) * ld + q % ny] = cpx(T(zeta_t(S, n2, (long long)r0 * ny + q)), T(0));
 	__syncthreads();
-	fft_lines<V, false>(a, rows, ny, 1, py, tw, false);
+	fft_lines<V, false>(a, rows, ld, 1, py, tw, false, true);
 	V* dst = A + blockIdx.y * n2 + (long long)r0 * ny;
-	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x) dst[q] = a[q];
+	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x) dst[q] = a[(q / ny) * ld + q % ny];
 }
 
 template <class T>
@@ -709,8 +716,9 @@ vel_rows_inv(const VelSlice<T>* __restrict__ sl, int nx, int ny, int R, int nz, 
              const typename C2<T>::type* __restrict__ B) {
 	using V = typename C2<T>::type;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	V* a = reinterpret_cast<V*>(smem_raw);  // (R + 1) x ny: the row above the band first
-	V* tw = a + (R + 1) * ny;               // ny
+	const int ld = ny + 1;                  // padded row stride
+	V* a = reinterpret_cast<V*>(smem_raw);  // R + 1 rows of ld: the row above the band first
+	V* tw = a + (R + 1) * ld;               // ny
 	const long long n2 = (long long)nx * ny;
 	const long long arr = blockIdx.y;  // slice * nz + depth
 	const int r0 = blockIdx.x * R, rows = min(R, nx - r0);
@@ -718,12 +726,12 @@ vel_rows_inv(const VelSlice<T>* __restrict__ sl, int nx, int ny, int R, int nz, 
 	const V* src = B + arr * n2;
 	for (int q = threadIdx.x; q < (rows + 1) * ny; q += blockDim.x) {
 		const int row = r0 - 1 + q / ny;
-		a[q] = row >= 0 ? src[(long long)row * ny + q % ny] : cpx(T(0), T(0));
+		a[(q / ny) * ld + q % ny] = row >= 0 ? src[(long long)row * ny + q % ny] : cpx(T(0), T(0));
 	}
 	__syncthreads();
-	fft_lines<V, true>(a, rows + 1, ny, 1, py, tw, false);
+	fft_lines<V, true>(a, rows + 1, ld, 1, py, tw, false, true);
 	const double inv = 1.0 / double(n2);
-	auto f = [&](int x, int y) -> double { return double(a[(x - r0 + 1) * ny + y].x) * inv; };
+	auto f = [&](int x, int y) -> double { return double(a[(x - r0 + 1) * ld + y].x) * inv; };
 	T* out = sl[arr / nz].out + (arr % nz) * n2 + (long long)r0 * ny;
 	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x)
 		out[q] = T(finish_at(r0 + q / ny, q % ny, nx, ny, f));
@@ -741,10 +749,10 @@ void velocity_general(Ctx* c, const VelSlice<T>* d_sl, int ns, int nx, int ny, c
 	const int CB = std::min(ny, std::max(1, budget / nx));
 	V* A = static_cast<V*>(scratch_take(c, sizeof(V) * n2 * ns));
 	V* B = static_cast<V*>(scratch_take(c, sizeof(V) * n2 * ns * nz));
-	const size_t s1 = sizeof(V) * (size_t(R) * ny + ny);
+	const size_t s1 = sizeof(V) * (size_t(R) * (ny + 1) + ny);
 	const size_t s2 = sizeof(V) * ((nz > 1 ? 2 : 1) * size_t(nx) * CB + nx) +
 	                  sizeof(int) * (size_t(nx) + ny);
-	const size_t s3 = sizeof(V) * (size_t(R + 1) * ny + ny);
+	const size_t s3 = sizeof(V) * (size_t(R + 1) * (ny + 1) + ny);
 	ARMA_CUDA_TRY(cudaFuncSetAttribute(vel_rows_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                                   int(s1)));
 	ARMA_CUDA_TRY(cudaFuncSetAttribute(vel_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -782,7 +790,7 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 	if (sizeof(T) == sizeof(float) && n2 <= kFuseMax) {
-		const size_t smem = sizeof(float2) * (size_t(n2) + nx + ny) + sizeof(int) * (nx + ny);
+		const size_t smem = sizeof(float2) * (size_t(nx) * (ny + 1) + nx + ny) + sizeof(int) * (nx + ny);
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(velocity_fused_kernel,
 		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
 		float2* spectra =
