@@ -161,7 +161,8 @@ __device__ __noinline__ void h_phase(const float* ss, const float* sh, const flo
 }
 
 template <int PY>
-__device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) {
+__device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned char* s_lo,
+                         int* err) {
 	const int tid = threadIdx.x;
 	const int grp = tid / GROUP;                 // 0 or 1: halves of the tap rows
 	const int lt = tid % GROUP;
@@ -189,6 +190,12 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 		const int j = q % PYP, ki = q / PYP;
 		sphi[q] = j < PY ? tk.phi[ki * PY + j] : 0.0f;
 		slo[q] = j < PY ? tk.phi_lo[ki * PY + j] : 0.0f;
+	}
+	// rows whose lo parts are all zero skip their second FMA chain
+	for (int ki = tid; ki < pt * px; ki += NTHREADS) {
+		bool nz = false;
+		for (int j = 0; j < PY; ++j) nz = nz || tk.phi_lo[ki * PY + j] != 0.0f;
+		s_lo[ki] = nz ? 1 : 0;
 	}
 	for (int q = tid; q < TX * TY; q += NTHREADS) {
 		sh[q] = tk.h[q];
@@ -256,7 +263,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 					win[4 * q + 2] = v.z;
 					win[4 * q + 3] = v.w;
 				}
-				float ph[PYP], pl[PYP];
+				float ph[PYP];
 #pragma unroll
 				for (int q = 0; q < PYP / 4; ++q) {
 					const float4 v = reinterpret_cast<const float4*>(prow + i * PYP)[q];
@@ -264,21 +271,35 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, int* err) 
 					ph[4 * q + 1] = v.y;
 					ph[4 * q + 2] = v.z;
 					ph[4 * q + 3] = v.w;
-					const float4 u = reinterpret_cast<const float4*>(lrow + i * PYP)[q];
-					pl[4 * q] = u.x;
-					pl[4 * q + 1] = u.y;
-					pl[4 * q + 2] = u.z;
-					pl[4 * q + 3] = u.w;
 				}
+				if (s_lo[k * px + i]) {  // warp-uniform: every thread handles this row
+					float pl[PYP];
 #pragma unroll
-				for (int r = 0; r < R; ++r) {
-					float p = 0.0f, q = 0.0f;
-#pragma unroll
-					for (int j = 0; j < PY; ++j) {
-						p = fmaf(ph[j], win[LH + r - j], p);
-						q = fmaf(pl[j], win[LH + r - j], q);
+					for (int q = 0; q < PYP / 4; ++q) {
+						const float4 u = reinterpret_cast<const float4*>(lrow + i * PYP)[q];
+						pl[4 * q] = u.x;
+						pl[4 * q + 1] = u.y;
+						pl[4 * q + 2] = u.z;
+						pl[4 * q + 3] = u.w;
 					}
-					kahan_add(s[r], c[r], p + q);
+#pragma unroll
+					for (int r = 0; r < R; ++r) {
+						float p = 0.0f, q = 0.0f;
+#pragma unroll
+						for (int j = 0; j < PY; ++j) {
+							p = fmaf(ph[j], win[LH + r - j], p);
+							q = fmaf(pl[j], win[LH + r - j], q);
+						}
+						kahan_add(s[r], c[r], p + q);
+					}
+				} else {
+#pragma unroll
+					for (int r = 0; r < R; ++r) {
+						float p = 0.0f;
+#pragma unroll
+						for (int j = 0; j < PY; ++j) p = fmaf(ph[j], win[LH + r - j], p);
+						kahan_add(s[r], c[r], p);
+					}
 				}
 			}
 		};
@@ -370,6 +391,7 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
              int* __restrict__ ticket_counter, int* __restrict__ err) {
 	extern __shared__ __align__(16) float smem[];
 	__shared__ int s_ticket;
+	__shared__ unsigned char s_lo[MAXO * (TX + 1)];  // per (k, i) tap row: lo part present
 	for (;;) {
 		if (threadIdx.x == 0) s_ticket = atomicAdd(ticket_counter, 1);
 		__syncthreads();
@@ -387,7 +409,7 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
 		const int local = ticket - tk.ticket_base;
 		const int bx = local / tk.tiles_y, by = local % tk.tiles_y;
 		switch (tk.py) {
-#define ARMA_PY_CASE(N) case N: run_tile<N>(tk, bx, by, smem, err); break;
+#define ARMA_PY_CASE(N) case N: run_tile<N>(tk, bx, by, smem, s_lo, err); break;
 			ARMA_PY_CASE(1) ARMA_PY_CASE(2) ARMA_PY_CASE(3) ARMA_PY_CASE(4) ARMA_PY_CASE(5)
 			ARMA_PY_CASE(6) ARMA_PY_CASE(7) ARMA_PY_CASE(8) ARMA_PY_CASE(9) ARMA_PY_CASE(10)
 			ARMA_PY_CASE(11) ARMA_PY_CASE(12) ARMA_PY_CASE(13)
