@@ -43,7 +43,7 @@ EXPORTS = (
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
     "arma_server_profile", "arma_velocity_linear_batch", "arma_validate_process",
-    "arma_poly_roots", "arma_ar_fit_choi",
+    "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf",
 )
 
 
@@ -194,6 +194,7 @@ def lib():
             "arma_validate_process": (i, [dp, ip, ip]),
             "arma_poly_roots": (i, [dp, i, dp, dp]),
             "arma_ar_fit_choi": (i, [dp, i, i, i, d, i, dp, ip, dp]),
+            "arma_driver_acf": (i, [vp, ip, dp, dp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -509,6 +510,14 @@ class Driver:
         out = np.empty(tuple(shape), np.float64)
         _check(lib().arma_driver_copy(self._h, what, _dp(out)))
         return out
+
+    def acf(self):
+        """(ACF table, grid step) of the model."""
+        shape, delta = (C.c_int * 3)(), (C.c_double * 3)()
+        _check(lib().arma_driver_acf(self._h, shape, delta, None))
+        out = np.empty(tuple(shape), np.float64)
+        _check(lib().arma_driver_acf(self._h, shape, delta, _dp(out)))
+        return out, tuple(delta)
 
     def zeta(self) -> np.ndarray:
         return self._copy(0, self.info()["shape"])

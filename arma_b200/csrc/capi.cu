@@ -930,6 +930,16 @@ int arma_driver_info(arma_driver* drv, int shape[3], double delta[3], int order[
 	});
 }
 
+int arma_driver_acf(arma_driver* drv, int shape[3], double delta[3], double* out) {
+	return guard([&] {
+		ARMA_REQUIRE(drv && shape && delta, ARMA_EINVAL, "null argument");
+		const double* data = nullptr;
+		driver_acf(drv->d, shape, delta, &data);
+		if (out && data)
+			std::memcpy(out, data, sizeof(double) * size_t(shape[0]) * shape[1] * shape[2]);
+	});
+}
+
 int arma_driver_copy(arma_driver* drv, int what, double* out) {
 	return guard([&] {
 		ARMA_REQUIRE(drv && out, ARMA_EINVAL, "null argument");

@@ -221,8 +221,10 @@ struct ArConfig {
 	double cdf_interval[2] = {0, 1};
 	double cdf_eps = 1e-6;
 	int cdf_iter = 100;
-	int acf_kind = -1;
+	int acf_kind = -1;      // analytic ACF (with `grid`)
 	Grid3 acf_grid;
+	bool acf_empirical = false;  // wave-group ACF (without `grid`)
+	EmpiricalAcf wave;
 	double amplitude = 1, velocity = 0, alpha[3] = {0, 0, 0}, beta[2] = {0, 0};
 	unsigned output = 0;
 	int order[3] = {0, 0, 0};
@@ -300,19 +302,67 @@ void read_ar(std::istream& in, ArConfig* c) {
 	     }},
 	    {"acf",
 	     [c](std::istream& s, const std::string& k) {
+		     // Without `grid` this is the reference's ACF_generator (a plain
+		     // wave group: func, amplitude, velocity, alpha, beta = wave
+		     // numbers, nwaves, shape; src/generator/acf_generator.cc:250-263);
+		     // with `grid` the analytic standing / propagating ACF of
+		     // ACF_wrapper (src/bits/acf_wrapper.cc:41-70).
 		     std::string func;
+		     bool has_grid = false, has_wave_keys = false;
+		     const double nan = std::numeric_limits<double>::quiet_NaN();
+		     double amp = nan, vel = nan, al[3] = {nan, nan, nan}, be[2] = {nan, nan};
+		     double nw[3] = {nan, nan, nan};
+		     int shp[3] = {-1, -1, -1};
 		     std::map<std::string, Reader> q = {
-		         {"grid", [c](std::istream& t, const std::string& kk) { read_grid(t, &c->acf_grid, kk); }},
+		         {"grid", [c, &has_grid](std::istream& t, const std::string& kk) {
+			          read_grid(t, &c->acf_grid, kk);
+			          has_grid = true;
+		          }},
 		         {"func", [&func](std::istream& t, const std::string&) { func = read_word(t); }},
-		         {"amplitude", number(&c->amplitude)},
-		         {"velocity", number(&c->velocity)},
-		         {"alpha", tuple<double, 3>(c->alpha)},
-		         {"beta", tuple<double, 2>(c->beta)},
+		         {"amplitude", number(&amp)},
+		         {"velocity", number(&vel)},
+		         {"alpha", tuple<double, 3>(al)},
+		         {"beta", tuple<double, 2>(be)},
+		         {"nwaves", [&](std::istream& t, const std::string& kk) {
+			          read_tuple<double, 3>(t, nw, kk);
+			          has_wave_keys = true;
+		          }},
+		         {"shape", [&](std::istream& t, const std::string& kk) {
+			          read_tuple<int, 3>(t, shp, kk);
+			          has_wave_keys = true;
+		          }},
 		     };
 		     read_params(s, q, true, k);
-		     if (func == "standing_wave") c->acf_kind = ARMA_ACF_STANDING;
-		     else if (func == "propagating_wave") c->acf_kind = ARMA_ACF_PROPAGATING;
-		     else throw Error{ARMA_EINVAL, "Bad ACF function name: \"" + func + "\""};
+		     auto pick = [](double v, double dflt) { return std::isnan(v) ? dflt : v; };
+		     if (has_grid) {
+			     if (has_wave_keys)
+				     throw Error{ARMA_EINVAL, "Bad \"acf\": grid with nwaves/shape"};
+			     c->amplitude = pick(amp, 1.0);
+			     c->velocity = pick(vel, 0.0);
+			     for (int i = 0; i < 3; ++i) c->alpha[i] = pick(al[i], 0.0);
+			     for (int i = 0; i < 2; ++i) c->beta[i] = pick(be[i], 0.0);
+			     if (func == "standing_wave") c->acf_kind = ARMA_ACF_STANDING;
+			     else if (func == "propagating_wave") c->acf_kind = ARMA_ACF_PROPAGATING;
+			     else throw Error{ARMA_EINVAL, "Bad ACF function name: \"" + func + "\""};
+		     } else {
+			     EmpiricalAcf& w = c->wave;
+			     if (func.empty() || func == "cos") w.func = 1;
+			     else if (func == "sin") w.func = 0;
+			     else if (func == "stokes") w.func = 2;
+			     else if (func == "standing_wave") w.func = 3;
+			     else throw Error{ARMA_EINVAL, "Invalid plain wave function: " + func};
+			     w.amplitude = pick(amp, 1.0);
+			     w.velocity = pick(vel, 1.0);
+			     for (int i = 0; i < 3; ++i) w.alpha[i] = pick(al[i], 0.06);
+			     w.wavenum[0] = pick(be[0], 0.8);
+			     w.wavenum[1] = pick(be[1], 0.0);
+			     for (int i = 0; i < 3; ++i) w.nwaves[i] = pick(nw[i], 1.5);
+			     for (int i = 0; i < 3; ++i) w.shape[i] = shp[i] < 0 ? 16 : shp[i];
+			     for (int i = 0; i < 3; ++i)
+				     if (w.shape[i] > 64) bad(k, "shape above 64");
+			     c->acf_empirical = true;
+			     c->acf_kind = -2;
+		     }
 	     }},
 	    {"output", [c](std::istream& s, const std::string& k) { c->output = read_flags(s, k); }},
 	    {"order", tuple<int, 3>(c->order)},
@@ -337,7 +387,7 @@ void read_ar(std::istream& in, ArConfig* c) {
 	read_params(in, p, true, "AR");
 	if (c->algorithm != "gauss_elimination" && c->algorithm != "choi_recursive")
 		throw Error{ARMA_EINVAL, "bad AR algorithm"};
-	if (c->acf_kind < 0) throw Error{ARMA_EINVAL, "Bad \"acf\": missing"};
+	if (c->acf_kind == -1) throw Error{ARMA_EINVAL, "Bad \"acf\": missing"};
 	for (int i = 0; i < 3; ++i)
 		if (c->out_grid.n[i] <= 0) bad("out_grid", "missing");
 }
@@ -381,6 +431,7 @@ struct Driver {
 	// results
 	std::vector<double> acf;
 	int acf_shape[3] = {0, 0, 0};
+	double acf_delta[3] = {1, 1, 1};
 	std::vector<double> phi;
 	double var_wn = 0;
 	int shape[3] = {0, 0, 0};
@@ -436,9 +487,14 @@ void parse_driver(std::istream& in, Driver* d) {
 // 56-66, src/generator/ar_model.cc:102-105).
 void finalise(Driver* d) {
 	ArConfig& a = d->ar;
-	for (int i = 0; i < 3; ++i) {
-		d->acf_shape[i] = a.acf_grid.n[i];
-		if (a.acf_grid.n[i] <= 0) bad("acf.grid", "missing");
+	if (a.acf_empirical) {  // the wave-group ACF is fixed by the configuration
+		d->acf = empirical_acf(a.wave, d->acf_shape, d->acf_delta);
+	} else {
+		for (int i = 0; i < 3; ++i) {
+			d->acf_shape[i] = a.acf_grid.n[i];
+			d->acf_delta[i] = a.acf_grid.delta(i);
+			if (a.acf_grid.n[i] <= 0) bad("acf.grid", "missing");
+		}
 	}
 	// all(order) == 0 in the reference: any zero component takes the ACF shape
 	if (a.order[0] == 0 || a.order[1] == 0 || a.order[2] == 0)
@@ -450,7 +506,7 @@ void finalise(Driver* d) {
 	// step is 2 pi times the ACF step
 	for (int i = 0; i < 3; ++i) {
 		d->shape[i] = a.out_grid.n[i];
-		d->delta[i] = a.acf_grid.delta(i) * kTwoPi;
+		d->delta[i] = d->acf_delta[i] * kTwoPi;
 	}
 }
 
@@ -459,10 +515,12 @@ void finalise(Driver* d) {
 // generate: ACF -> order -> grid rescale -> YW fit -> noise -> AR -> renorm -> NIT
 void driver_generate(Ctx* c, Driver* d) {
 	ArConfig& a = d->ar;
-	double adelta[3] = {a.acf_grid.delta(0), a.acf_grid.delta(1), a.acf_grid.delta(2)};
-	d->acf.resize(size_t(d->acf_shape[0]) * d->acf_shape[1] * d->acf_shape[2]);
-	acf_eval(a.acf_kind, a.amplitude, a.velocity, a.alpha, a.beta, adelta, d->acf_shape,
-	         d->acf.data());
+	double adelta[3] = {d->acf_delta[0], d->acf_delta[1], d->acf_delta[2]};
+	if (!a.acf_empirical) {
+		d->acf.resize(size_t(d->acf_shape[0]) * d->acf_shape[1] * d->acf_shape[2]);
+		acf_eval(a.acf_kind, a.amplitude, a.velocity, a.alpha, a.beta, adelta, d->acf_shape,
+		         d->acf.data());
+	}
 	// The reference NIT-transforms a copy of the ACF and discards it
 	// (src/generator/basic_arma_model.cc:74-79): the fit uses the Gaussian ACF.
 	if (a.algorithm == "choi_recursive") {
@@ -483,8 +541,12 @@ void driver_generate(Ctx* c, Driver* d) {
 	} else {
 		const int P0 = a.order[0] * a.order[1] * a.order[2];
 		d->phi.assign(P0, 0.0);
-		const int info = fit_analytic(a.acf_kind, a.amplitude, a.velocity, a.alpha, a.beta, adelta,
-		                              a.order, d->phi.data(), &d->var_wn);
+		const int info =
+		    a.acf_empirical
+		        ? fit_gauss_table(d->acf.data(), d->acf_shape, a.order, ARMA_FIT_CHOLESKY,
+		                          d->phi.data(), &d->var_wn)
+		        : fit_analytic(a.acf_kind, a.amplitude, a.velocity, a.alpha, a.beta, adelta, a.order,
+		                       d->phi.data(), &d->var_wn);
 		if (info != 0)
 			throw Error{ARMA_ENUMERIC, "Yule-Walker matrix is not positive definite"};
 	}
@@ -662,6 +724,14 @@ void driver_info(const Driver* d, int shape[3], double delta[3], int order[3], d
 		vshape[2] = d->vel.empty() ? 0 : d->shape[1];
 		vshape[3] = d->vel.empty() ? 0 : d->shape[2];
 	}
+}
+
+void driver_acf(const Driver* d, int shape[3], double delta[3], const double** data) {
+	for (int i = 0; i < 3; ++i) {
+		shape[i] = d->acf_shape[i];
+		delta[i] = d->acf_delta[i];
+	}
+	*data = d->acf.empty() ? nullptr : d->acf.data();
 }
 
 const double* driver_zeta(const Driver* d) { return d->zeta.empty() ? nullptr : d->zeta.data(); }

@@ -244,12 +244,27 @@ void driver_write(Driver* d, const std::string& dir);
 void driver_info(const Driver* d, int shape[3], double delta[3], int order[3], double* var_wn,
                  int vshape[4], unsigned* oflags);
 const double* driver_zeta(const Driver* d);
+void driver_acf(const Driver* d, int shape[3], double delta[3], const double** data);
 const double* driver_phi(const Driver* d);
 const double* driver_velocity_data(const Driver* d);
 
 // Inverse-CDF table for the NIT LUT path.
 void nit_build_lut(int dist, const double params[3], double stdev, int nodes,
                    double range, double* x0, double* dx, std::vector<double>& y);
+
+// The empirical ACF of a plain-wave group (acf_gen.cc): func 0 sin, 1 cos,
+// 2 stokes, 3 standing wave; wavenum = (kx, ky); shape = ACF shape (a zero
+// component selects the doubling search).  Returns the ACF table and its shape
+// and grid step.
+struct EmpiricalAcf {
+	int func = 1;
+	double amplitude = 1.0, velocity = 1.0;
+	double wavenum[2] = {0.8, 0.0};
+	double alpha[3] = {0.06, 0.06, 0.06};
+	double nwaves[3] = {1.5, 1.5, 1.5};
+	int shape[3] = {16, 16, 16};
+};
+std::vector<double> empirical_acf(const EmpiricalAcf& p, int shape[3], double delta[3]);
 
 // Choi's order-recursive Yule-Walker solver (choi.cc) on a cubic n^3 ACF:
 // 0 with phi (order[0] x order[1] x order[2]) and the solver's variance, 1 bad

@@ -254,7 +254,9 @@ int arma_poly_roots(const double* c, int n, double* re, double* im);
 /* ------------------------------------------------ programme layer */
 /* The reference's ARMA_driver (src/arma_driver.hh:43-150): parses a `.arma`
  * configuration (`model = AR {...}`, `velocity_potential_solver = linear
- * {...}`; the other registered names return ARMA_ENOTSUP), runs
+ * {...}`; the other registered names return ARMA_ENOTSUP; `acf = {...}`
+ * without `grid` is the reference's wave-group ACF_generator, with `grid` the
+ * analytic standing / propagating ACF), runs
  * generate_wavy_surface / compute_velocity_potentials on the device, and
  * writes zeta / zeta.csv / zeta.bin / phi / phi.csv like write_all
  * (src/arma_driver.cc:29-178).  Extensions: `seed`, `mt_file`,
@@ -273,6 +275,9 @@ int arma_driver_info(arma_driver* drv, int shape[3], double delta[3], int order[
                      double* var_wn, int vshape[4], unsigned* output_flags);
 /* Copies zeta (what = 0), phi coefficients (1) or velocity potentials (2). */
 int arma_driver_copy(arma_driver* drv, int what, double* out);
+/* The model's ACF table (available after open): its shape and grid step, and
+ * the values into out when out is not NULL. */
+int arma_driver_acf(arma_driver* drv, int shape[3], double delta[3], double* out);
 
 /* ------------------------------------------------ serving */
 /* No counterpart in the reference.  A server owns device-resident surface

@@ -10,6 +10,8 @@ registry (src/register_all.hh:47-68), the output grid rescaling
 """
 import math
 
+import numpy as np
+
 import pytest
 
 import arma_b200 as A
@@ -83,8 +85,10 @@ def test_order_larger_than_acf_rejected():
 
 
 def test_unknown_parameter():
+    e = err(config(acf="func = standing_wave\n\t\tgrid = (10,10,10)\n\t\twavelength = (1,2,3)"))
+    assert e.code == -1 and 'Unknown parameter: "wavelength"' in str(e)
     e = err(config(acf="func = standing_wave\n\t\tgrid = (10,10,10)\n\t\tnwaves = (1,2,3)"))
-    assert e.code == -1 and 'Unknown parameter: "nwaves"' in str(e)
+    assert e.code == -1 and "grid with nwaves" in str(e)
 
 
 def test_comments_and_blank_lines():
@@ -183,3 +187,62 @@ def test_cli_usage(capsys):
     assert main(["-h"]) == 0
     assert "usage:" in capsys.readouterr().out
     assert main([]) == 1
+
+
+# ----------------------------------------------------------------- wave-group ACF
+def wave_acf_numpy(func, amplitude, velocity, alpha, wavenum, nwaves, shape):
+    """The reference's ACF_generator restated with numpy (FFT-based circular
+    auto-covariance), src/generator/acf_generator.cc:132-244."""
+    n = [2 * s + 1 for s in shape]
+    ax = [np.linspace(-r, r, m) for r, m in zip(nwaves, n)]
+    t, x, y = np.meshgrid(*ax, indexing="ij")
+    kx, ky = wavenum
+    th = 2 * np.pi * (kx * x + ky * y - velocity * t)
+    if func == "sin":
+        w = amplitude * np.sin(th)
+    elif func == "cos":
+        w = amplitude * np.sin(th + 0.5 * np.pi)
+    elif func == "stokes":
+        st = 2 * np.pi * amplitude * np.hypot(kx, ky)
+        w = amplitude * (np.cos(th) + 0.5 * st * np.cos(2 * th) + 3 / 8 * st * st * np.cos(3 * th))
+    else:
+        w = amplitude * np.cos(2 * np.pi * (kx * x + ky * y)) * np.cos(2 * np.pi * velocity * t)
+    we = w * np.exp(-(np.abs(t * alpha[0]) + np.abs(x * alpha[1]) + np.abs(y * alpha[2])))
+    we *= np.sqrt(w.var(ddof=1) / we.var(ddof=1))
+    acf = np.fft.ifftn(np.abs(np.fft.fftn(we)) ** 2).real / we.size
+    h = [m // 2 for m in n]
+    return acf[:h[0], :h[1], :h[2]], tuple(r / (s - 1) for r, s in zip(nwaves, h))
+
+
+@pytest.mark.parametrize("func,amp,vel,alpha,beta,nwaves,shape", [
+    ("cos", 1.0, 1.0, (0.06, 0.06, 0.06), (0.8, 0.0), (1.5, 1.5, 1.5), (8, 8, 8)),
+    ("standing_wave", 3.0, 0.5, (2.0, 0.2, 1.0), (0.0625, 0.0), (1.85, 16.0, 1.0), (10, 12, 6)),
+    ("sin", 2.0, 0.3, (0.1, 0.1, 0.1), (0.3, 0.4), (2.0, 2.0, 2.0), (7, 9, 11)),
+    ("stokes", 0.5, 0.7, (0.05, 0.05, 0.05), (0.2, 0.1), (1.0, 1.5, 2.0), (6, 6, 6)),
+])
+def test_wave_group_acf_matches_numpy(func, amp, vel, alpha, beta, nwaves, shape):
+    acf_text = (f"func = {func}\n\t\tamplitude = {amp}\n\t\tvelocity = {vel}\n"
+                f"\t\talpha = ({alpha[0]},{alpha[1]},{alpha[2]})\n\t\tbeta = ({beta[0]},{beta[1]})\n"
+                f"\t\tnwaves = ({nwaves[0]},{nwaves[1]},{nwaves[2]})\n"
+                f"\t\tshape = ({shape[0]},{shape[1]},{shape[2]})")
+    d = A.Driver(config("\torder = (3,3,3)\n", acf=acf_text))
+    got, delta = d.acf()
+    ref, rdelta = wave_acf_numpy(func, amp, vel, alpha, beta, nwaves, shape)
+    assert got.shape == ref.shape == tuple(shape)
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+    assert delta == pytest.approx(rdelta, rel=1e-15)
+    # the output step is 2 pi times the ACF step (basic_arma_model.cc:62-66)
+    assert d.info()["delta"] == pytest.approx(tuple(2 * np.pi * v for v in rdelta), rel=1e-15)
+
+
+def test_wave_group_defaults_and_order():
+    """No keys at all: cos wave, 16^3 ACF; the order defaults to the ACF shape."""
+    d = A.Driver(config("", acf="func = cos"))
+    acf, delta = d.acf()
+    assert acf.shape == (16, 16, 16) and d.info()["order"] == (16, 16, 16)
+    assert delta == pytest.approx((1.5 / 15,) * 3)
+
+
+def test_wave_group_bad_function():
+    e = err(config(acf="func = square"))
+    assert e.code == -1 and "Invalid plain wave function: square" in str(e)

@@ -161,3 +161,48 @@ def test_driver_choi_default_algorithm(ctx, tmp_path):
     assert d.info()["var_wn"] == var
     zeta_ref = oracle_surface(phi, var, acf[0, 0, 0])
     assert np.abs(d.zeta() - zeta_ref).max() <= 1e-12 * np.abs(zeta_ref).max()
+
+
+def test_driver_wave_group_acf_end_to_end(ctx, tmp_path):
+    """The reference's default model set-up: a wave-group ACF (no `grid`),
+    Choi's solver, validate_process on, velocity on slices of non-power-of-two
+    sides.  The surface equals the oracle chain on the driver's coefficients
+    and the velocity equals the oracle solver."""
+    mt = write_mt(tmp_path / "mt.dat")
+    text = f"""model = AR {{
+	out_grid = (30,40,20)
+	acf = {{
+		func = standing_wave
+		amplitude = 2
+		alpha = (1.5,0.3,0.8)
+		velocity = 0.5
+		beta = (0.125,0)
+		nwaves = (1.5,4,1)
+		shape = (8,8,8)
+	}}
+	order = (4,4,4)
+	output = none
+	validate = 1
+	seed = 99
+	mt_file = {mt}
+}}
+velocity_potential_solver = linear {{
+	depth = 12
+	domain = from (5,-12) to (25,3) npoints (3,6)
+}}
+"""
+    d = A.Driver(text)
+    d.generate_wavy_surface(ctx)
+    acf, _ = d.acf()
+    phi, var = A.ar_fit_choi(acf, max_order=4)
+    np.testing.assert_array_equal(d.phi(), phi)
+    shape = (30, 40, 20)
+    eps = O.white_noise(O.mt19937_params(), 99, math.sqrt(var), int(np.prod(shape))).reshape(shape)
+    zeta_ref, _ = O.variance_renorm(O.ar_filter(eps, phi), acf[0, 0, 0])
+    zeta = d.zeta()
+    assert np.abs(zeta - zeta_ref).max() <= 1e-12 * np.abs(zeta_ref).max()
+    d.compute_velocity_potentials(ctx)
+    info = d.info()
+    zs = list(np.linspace(-12.0, 3.0, 6))
+    ref = O.velocity_linear(zeta, info["delta"], 12.0, zs, [5, 15, 25])
+    assert np.abs(d.velocity_potentials() - ref).max() <= 1e-9 * np.abs(ref).max()
