@@ -43,7 +43,7 @@ EXPORTS = (
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
     "arma_server_profile", "arma_velocity_linear_batch", "arma_validate_process",
-    "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf",
+    "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf", "arma_velocity_high_amplitude",
 )
 
 
@@ -195,6 +195,7 @@ def lib():
             "arma_poly_roots": (i, [dp, i, dp, dp]),
             "arma_ar_fit_choi": (i, [dp, i, i, i, d, i, dp, ip, dp]),
             "arma_driver_acf": (i, [vp, ip, dp, dp]),
+            "arma_velocity_high_amplitude": (i, [vp, vp, ip, i, dp, d, dp, i, ip, i, vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -398,14 +399,13 @@ class Context:
                                     lut_nodes, lut_range, n, precision, C.c_void_p(d_zeta)))
 
     def velocity_linear(self, d_zeta: int, shape, precision: int, delta, depth: float,
-                        z_levels, t_idx, d_out: int):
+                        z_levels, t_idx, d_out: int, high_amplitude: bool = False):
         dl, dlp = _d(delta)
         zs, zsp = _d(z_levels)
         ti = np.ascontiguousarray(t_idx, np.int32)
-        _check(lib().arma_velocity_linear(self._h, C.c_void_p(d_zeta), _i3(shape), precision,
-                                          dlp, depth, zsp, len(zs),
-                                          ti.ctypes.data_as(C.POINTER(C.c_int)), len(ti),
-                                          C.c_void_p(d_out)))
+        fn = lib().arma_velocity_high_amplitude if high_amplitude else lib().arma_velocity_linear
+        _check(fn(self._h, C.c_void_p(d_zeta), _i3(shape), precision, dlp, depth, zsp, len(zs),
+                  ti.ctypes.data_as(C.POINTER(C.c_int)), len(ti), C.c_void_p(d_out)))
 
     def velocity_linear_batch(self, jobs, nx: int, ny: int, precision: int, depth: float,
                               z_levels):

@@ -682,9 +682,10 @@ int arma_nit_apply(arma_ctx* ctx, int d, const double params[3], double stdev, i
 	});
 }
 
-int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3], int precision,
-                         const double delta[3], double depth, const double* z, int nz,
-                         const int* t_idx, int ntd, void* d_phi_out) {
+namespace {
+int velocity_call(arma_ctx* ctx, const void* d_zeta, const int shape[3], int precision,
+                  const double delta[3], double depth, const double* z, int nz, const int* t_idx,
+                  int ntd, void* d_phi_out, int mode) {
 	return guard([&] {
 		ARMA_REQUIRE(ctx && d_zeta && delta && z && t_idx && d_phi_out, ARMA_EINVAL,
 		             "null argument");
@@ -699,9 +700,25 @@ int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3], 
 		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
 		scratch_begin(&ctx->c, 0);
 		launch_velocity_linear(&ctx->c, d_zeta, shape, precision, delta, depth, z, nz, t_idx,
-		                       ntd, d_phi_out);
+		                       ntd, d_phi_out, mode);
 		ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
 	});
+}
+}  // namespace
+
+int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3], int precision,
+                         const double delta[3], double depth, const double* z, int nz,
+                         const int* t_idx, int ntd, void* d_phi_out) {
+	return velocity_call(ctx, d_zeta, shape, precision, delta, depth, z, nz, t_idx, ntd, d_phi_out,
+	                     0);
+}
+
+int arma_velocity_high_amplitude(arma_ctx* ctx, const void* d_zeta, const int shape[3],
+                                 int precision, const double delta[3], double depth,
+                                 const double* z, int nz, const int* t_idx, int ntd,
+                                 void* d_phi_out) {
+	return velocity_call(ctx, d_zeta, shape, precision, delta, depth, z, nz, t_idx, ntd, d_phi_out,
+	                     1);
 }
 
 int arma_velocity_linear_batch(arma_ctx* ctx, const arma_velocity_job* jobs, int n, int nx, int ny,

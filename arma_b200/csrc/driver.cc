@@ -452,7 +452,7 @@ const std::map<std::string, bool>& model_registry() {
 }
 const std::map<std::string, bool>& solver_registry() {
 	static const std::map<std::string, bool> m = {
-	    {"linear", true}, {"plain", false}, {"high_amplitude", false}, {"small_amplitude", false}};
+	    {"linear", true}, {"plain", false}, {"high_amplitude", true}, {"small_amplitude", false}};
 	return m;
 }
 
@@ -631,7 +631,8 @@ void driver_velocity(Ctx* c, Driver* d) {
 	double* dout = static_cast<double*>(scratch_take(c, n2 * tidx.size() * d->vel_z.size() * 8));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(dz, d->zeta.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
 	launch_velocity_linear(c, dz, d->shape, ARMA_FP64, d->delta, d->solver.depth, d->vel_z.data(),
-	                       int(d->vel_z.size()), tidx.data(), int(tidx.size()), dout);
+	                       int(d->vel_z.size()), tidx.data(), int(tidx.size()), dout,
+	                       d->solver_name == "high_amplitude" ? 1 : 0);
 	d->vel.resize(n2 * tidx.size() * d->vel_z.size());
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d->vel.data(), dout, d->vel.size() * 8, cudaMemcpyDeviceToHost,
 	                              c->stream));

@@ -198,10 +198,12 @@ void launch_nit_lut(Ctx* c, const double* d_lut_y, int nodes, double x0,
                     double dx, uint64_t n, int precision, void* d_zeta);
 
 // Velocity.
+// mode 0: the linear solver; mode 1: the high-amplitude solver (slopes from
+// delta[1], delta[2]).
 void launch_velocity_linear(Ctx* c, const void* d_zeta, const int shape[3],
                             int precision, const double delta[3], double depth,
                             const double* z, int nz, const int* t_idx, int ntd,
-                            void* d_out);
+                            void* d_out, int mode = 0);
 // Many surfaces of one slice shape nx x ny in one set of launches: surface k
 // has nt slices at zeta, its slices t_idx[0..ntd) go to out as (ntd, nz, nx,
 // ny); dt is its time step.
@@ -212,6 +214,8 @@ struct VelocitySurface {
 	const int* t_idx;
 	int ntd;
 	double dt;
+	int mode = 0;               // 0 linear, 1 high amplitude
+	double dx = 1.0, dy = 1.0;  // steps for the slopes of mode 1
 };
 void launch_velocity_linear_batch(Ctx* c, const VelocitySurface* v, int n, int nx, int ny,
                                   int precision, double depth, const double* z, int nz);

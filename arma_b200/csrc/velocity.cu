@@ -59,6 +59,8 @@ struct VelSlice {
 	T* out;         // this slice's output: nz planes of nx*ny
 	int nt, d;      // surface length, slice index
 	double dt;
+	int mode;        // 0 linear, 1 high amplitude
+	double dx, dy;   // grid steps for the slope terms of mode 1
 };
 
 // ---------------------------------------------------------------- 1. zeta_t
@@ -81,6 +83,45 @@ __device__ __forceinline__ double zeta_t(const VelSlice<T>& s, long long n2, lon
 		r = 0.5 * (double(f[(d + 1) * n2]) - double(f[(d - 1) * n2])) / s.dt;
 	}
 	return -r;
+}
+
+// d zeta / dx (axis 1) or d zeta / dy (axis 2) at point p of slice s, with
+// the same border rules (src/derivative.hh:8-73).
+template <class T>
+__device__ __forceinline__ double zeta_xy(const VelSlice<T>& s, int nx, int ny, long long p,
+                                          int axis) {
+	const T* f = s.zeta + (long long)s.d * nx * ny;
+	const int i = int(p / ny), j = int(p % ny);
+	const int n = axis == 1 ? nx : ny, k = axis == 1 ? i : j;
+	const double h = axis == 1 ? s.dx : s.dy;
+	auto at = [&](int kk) -> double {
+		return axis == 1 ? double(f[(long long)kk * ny + j]) : double(f[(long long)i * ny + kk]);
+	};
+	if (n - 1 < 2) return at(k);
+	if (k == 0) return 0.5 * (-at(2) + 4.0 * at(1) - 3.0 * at(0)) / h;
+	if (k == n - 1) return 0.5 * (3.0 * at(k) - 4.0 * at(k - 1) + at(k - 2)) / h;
+	return 0.5 * (at(k + 1) - at(k - 1)) / h;
+}
+
+// The solver's transformed input at point p: the linear solver's -zeta_t, or
+// the high-amplitude solver's d zeta/dt / (i ((zx + zy) / s - zx - zy) - 1/s)
+// with s = sqrt(1 + zx^2 + zy^2) (src/velocity/high_amplitude_solver.cc:7-23).
+template <class T>
+__device__ __forceinline__ void solver_input(const VelSlice<T>& s, int nx, int ny, long long p,
+                                             double& re, double& im) {
+	const long long n2 = (long long)nx * ny;
+	if (s.mode == 0) {
+		re = zeta_t(s, n2, p);
+		im = 0.0;
+		return;
+	}
+	const double rt = -zeta_t(s, n2, p);
+	const double zx = zeta_xy(s, nx, ny, p, 1), zy = zeta_xy(s, nx, ny, p, 2);
+	const double sq = sqrt(1.0 + zx * zx + zy * zy);
+	const double dr = -1.0 / sq, di = (zx + zy) / sq - zx - zy;
+	const double den = dr * dr + di * di;
+	re = rt * dr / den;
+	im = -rt * di / den;
 }
 
 // ---------------------------------------------------------------- 2. wnmax
@@ -587,7 +628,11 @@ velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, Ff
 	make_window_index(wix, px);
 	make_window_index(wiy, py);
 	for (int q = threadIdx.x; q < n2; q += blockDim.x)
-		a[(q / ny) * ld + q % ny] = make_float2(float(zeta_t(S, n2, q)), 0.0f);
+	{
+		double re, im;
+		solver_input(S, nx, ny, q, re, im);
+		a[(q / ny) * ld + q % ny] = make_float2(float(re), float(im));
+	}
 	__syncthreads();
 	fft_lines<float2, false>(a, nx, ld, 1, py, twy, false, true);  // rows
 	fft_lines<float2, false>(a, ny, 1, ld, px, twx, true);         // columns
@@ -663,7 +708,11 @@ vel_rows_fwd(const VelSlice<T>* __restrict__ sl, int nx, int ny, int R, FftPlan 
 	const int r0 = blockIdx.x * R, rows = min(R, nx - r0);
 	make_twiddles(tw, ny);
 	for (int q = threadIdx.x; q < rows * ny; q += blockDim.x)
-		a[(q / ny) * ld + q % ny] = cpx(T(zeta_t(S, n2, (long long)r0 * ny + q)), T(0));
+	{
+		double re, im;
+		solver_input(S, nx, ny, (long long)r0 * ny + q, re, im);
+		a[(q / ny) * ld + q % ny] = cpx(T(re), T(im));
+	}
 	__syncthreads();
 	fft_lines<V, false>(a, rows, ld, 1, py, tw, false, true);
 	V* dst = A + blockIdx.y * n2 + (long long)r0 * ny;
@@ -822,8 +871,8 @@ bool velocity_supported(int nx, int ny) {
 
 void launch_velocity_linear(Ctx* c, const void* d_zeta, const int shape[3], int precision,
                             const double delta[3], double depth, const double* z, int nz,
-                            const int* t_idx, int ntd, void* d_out) {
-	VelocitySurface v{d_zeta, d_out, shape[0], t_idx, ntd, delta[0]};
+                            const int* t_idx, int ntd, void* d_out, int mode) {
+	VelocitySurface v{d_zeta, d_out, shape[0], t_idx, ntd, delta[0], mode, delta[1], delta[2]};
 	launch_velocity_linear_batch(c, &v, 1, shape[1], shape[2], precision, depth, z, nz);
 }
 
@@ -837,7 +886,8 @@ void launch_velocity_linear_batch(Ctx* c, const VelocitySurface* v, int n, int n
 			for (int i = 0; i < v[k].ntd; ++i)
 				sl.push_back(VelSlice<double>{static_cast<const double*>(v[k].zeta),
 				                              static_cast<double*>(v[k].out) + (long long)i * nz * n2,
-				                              v[k].nt, v[k].t_idx[i], v[k].dt});
+				                              v[k].nt, v[k].t_idx[i], v[k].dt, v[k].mode, v[k].dx,
+				                              v[k].dy});
 		velocity_slices<double>(c, sl, nx, ny, depth, z, nz);
 	} else {
 		std::vector<VelSlice<float>> sl;
@@ -845,7 +895,8 @@ void launch_velocity_linear_batch(Ctx* c, const VelocitySurface* v, int n, int n
 			for (int i = 0; i < v[k].ntd; ++i)
 				sl.push_back(VelSlice<float>{static_cast<const float*>(v[k].zeta),
 				                             static_cast<float*>(v[k].out) + (long long)i * nz * n2,
-				                             v[k].nt, v[k].t_idx[i], v[k].dt});
+				                             v[k].nt, v[k].t_idx[i], v[k].dt, v[k].mode, v[k].dx,
+				                             v[k].dy});
 		velocity_slices<float>(c, sl, nx, ny, depth, z, nz);
 	}
 }

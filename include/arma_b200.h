@@ -183,6 +183,14 @@ int arma_velocity_linear(arma_ctx* ctx, const void* d_zeta, const int shape[3],
                          int precision, const double delta[3], double depth,
                          const double* z, int nz, const int* t_idx, int ntd,
                          void* d_phi_out);
+/* High_amplitude_solver (src/velocity/high_amplitude_solver.cc:7-23): the
+ * linear solver's pipeline on the complex input d zeta/dt / (i ((zx + zy)/s -
+ * zx - zy) - 1/s), s = sqrt(1 + zx^2 + zy^2), slopes zx, zy from delta[1],
+ * delta[2].  Same arguments as arma_velocity_linear. */
+int arma_velocity_high_amplitude(arma_ctx* ctx, const void* d_zeta, const int shape[3],
+                                 int precision, const double delta[3], double depth,
+                                 const double* z, int nz, const int* t_idx, int ntd,
+                                 void* d_phi_out);
 
 /* Many surfaces of one slice shape nx x ny in one set of launches (no
  * counterpart in the reference): job k reads nt slices at d_zeta and writes
@@ -253,8 +261,8 @@ int arma_poly_roots(const double* c, int n, double* re, double* im);
 
 /* ------------------------------------------------ programme layer */
 /* The reference's ARMA_driver (src/arma_driver.hh:43-150): parses a `.arma`
- * configuration (`model = AR {...}`, `velocity_potential_solver = linear
- * {...}`; the other registered names return ARMA_ENOTSUP; `acf = {...}`
+ * configuration (`model = AR {...}`, `velocity_potential_solver = linear |
+ * high_amplitude {...}`; the other registered names return ARMA_ENOTSUP; `acf = {...}`
  * without `grid` is the reference's wave-group ACF_generator, with `grid` the
  * analytic standing / propagating ACF), runs
  * generate_wavy_surface / compute_velocity_potentials on the device, and

@@ -94,6 +94,7 @@ def lib():
             "orc_window_function": (None, [i, i, d, d, d, d, _dp]),
             "orc_fft2": (None, [_dp, _dp, i, i, i]),
             "orc_velocity_linear": (None, [_dp, i, i, i, _dp, d, _dp, i, _ip, i, _dp, i]),
+            "orc_velocity_solve": (None, [i, _dp, i, i, i, _dp, d, _dp, i, _ip, i, _dp, i]),
             "orc_write_zeta_bin": (i, [C.c_char_p, _dp, sz]),
             "orc_write_zeta_csv": (i, [C.c_char_p, _dp, i, i, i, _dp]),
         }
@@ -319,6 +320,17 @@ def velocity_linear(zeta, delta, depth, z_levels, t_idx, nthreads=0):
     out = np.empty((len(ti), len(zs)) + zeta.shape[1:], np.float64)
     lib().orc_velocity_linear(_d(zeta), *zeta.shape, _d(dl), depth, _d(zs), len(zs),
                               ti.ctypes.data_as(_ip), len(ti), _d(out), nthreads)
+    return out
+
+
+def velocity_high_amplitude(zeta, delta, depth, z_levels, t_idx, nthreads=0):
+    zeta = _f64(zeta)
+    zs = _f64(z_levels)
+    ti = np.ascontiguousarray(t_idx, np.int32)
+    dl = _f64(delta)
+    out = np.empty((len(ti), len(zs)) + zeta.shape[1:], np.float64)
+    lib().orc_velocity_solve(1, _d(zeta), *zeta.shape, _d(dl), depth, _d(zs), len(zs),
+                             ti.ctypes.data_as(_ip), len(ti), _d(out), nthreads)
     return out
 
 

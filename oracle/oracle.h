@@ -135,6 +135,9 @@ void orc_velocity_linear(const double* zeta, int nt, int nx, int ny,
                          const double delta[3], double depth,
                          const double* z, int nz, const int* t_idx, int ntd,
                          double* out /* ntd*nz*nx*ny */, int nthreads);
+void orc_velocity_solve(int mode, const double* zeta, int nt, int nx, int ny,
+                        const double delta[3], double depth, const double* zs, int nz,
+                        const int* t_idx, int ntd, double* out, int nthreads);
 
 /* ---- O1: output layout (src/arma_driver.cc:29-69) ---- */
 int orc_write_zeta_bin(const char* path, const double* zeta, size_t n);

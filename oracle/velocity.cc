@@ -221,21 +221,55 @@ extern "C" void orc_fft2(double* re, double* im, int nx, int ny, int sign) {
 	for (size_t i = 0; i < a.size(); ++i) { re[i] = a[i].real(); im[i] = a[i].imag(); }
 }
 
+// d zeta / dx (axis 1) or d zeta / dy (axis 2) of slice it, with the
+// reference's one-sided differences at the borders and the slice itself when
+// the axis has fewer than three points (src/derivative.hh:8-73).
+static void derivative_xy(const double* zeta, int nx, int ny, int it, int axis, double d,
+                          double* out) {
+	const double* f = zeta + size_t(it) * nx * ny;
+	const int n = axis == 1 ? nx : ny;
+	for (int i = 0; i < nx; ++i)
+		for (int j = 0; j < ny; ++j) {
+			const int k = axis == 1 ? i : j;
+			auto at = [&](int kk) {
+				return axis == 1 ? f[size_t(kk) * ny + j] : f[size_t(i) * ny + kk];
+			};
+			double r;
+			if (n - 1 < 2) r = at(k);
+			else if (k == 0) r = 0.5 * (-at(2) + 4.0 * at(1) - 3.0 * at(0)) / d;
+			else if (k == n - 1) r = 0.5 * (3.0 * at(k) - 4.0 * at(k - 1) + at(k - 2)) / d;
+			else r = 0.5 * (at(k + 1) - at(k - 1)) / d;
+			out[size_t(i) * ny + j] = r;
+		}
+}
+
 // Reference: src/velocity/basic_solver.cc:38-77 and 95-112 with the
-// Linear_solver hooks (src/velocity/linear_solver.cc:39-121).  t_idx holds the
-// integer slice indices that the reference obtains by truncating the domain's
-// t coordinates; z holds the depth levels.
-extern "C" void orc_velocity_linear(const double* zeta, int nt, int nx, int ny,
-                                    const double delta[3], double depth,
-                                    const double* zs, int nz, const int* t_idx,
-                                    int ntd, double* out, int nthreads) {
+// Linear_solver hooks (src/velocity/linear_solver.cc:39-121); mode 1 swaps in
+// High_amplitude_solver::precompute (src/velocity/high_amplitude_solver.cc:
+// 7-23), whose transformed input is the complex
+//     d zeta/dt / (i ((zx + zy) / s - zx - zy) - 1 / s),  s = sqrt(1 + zx^2 + zy^2).
+// t_idx holds the integer slice indices that the reference obtains by
+// truncating the domain's t coordinates; z holds the depth levels.
+extern "C" void orc_velocity_solve(int mode, const double* zeta, int nt, int nx, int ny,
+                                   const double delta[3], double depth, const double* zs, int nz,
+                                   const int* t_idx, int ntd, double* out, int nthreads) {
 	if (nthreads <= 0) nthreads = omp_get_max_threads();
 	const size_t N = size_t(nx) * ny;
-	std::vector<double> zt(N);
+	std::vector<double> zt(N), zx(N), zy(N);
+	std::vector<cplx> zc(N);
 	for (int i = 0; i < ntd; ++i) {
 		const int it = t_idx[i];
 		orc_derivative_t(zeta, nt, nx, ny, delta[0], it, zt.data());
-		for (size_t p = 0; p < N; ++p) zt[p] = -zt[p];
+		if (mode == 1) {
+			derivative_xy(zeta, nx, ny, it, 1, delta[1], zx.data());
+			derivative_xy(zeta, nx, ny, it, 2, delta[2], zy.data());
+			for (size_t p = 0; p < N; ++p) {
+				const double sq = std::sqrt(1.0 + zx[p] * zx[p] + zy[p] * zy[p]);
+				zc[p] = zt[p] / cplx(-1.0 / sq, (zx[p] + zy[p]) / sq - zx[p] - zy[p]);
+			}
+		} else {
+			for (size_t p = 0; p < N; ++p) zc[p] = cplx(-zt[p], 0.0);
+		}
 		double kmin[2], kmax[2];
 		// factor_waves(slice, int(t coordinate), dt)
 		const int tcoord = int(delta[0] * it);
@@ -245,8 +279,7 @@ extern "C" void orc_velocity_linear(const double* zeta, int nt, int nx, int ny,
 		for (int j = 0; j < nz; ++j) {
 			std::vector<double> w(N);
 			orc_window_function(nx, ny, wx, wy, zs[j], depth, w.data());
-			std::vector<cplx> a(N);
-			for (size_t p = 0; p < N; ++p) a[p] = cplx(zt[p], 0.0);
+			std::vector<cplx> a(zc);
 			fft2(a.data(), nx, ny, -1);
 			for (size_t p = 0; p < N; ++p) a[p] *= w[p];
 			fft2(a.data(), nx, ny, +1);
@@ -259,4 +292,10 @@ extern "C" void orc_velocity_linear(const double* zeta, int nt, int nx, int ny,
 				res[l] = interp(res, ny, 1, l - 1, 1, l, 2, l - 1, 0, l);
 		}
 	}
+}
+
+extern "C" void orc_velocity_linear(const double* zeta, int nt, int nx, int ny,
+                                    const double delta[3], double depth, const double* zs, int nz,
+                                    const int* t_idx, int ntd, double* out, int nthreads) {
+	orc_velocity_solve(0, zeta, nt, nx, ny, delta, depth, zs, nz, t_idx, ntd, out, nthreads);
 }

@@ -102,7 +102,7 @@ def test_registered_models_not_built(name):
     assert e.code == -8 and name in str(e)
 
 
-@pytest.mark.parametrize("name", ["plain", "high_amplitude", "small_amplitude"])
+@pytest.mark.parametrize("name", ["plain", "small_amplitude"])
 def test_registered_solvers_not_built(name):
     e = err(config(solver_name=name))
     assert e.code == -8 and name in str(e)
@@ -246,3 +246,7 @@ def test_wave_group_defaults_and_order():
 def test_wave_group_bad_function():
     e = err(config(acf="func = square"))
     assert e.code == -1 and "Invalid plain wave function: square" in str(e)
+
+
+def test_high_amplitude_solver_is_built():
+    A.Driver(config(solver_name="high_amplitude"))

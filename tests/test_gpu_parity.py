@@ -345,3 +345,28 @@ def test_velocity_mixed_radix_vs_oracle(ctx, shape, depth, zs):
                             out.data_ptr())
         got = out.cpu().numpy().astype(np.float64)
         assert np.abs(got - ref).max() <= tol * scale, (prec, np.abs(got - ref).max() / scale)
+
+
+@pytest.mark.parametrize("shape,depth,zs,amp", [
+    ((8, 32, 24), 12.0, [0.0, -2.0], 1.0),
+    ((6, 20, 30), np.inf, [0.0], 3.0),       # steep: slopes of order one
+    ((4, 200, 100), np.inf, [0.0, -1.0], 2.0),
+])
+def test_velocity_high_amplitude_vs_oracle(ctx, shape, depth, zs, amp):
+    """High_amplitude_solver: the complex slope-corrected input through the
+    same window and FFTs; FP64 within 1e-9 and FP32 within 2e-4 of max|phi|,
+    with non-unit grid steps for the slopes."""
+    phi, var = A.ar_fit_analytic(A.ACF_STANDING, (3, 3, 3), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    eps = O.white_noise(O.mt19937_params(), 8, np.sqrt(var), int(np.prod(shape))).reshape(shape)
+    zeta = amp * O.ar_filter(eps, phi)
+    delta = (0.5, 0.8, 1.25)
+    tidx = list(range(shape[0]))
+    ref = O.velocity_high_amplitude(zeta, delta, depth, zs, tidx)
+    scale = np.abs(ref).max()
+    for prec, dt, tol in [(A.FP64, torch.float64, 1e-9), (A.FP32C, torch.float32, 2e-4)]:
+        z = dev(zeta, dt)
+        out = torch.zeros(ref.shape, dtype=dt, device="cuda")
+        ctx.velocity_linear(z.data_ptr(), shape, prec, delta, depth, zs, tidx, out.data_ptr(),
+                            high_amplitude=True)
+        got = out.cpu().numpy().astype(np.float64)
+        assert np.abs(got - ref).max() <= tol * scale, (prec, np.abs(got - ref).max() / scale)
