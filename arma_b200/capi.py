@@ -44,6 +44,7 @@ EXPORTS = (
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
     "arma_server_profile", "arma_velocity_linear_batch", "arma_validate_process",
     "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf", "arma_velocity_high_amplitude",
+    "arma_ma_fit", "arma_ma_filter", "arma_ma_generate",
 )
 
 
@@ -196,6 +197,9 @@ def lib():
             "arma_ar_fit_choi": (i, [dp, i, i, i, d, i, dp, ip, dp]),
             "arma_driver_acf": (i, [vp, ip, dp, dp]),
             "arma_velocity_high_amplitude": (i, [vp, vp, ip, i, dp, d, dp, i, ip, i, vp]),
+            "arma_ma_fit": (i, [dp, ip, ip, dp, dp, ip]),
+            "arma_ma_filter": (i, [vp, dp, ip, ip, i, vp, vp]),
+            "arma_ma_generate": (i, [vp, C.POINTER(Surface), i, i]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -268,6 +272,18 @@ def ar_fit_choi(acf, max_order=None, determine_order=True, var_epsilon=1e-6, cho
                                   1 if chop else 0, _dp(buf), order, C.byref(var)))
     shape = tuple(order)
     return buf[:int(np.prod(shape))].reshape(shape).copy(), var.value
+
+
+def ma_fit(acf, order):
+    """MA coefficients by fixed-point iteration: (theta, var_wn, iterations),
+    theta of shape `order` with theta[0, 0, 0] = -1."""
+    acf = np.ascontiguousarray(acf, np.float64)
+    theta = np.zeros(tuple(order))
+    var = C.c_double()
+    it = C.c_int()
+    _check(lib().arma_ma_fit(_dp(acf), _i3(acf.shape), _i3(order), _dp(theta), C.byref(var),
+                             C.byref(it)))
+    return theta, var.value, it.value
 
 
 def validate_process(phi) -> int:
@@ -420,6 +436,20 @@ class Context:
         zs, zsp = _d(z_levels)
         _check(lib().arma_velocity_linear_batch(self._h, arr, len(jobs), nx, ny, precision, depth,
                                                 zsp, len(zs)))
+
+    def ma_filter(self, theta, shape, precision: int, d_eps: int, d_zeta: int):
+        """zeta = eps - sum_{m != 0} theta(m) eps(n - m) on device buffers."""
+        theta = np.ascontiguousarray(theta, np.float64)
+        _check(lib().arma_ma_filter(self._h, _dp(theta), _i3(theta.shape), _i3(shape), precision,
+                                    C.c_void_p(d_eps), C.c_void_p(d_zeta)))
+
+    def ma_generate(self, surfaces, precision: int):
+        """Noise + MA filter + renormalisation; each surface's phi holds theta."""
+        arr = (Surface * len(surfaces))(*surfaces)
+        _check(lib().arma_ma_generate(self._h, arr, len(surfaces), precision))
+        for k, s in enumerate(surfaces):
+            s.scale = arr[k].scale
+        return [arr[k].scale for k in range(len(surfaces))]
 
     def batch_generate(self, surfaces, precision: int, host: bool = False):
         arr = (Surface * len(surfaces))(*surfaces)

@@ -2,12 +2,15 @@
 
     python -m arma_b200.cases velocity --side 128 --slices 400 --nz 4 [--fp64]
     python -m arma_b200.cases ar --side 256 --slices 256 --order 8 [--surfaces 8]
+    python -m arma_b200.cases ma --side 256 --slices 256 --order 20,10,10 [--fp64]
 
 `velocity` generates one propagating-wave surface (order 10^3, FP32
 compensated) of `slices` x side x side and times the linear velocity solver
 on every slice at nz depth levels in {0, -1, -2, -4, ...}, infinite depth.
 `ar` times the batched FP32 AR path on `surfaces` standing-wave surfaces of
-the given shape and order.  Each prints one line with the per-call device
+the given shape and order.  `ma` times the MA filter (zeta = eps - theta * eps)
+of one surface on unit normal noise with random coefficients of the given
+order.  Each prints one line with the per-call device
 time (CUDA events, three warm-up calls, five timed calls).
 """
 from __future__ import annotations
@@ -76,6 +79,27 @@ def ar_case(args):
     ctx.close()
 
 
+def ma_case(args):
+    import torch
+    import arma_b200 as A
+    ctx = A.Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    shape = (args.slices, args.side, args.side)
+    order = tuple(int(v) for v in args.order.split(","))
+    rng = np.random.default_rng(1)
+    theta = rng.normal(0.0, 0.2 / np.sqrt(np.prod(order)), order)
+    prec, dt = (A.FP64, torch.float64) if args.fp64 else (A.FP32C, torch.float32)
+    eps = torch.randn(shape, dtype=dt, device="cuda")
+    z = torch.empty_like(eps)
+    ms = _timed(ctx, stream, lambda: ctx.ma_filter(theta, shape, prec, eps.data_ptr(), z.data_ptr()))
+    pts = int(np.prod(shape))
+    flop = pts * 2.0 * int(np.prod(order))
+    print(f"ma {shape} order {order} {'fp64' if args.fp64 else 'fp32'}: {ms:.3f} ms/call, "
+          f"{pts / ms / 1e6:.2f} G points/s, {flop / ms / 1e9:.2f} TFLOP/s algorithmic")
+    ctx.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m arma_b200.cases")
     sub = ap.add_subparsers(dest="case", required=True)
@@ -89,8 +113,13 @@ def main(argv=None):
     a.add_argument("--slices", type=int, default=256)
     a.add_argument("--order", type=int, default=8)
     a.add_argument("--surfaces", type=int, default=8)
+    m = sub.add_parser("ma")
+    m.add_argument("--side", type=int, default=256)
+    m.add_argument("--slices", type=int, default=256)
+    m.add_argument("--order", default="20,10,10")
+    m.add_argument("--fp64", action="store_true")
     args = ap.parse_args(argv)
-    (velocity_case if args.case == "velocity" else ar_case)(args)
+    {"velocity": velocity_case, "ar": ar_case, "ma": ma_case}[args.case](args)
 
 
 if __name__ == "__main__":

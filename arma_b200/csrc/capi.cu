@@ -749,6 +749,9 @@ int arma_velocity_linear_batch(arma_ctx* ctx, const arma_velocity_job* jobs, int
 // ---------------------------------------------------------------- batches
 namespace {
 
+void renorm_surfaces(Ctx* c, arma_surface* s, int n, int precision, const std::vector<void*>& dz,
+                     bool host);
+
 void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 	const size_t es = elem_size(precision);
 	std::vector<void*> dz(n);
@@ -781,6 +784,14 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 		check_device_error(c);
 	}
+	renorm_surfaces(c, s, n, precision, dz, host);
+}
+
+// The variance renormalisation of each surface with acf0 > 0 (and the copy to
+// the host buffers when `host`), then the scales back into s[k].scale.
+void renorm_surfaces(Ctx* c, arma_surface* s, int n, int precision, const std::vector<void*>& dz,
+                     bool host) {
+	const size_t es = elem_size(precision);
 	double* d_scale = static_cast<double*>(scratch_take(c, sizeof(double) * n));
 	std::vector<RenormSpec> rs;
 	for (int k = 0; k < n; ++k)
@@ -802,6 +813,27 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 	for (int k = 0; k < n; ++k) s[k].scale = s[k].acf0 > 0.0 ? sc[k] : 1.0;
 }
 
+// White noise into scratch, the MA filter into each surface's buffer, then the
+// renormalisation (MA_model::do_generate, src/generator/ma_model.cc:30-40).
+void ma_batch(Ctx* c, arma_surface* s, int n, int precision) {
+	const size_t es = elem_size(precision);
+	std::vector<void*> eps(n), dz(n);
+	for (int k = 0; k < n; ++k) {
+		require_shape(s[k].shape, "out_grid");
+		require_shape(s[k].order, "order");
+		require_mt(&s[k].mt);
+		ARMA_REQUIRE(s[k].phi && s[k].d_zeta, ARMA_EINVAL, "null surface buffer");
+		ARMA_REQUIRE(s[k].var_wn >= 0.0, ARMA_EINVAL, "variance is less than zero");
+		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
+		eps[k] = scratch_take(c, np * es);
+		dz[k] = s[k].d_zeta;
+	}
+	white_noise_batch(c, s, n, precision, eps);
+	for (int k = 0; k < n; ++k)
+		launch_ma_filter(c, s[k].phi, s[k].order, s[k].shape, precision, eps[k], dz[k]);
+	renorm_surfaces(c, s, n, precision, dz, false);
+}
+
 }  // namespace
 
 }  // extern "C"
@@ -809,6 +841,9 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 namespace armab {
 void batch_generate_device(Ctx* c, arma_surface* s, int n, int precision) {
 	batch(c, s, n, precision, false);
+}
+void ma_generate_device(Ctx* c, arma_surface* s, int n, int precision) {
+	ma_batch(c, s, n, precision);
 }
 }  // namespace armab
 
@@ -878,6 +913,53 @@ int arma_validate_process(const double* phi, const int order[3], int* bad_roots)
 			throw Error{ARMA_EINVAL,
 			            "AR/MA process is not stationary/invertible: some roots lie inside unit "
 			            "circle or on its borderline."};
+	});
+}
+
+// ---------------------------------------------------------------- M
+int arma_ma_fit(const double* acf, const int acf_shape[3], const int order[3],
+                double* theta_out, double* var_wn, int* iterations) {
+	return guard([&] {
+		ARMA_REQUIRE(acf && acf_shape && order && theta_out && var_wn, ARMA_EINVAL,
+		             "null argument");
+		require_shape(acf_shape, "acf");
+		std::vector<double> theta;
+		double var = 0.0;
+		int it = 0;
+		const int rc = ma_fit_fixed_point(acf, acf_shape, order, MaFitOptions{}, &theta, &var, &it,
+		                                  nullptr);
+		if (rc == 1) throw Error{ARMA_EINVAL, "bad order"};
+		if (rc == 2) throw Error{ARMA_ENUMERIC, "bad MA model coefficients"};
+		if (rc == 3) throw Error{ARMA_ENUMERIC, "bad white noise variance"};
+		std::copy(theta.begin(), theta.end(), theta_out);
+		*var_wn = var;
+		if (iterations) *iterations = it;
+	});
+}
+
+int arma_ma_filter(arma_ctx* ctx, const double* theta, const int order[3], const int shape[3],
+                   int precision, const void* d_eps, void* d_zeta) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && theta && order && shape && d_eps && d_zeta, ARMA_EINVAL,
+		             "null argument");
+		require_shape(shape, "out_grid");
+		require_shape(order, "order");
+		const size_t bytes = size_t(shape[0]) * shape[1] * shape[2] * elem_size(precision);
+		const char* e = static_cast<const char*>(d_eps);
+		const char* z = static_cast<const char*>(d_zeta);
+		ARMA_REQUIRE(e + bytes <= z || z + bytes <= e, ARMA_EINVAL, "eps and zeta overlap");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		launch_ma_filter(&ctx->c, theta, order, shape, precision, d_eps, d_zeta);
+	});
+}
+
+int arma_ma_generate(arma_ctx* ctx, arma_surface* surfaces, int n, int precision) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && surfaces && n > 0, ARMA_EINVAL, "bad argument");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		ma_batch(&ctx->c, surfaces, n, precision);
 	});
 }
 

@@ -211,6 +211,7 @@ unsigned read_flags(std::istream& in, const std::string& key) {
 }
 
 struct ArConfig {
+	bool ma = false;  // model = MA (else AR)
 	Grid3 out_grid;
 	bool no_seed = false;
 	bool has_seed = false;
@@ -384,9 +385,14 @@ void read_ar(std::istream& in, ArConfig* c) {
 		     else bad(k, w);
 	     }},
 	};
-	read_params(in, p, true, "AR");
-	if (c->algorithm != "gauss_elimination" && c->algorithm != "choi_recursive")
+	read_params(in, p, true, c->ma ? "MA" : "AR");
+	if (c->ma) {
+		// MA_algorithm names (src/ma_algorithm.cc:7-21)
+		if (c->algorithm != "fixed_point_iteration" && c->algorithm != "newton_raphson")
+			throw Error{ARMA_EINVAL, "Invalid MA algorithm: " + c->algorithm};
+	} else if (c->algorithm != "gauss_elimination" && c->algorithm != "choi_recursive") {
 		throw Error{ARMA_EINVAL, "bad AR algorithm"};
+	}
 	if (c->acf_kind == -1) throw Error{ARMA_EINVAL, "Bad \"acf\": missing"};
 	for (int i = 0; i < 3; ++i)
 		if (c->out_grid.n[i] <= 0) bad("out_grid", "missing");
@@ -447,7 +453,7 @@ namespace {
 // does not build report ARMA_ENOTSUP (src/register_all.hh:47-68).
 const std::map<std::string, bool>& model_registry() {
 	static const std::map<std::string, bool> m = {
-	    {"AR", true}, {"MA", false}, {"ARMA", false}, {"plain_wave", false}, {"LH", false}};
+	    {"AR", true}, {"MA", true}, {"ARMA", false}, {"plain_wave", false}, {"LH", false}};
 	return m;
 }
 const std::map<std::string, bool>& solver_registry() {
@@ -465,6 +471,10 @@ void parse_driver(std::istream& in, Driver* d) {
 		     if (it == model_registry().end()) throw Error{ARMA_EINVAL, "bad object"};
 		     if (!it->second)
 			     throw Error{ARMA_ENOTSUP, "model \"" + d->model_name + "\" is not built"};
+		     if (d->model_name == "MA") {
+			     d->ar.ma = true;
+			     d->ar.algorithm = "fixed_point_iteration";
+		     }
 		     read_ar(s, &d->ar);
 	     }},
 	    {"velocity_potential_solver",
@@ -501,7 +511,7 @@ void finalise(Driver* d) {
 		for (int i = 0; i < 3; ++i) a.order[i] = d->acf_shape[i];
 	for (int i = 0; i < 3; ++i)
 		if (a.order[i] <= 0 || a.order[i] > d->acf_shape[i])
-			throw Error{ARMA_EINVAL, "bad AR model order"};
+			throw Error{ARMA_EINVAL, a.ma ? "bad order" : "bad AR model order"};
 	// output grid lengths := acf.delta * npatches * 2 pi, i.e. the output
 	// step is 2 pi times the ACF step
 	for (int i = 0; i < 3; ++i) {
@@ -512,7 +522,8 @@ void finalise(Driver* d) {
 
 }  // namespace
 
-// generate: ACF -> order -> grid rescale -> YW fit -> noise -> AR -> renorm -> NIT
+// generate: ACF -> order -> grid rescale -> fit (AR: Yule-Walker, MA: fixed
+// point) -> noise -> AR or MA filter -> renorm -> NIT
 void driver_generate(Ctx* c, Driver* d) {
 	ArConfig& a = d->ar;
 	double adelta[3] = {d->acf_delta[0], d->acf_delta[1], d->acf_delta[2]};
@@ -523,7 +534,18 @@ void driver_generate(Ctx* c, Driver* d) {
 	}
 	// The reference NIT-transforms a copy of the ACF and discards it
 	// (src/generator/basic_arma_model.cc:74-79): the fit uses the Gaussian ACF.
-	if (a.algorithm == "choi_recursive") {
+	if (a.ma) {
+		// MA_model::determine_coefficients / fixed_point_iteration
+		// (src/generator/ma_model.cc:96-107, 153-163)
+		if (a.algorithm != "fixed_point_iteration")
+			throw Error{ARMA_ENOTSUP, "only fixed_point_iteration is supported"};
+		const int rc = ma_fit_fixed_point(d->acf.data(), d->acf_shape, a.order, MaFitOptions{},
+		                                  &d->phi, &d->var_wn, nullptr, nullptr);
+		if (rc == 1) throw Error{ARMA_EINVAL, "bad order"};
+		if (rc == 2) throw Error{ARMA_ENUMERIC, "bad MA model coefficients"};
+		if (rc == 3) throw Error{ARMA_ENUMERIC, "bad white noise variance"};
+		d->var_wn = ma_white_noise_variance(d->acf.data(), d->phi.data(), a.order);
+	} else if (a.algorithm == "choi_recursive") {
 		// determine_coefficients_choi (src/generator/ar_model.cc:136-152): the
 		// order-recursive solver on the ACF table, maximum order max(order),
 		// variance tolerance 1e-6, chopped; the model's order replaces the
@@ -590,7 +612,8 @@ void driver_generate(Ctx* c, Driver* d) {
 	s.mt = mt;
 	s.seed = seed;
 	s.d_zeta = dz;
-	batch_generate_device(c, &s, 1, a.precision);
+	if (a.ma) ma_generate_device(c, &s, 1, a.precision);
+	else batch_generate_device(c, &s, 1, a.precision);
 	if (a.nit) {
 		launch_nit_bisection(c, a.nit_dist, a.nit_params, std::sqrt(d->acf[0]), a.cdf_interval[0],
 		                     a.cdf_interval[1], a.cdf_eps, a.cdf_iter, n, a.precision, dz);

@@ -237,6 +237,8 @@ void intra_slice_response(const double* phi, const int order[3], int tx, int ty,
                           double* h);
 // White noise + AR filter (+ renormalisation) into device buffers (capi.cu).
 void batch_generate_device(Ctx* c, arma_surface* s, int n, int precision);
+// The MA form: s[k].phi holds theta (noise, MA filter, renormalisation).
+void ma_generate_device(Ctx* c, arma_surface* s, int n, int precision);
 
 // The `.arma` programme layer (driver.cc).
 struct Driver;
@@ -287,6 +289,27 @@ int poly_roots(const double* c, int n, std::vector<std::complex<double>>& roots)
 // validate_process on the flattened phi (P coefficients): 0 stationary, 3 with
 // *bad_roots roots of modulus <= 1, or poly_roots' failure code.
 int validate_ar_process(const double* phi, int P, int* bad_roots);
+
+// MA coefficients by fixed-point iteration (ma_fit.cc), the solver's defaults
+// (src/generator/ma_coefficient_solver.hh:27-40).
+struct MaFitOptions {
+	int max_iterations = 1000;
+	double max_residual = 1e-5;
+	double min_var_wn = 1e-6;
+	double eps = 1e-5;
+};
+// 0 with theta (order box, theta(0,0,0) = -1) and var_wn; 1 order outside the
+// ACF; 2 non-finite coefficients; 3 white-noise variance at or below the
+// minimum (*var_out holds it).
+int ma_fit_fixed_point(const double* acf, const int acf_shape[3], const int order[3],
+                       const MaFitOptions& opt, std::vector<double>* theta_out, double* var_out,
+                       int* iterations, double* residual_out);
+// acf(0,0,0) / sum theta^2 (src/arma.cc:73-79).
+double ma_white_noise_variance(const double* acf, const double* theta, const int order[3]);
+// zeta = eps - sum_{m != 0} theta(m) eps(n - m) on the device (ma.cu); eps and
+// zeta must not overlap.
+void launch_ma_filter(Ctx* c, const double* theta, const int order[3], const int shape[3],
+                      int precision, const void* d_eps, void* d_zeta);
 
 // Polar attempts generated for n normals: the expected count plus 8 sigma,
 // times `margin` (capi.cu).

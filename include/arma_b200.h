@@ -259,6 +259,32 @@ int arma_validate_process(const double* phi, const int order[3], int* bad_roots)
  * re/im (n-1 each), as gsl_poly_complex_solve. */
 int arma_poly_roots(const double* c, int n, double* re, double* im);
 
+/* ------------------------------------------------ M: moving-average model */
+/* MA coefficients by fixed-point iteration: replaces
+ * MA_coefficient_solver::solve_fixed_point_iteration
+ * (src/generator/ma_coefficient_solver.cc:36-139) with its defaults
+ * (max_iterations 1000, max_residual 1e-5, min white-noise variance 1e-6,
+ * variance tolerance 1e-5; src/generator/ma_coefficient_solver.hh:27-40).
+ * acf has acf_shape (t,x,y) values; order <= acf_shape per axis.  theta_out
+ * receives order[0]*order[1]*order[2] doubles with theta(0,0,0) = -1;
+ * var_wn = acf(0,0,0) / sum theta^2 (src/arma.cc:73-79); iterations may be
+ * NULL.  ARMA_EINVAL "bad order"; ARMA_ENUMERIC "bad MA model coefficients"
+ * (non-finite) or "bad white noise variance" (at or below 1e-6). */
+int arma_ma_fit(const double* acf, const int acf_shape[3], const int order[3],
+                double* theta_out, double* var_wn, int* iterations);
+/* The MA filter on device buffers of `precision`: zeta = eps - sum over
+ * m != 0 of theta(m) eps(n - m), zero history; replaces
+ * MA_model::generate_surface (src/generator/ma_model.cc:42-61, FFT
+ * convolution with K = -theta, K(0,0,0) = 1).  theta is host, order-box
+ * sized (theta(0,0,0) is ignored); d_eps and d_zeta must not overlap. */
+int arma_ma_filter(arma_ctx* ctx, const double* theta, const int order[3],
+                   const int shape[3], int precision, const void* d_eps, void* d_zeta);
+/* White noise + MA filter (+ renormalisation) for n surfaces, as
+ * arma_batch_generate with surfaces[k].phi holding theta: MA_model::do_generate
+ * (src/generator/ma_model.cc:30-40) followed by the variance renormalisation
+ * of Basic_ARMA_model::generate (src/generator/basic_arma_model.cc:98-103). */
+int arma_ma_generate(arma_ctx* ctx, arma_surface* surfaces, int n, int precision);
+
 /* ------------------------------------------------ programme layer */
 /* The reference's ARMA_driver (src/arma_driver.hh:43-150): parses a `.arma`
  * configuration (`model = AR {...}`, `velocity_potential_solver = linear |

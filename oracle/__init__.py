@@ -78,6 +78,8 @@ def lib():
             "orc_white_noise": (None, [C.POINTER(MtParams), u32, d, sz, _dp]),
             "orc_white_noise_words": (sz, [C.POINTER(MtParams), u32, sz]),
             "orc_ar_filter": (None, [_dp, i, i, i, _dp, i, i, i]),
+            "orc_ma_fit": (i, [_dp, i, i, i, i, i, i, _dp, _dp, _ip]),
+            "orc_ma_filter": (None, [_dp, i, i, i, _dp, i, i, i, _dp]),
             "orc_ar_filter_f32": (None, [_fp, i, i, i, _fp, i, i, i]),
             "orc_ar_generate_omp": (i, [_dp, i, i, i, _dp, i, i, i, i,
                                         C.POINTER(MtParams), i, _u32p, d, i, _ip]),
@@ -205,6 +207,67 @@ def ar_filter(zeta, phi):
     phi = _f64(phi)
     lib().orc_ar_filter(_d(z), *z.shape, _d(phi), *phi.shape)
     return z
+
+
+# ---------------------------------------------------------------- MA model
+def ma_fit(acf_arr, order):
+    """Fixed-point MA fit: (status, theta, var_wn, iterations)."""
+    a = _f64(acf_arr)
+    theta = np.zeros(tuple(order))
+    var = C.c_double()
+    it = C.c_int()
+    rc = lib().orc_ma_fit(_d(a), *a.shape, *order, _d(theta), C.byref(var), C.byref(it))
+    return rc, theta, var.value, it.value
+
+
+def ma_filter(eps, theta):
+    """Direct MA sum (src/test/convolution-test.cc:17-50)."""
+    e = _f64(eps)
+    th = _f64(theta)
+    z = np.empty_like(e)
+    lib().orc_ma_filter(_d(th), *th.shape, _d(e), *e.shape, _d(z))
+    return z
+
+
+def ma_block_shape(signal_shape, kernel_shape, parallelism=2):
+    """Convolution::get_block_shape (src/apmath/convolution.hh:146-161) with the
+    non-OpenMP parallelism of 2."""
+    s = np.asarray(signal_shape)
+    k = np.asarray(kernel_shape)
+    g1 = np.minimum(s, 4 * k)
+    g2 = np.maximum(k, s // parallelism)
+    return tuple(int(v) for v in np.minimum(g1, g2) + np.abs(g1 - g2) // 2)
+
+
+def ma_convolve_fft(eps, theta, parallelism=2):
+    """The reference's production MA form: FFT overlap-add of the noise with K =
+    -theta, K(0,0,0) = 1, blocks of Convolution::get_block_shape zero-padded by
+    the kernel's shape, each block's linear convolution added back at its
+    offset and truncated to the surface (src/apmath/convolution.hh:58-130,
+    src/generator/ma_model.cc:42-61).  Complex FP64 numpy FFTs."""
+    e = _f64(eps)
+    kern = -_f64(theta).astype(np.complex128)
+    kern[0, 0, 0] = 1.0
+    bs = np.asarray(ma_block_shape(e.shape, kern.shape, parallelism))
+    pad = np.asarray(kern.shape)
+    if np.any(kern.shape > bs) or np.any(bs > np.asarray(e.shape)):
+        raise ValueError("bad block size")
+    full = tuple(int(v) for v in bs + pad)
+    kf = np.fft.fftn(kern, full)
+    lim = np.asarray(e.shape)
+    nparts = -(-lim // bs)
+    out = np.zeros(e.shape, np.complex128)
+    for idx in np.ndindex(*nparts):
+        off = np.asarray(idx) * bs
+        to = np.minimum(lim, off + bs)
+        part = np.zeros(full, np.complex128)
+        part[tuple(slice(0, int(t - o)) for o, t in zip(off, to))] = \
+            e[tuple(slice(int(o), int(t)) for o, t in zip(off, to))]
+        res = np.fft.ifftn(np.fft.fftn(part) * kf)
+        hi = np.minimum(to + pad, lim)
+        out[tuple(slice(int(o), int(h)) for o, h in zip(off, hi))] += \
+            res[tuple(slice(0, int(h - o)) for o, h in zip(off, hi))]
+    return out.real
 
 
 def ar_filter_f32(zeta, phi):

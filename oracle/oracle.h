@@ -144,6 +144,14 @@ int orc_write_zeta_bin(const char* path, const double* zeta, size_t n);
 int orc_write_zeta_csv(const char* path, const double* zeta, int nt, int nx,
                        int ny, const double delta[3]);
 
+/* ---- M: moving-average model (ma.cc) ---- */
+/* fixed-point MA fit: 0 ok, 1 bad order, 2 non-finite, 3 variance <= 1e-6 */
+int orc_ma_fit(const double* acf, int at, int ax, int ay, int pt, int px, int py,
+               double* theta, double* var_wn, int* iterations);
+/* direct MA sum zeta = eps - sum_{m != 0} theta(m) eps(n - m) */
+void orc_ma_filter(const double* theta, int pt, int px, int py, const double* eps, int nt,
+                   int nx, int ny, double* zeta);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,7 +96,7 @@ def test_comments_and_blank_lines():
     assert A.Driver(text).info()["order"] == (3, 3, 3)
 
 
-@pytest.mark.parametrize("name", ["MA", "ARMA", "plain_wave", "LH"])
+@pytest.mark.parametrize("name", ["ARMA", "plain_wave", "LH"])
 def test_registered_models_not_built(name):
     e = err(config(model=name))
     assert e.code == -8 and name in str(e)
