@@ -22,7 +22,11 @@
 // The coefficients are carried as hi + lo float pairs (rounding phi to one
 // float perturbs a high-gain recursion far more than FP32 summation does):
 // each (k,i) row of taps is two FP32 FMA chains over one register window, and
-// row totals are combined with Kahan compensation; H likewise.  Tiles are handed out through a global ticket
+// row totals are combined with Kahan compensation.  H is applied in plain
+// FP32 with Kahan-added partial sums: it acts once per slice on the current
+// slice alone, and its rounding changes the surface by far less than phi's
+// (a lo part for H moved the RMS error by under 1e-7 at 18 % of the filter's
+// time).  Tiles are handed out through a global ticket
 // counter in dependency order, so a CTA only ever waits on tiles that are
 // already owned by running CTAs.
 #include <algorithm>
@@ -54,8 +58,7 @@ struct Task {
 	float* zeta;
 	const float* phi;     // hi part, pt*px*py
 	const float* phi_lo;  // lo part: phi - hi, pt*px*py
-	const float* h;       // hi part of the intra-slice response, TX*TY
-	const float* h_lo;
+	const float* h;       // intra-slice response, TX*TY
 	int* flags;
 };
 
@@ -106,8 +109,8 @@ __device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need
 // (xl, yl0 .. yl0+R-1), dx restricted to [dx_lo, min(dx_hi, xl+1)): writes the
 // Kahan-compensated partial strip to out[0..R).  Shared by every tap-count
 // instantiation of run_tile, so its code exists once.
-__device__ __noinline__ void h_phase(const float* ss, const float* sh, const float* shl, int xl,
-                                     int yl0, int dx_lo, int dx_hi, float* out) {
+__device__ __noinline__ void h_phase(const float* ss, const float* sh, int xl, int yl0, int dx_lo,
+                                     int dx_hi, float* out) {
 	float a[R], ac[R];
 #pragma unroll
 	for (int r = 0; r < R; ++r) { a[r] = 0.0f; ac[r] = 0.0f; }
@@ -115,7 +118,6 @@ __device__ __noinline__ void h_phase(const float* ss, const float* sh, const flo
 	for (int dx = dx_lo; dx <= dx_end; ++dx) {
 		const float* srow = ss + (xl - dx) * SW + SPAD;
 		const float* hrow = sh + dx * TY;
-		const float* hlrow = shl + dx * TY;
 		for (int dy0 = 0; dy0 <= yl0; dy0 += R) {
 			// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
 			float w[2 * R];
@@ -128,9 +130,8 @@ __device__ __noinline__ void h_phase(const float* ss, const float* sh, const flo
 				w[4 * q + 2] = v.z;
 				w[4 * q + 3] = v.w;
 			}
-			float hv[R], hl[R];
+			float hv[R];
 			const float4* hp = reinterpret_cast<const float4*>(hrow + dy0);
-			const float4* hq = reinterpret_cast<const float4*>(hlrow + dy0);
 #pragma unroll
 			for (int q = 0; q < R / 4; ++q) {
 				const float4 v = hp[q];
@@ -138,21 +139,13 @@ __device__ __noinline__ void h_phase(const float* ss, const float* sh, const flo
 				hv[4 * q + 1] = v.y;
 				hv[4 * q + 2] = v.z;
 				hv[4 * q + 3] = v.w;
-				const float4 u = hq[q];
-				hl[4 * q] = u.x;
-				hl[4 * q + 1] = u.y;
-				hl[4 * q + 2] = u.z;
-				hl[4 * q + 3] = u.w;
 			}
 #pragma unroll
 			for (int r = 0; r < R; ++r) {
-				float p = 0.0f, q = 0.0f;
+				float p = 0.0f;
 #pragma unroll
-				for (int dd = 0; dd < R; ++dd) {
-					p = fmaf(hv[dd], w[R + r - dd], p);
-					q = fmaf(hl[dd], w[R + r - dd], q);
-				}
-				kahan_add(a[r], ac[r], p + q);
+				for (int dd = 0; dd < R; ++dd) p = fmaf(hv[dd], w[R + r - dd], p);
+				kahan_add(a[r], ac[r], p);
 			}
 		}
 	}
@@ -179,9 +172,8 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 	float* ring = smem;                          // pt slots
 	float* sphi = ring + pt * slot_sz;           // pt*px*PYP (hi)
 	float* slo = sphi + pt * px * PYP;           // pt*px*PYP (lo)
-	float* sh = slo + pt * px * PYP;             // TX*TY (hi)
-	float* shl = sh + TX * TY;                   // TX*TY (lo)
-	float* ss = shl + TX * TY;                   // TX*SW
+	float* sh = slo + pt * px * PYP;             // TX*TY
+	float* ss = sh + TX * TY;                    // TX*SW
 	float* comb = ss + TX * SW;                  // GROUP*R: group 1 partials
 	float* hres = comb + GROUP * R;              // NTHREADS*R: H-phase partials
 
@@ -197,10 +189,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 		for (int j = 0; j < PY; ++j) nz = nz || tk.phi_lo[ki * PY + j] != 0.0f;
 		s_lo[ki] = nz ? 1 : 0;
 	}
-	for (int q = tid; q < TX * TY; q += NTHREADS) {
-		sh[q] = tk.h[q];
-		shl[q] = tk.h_lo[q];
-	}
+	for (int q = tid; q < TX * TY; q += NTHREADS) sh[q] = tk.h[q];
 	for (int q = tid; q < pt * slot_sz; q += NTHREADS) ring[q] = 0.0f;
 	for (int q = tid; q < TX * SW; q += NTHREADS) ss[q] = 0.0f;
 	__syncthreads();
@@ -362,7 +351,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 		__syncthreads();
 
 		//    zeta = H * S over the quarter plane of the tile
-		h_phase(ss, sh, shl, xl, yl0, dx_lo, dx_hi, hres + tid * R);
+		h_phase(ss, sh, xl, yl0, dx_lo, dx_hi, hres + tid * R);
 
 		// 5. store the solved slice and publish it
 		__syncthreads();
@@ -423,7 +412,7 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
 size_t smem_bytes(int pt, int px, int py) {
 	const int rows = TX + px - 1;
 	const int pyp = (py + 3) & ~3;
-	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + 2 * TX * TY + TX * SW +
+	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + TX * TY + TX * SW +
 	                        GROUP * R + NTHREADS * R);
 }
 
@@ -465,7 +454,7 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 		t.t0 = s.t0;
 		t.tiles_x = s.tiles_x; t.tiles_y = s.tiles_y;
 		t.ticket_base = total;
-		t.zeta = s.zeta; t.phi = s.phi; t.phi_lo = s.phi_lo; t.h = s.h; t.h_lo = s.h_lo;
+		t.zeta = s.zeta; t.phi = s.phi; t.phi_lo = s.phi_lo; t.h = s.h;
 		t.flags = flags + foff;
 		foff += size_t(s.tiles_x) * s.tiles_y;
 		total += s.tiles_x * s.tiles_y;
@@ -531,7 +520,7 @@ constexpr size_t kOffErr = 260;
 constexpr size_t kOffFlags = 512;
 constexpr size_t kOffPhi = kOffFlags + sizeof(int) * kStaticMaxTiles;
 constexpr size_t kOffH = kOffPhi + 2 * sizeof(float) * kStaticMaxTaps;
-constexpr size_t kStaticEnd = kOffH + 2 * sizeof(float) * TX * TY;
+constexpr size_t kStaticEnd = kOffH + sizeof(float) * TX * TY;
 static_assert(kStaticEnd <= kStaticScratchBytes, "static scratch layout overflows");
 static_assert(sizeof(Task) <= kOffTicket, "task record overflows its slot");
 
@@ -584,11 +573,8 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 	// host-side tables on the stack
 	double h[TX * TY];
 	intra_slice_response(phi, order, TX, TY, h);
-	float hbuf[2 * TX * TY];
-	for (int i = 0; i < TX * TY; ++i) {
-		hbuf[i] = float(h[i]);
-		hbuf[TX * TY + i] = float(h[i] - double(hbuf[i]));
-	}
+	float hbuf[TX * TY];
+	for (int i = 0; i < TX * TY; ++i) hbuf[i] = float(h[i]);
 	float pbuf[2 * kStaticMaxTaps];
 	for (int i = 0; i < P; ++i) {
 		pbuf[i] = float(phi[i]);
@@ -604,7 +590,6 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 	t.phi = d_phi;
 	t.phi_lo = d_phi + P;
 	t.h = d_h;
-	t.h_lo = d_h + TX * TY;
 	t.flags = reinterpret_cast<int*>(base + kOffFlags);
 	int* d_ticket = reinterpret_cast<int*>(base + kOffTicket);
 	int* d_err = reinterpret_cast<int*>(base + kOffErr);

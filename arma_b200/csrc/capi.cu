@@ -504,7 +504,7 @@ int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed, doub
 namespace armab {
 
 size_t ar32_coefficient_count(const int order[3]) {
-	return 2 * size_t(order[0]) * order[1] * order[2] + 2 * size_t(ar32c_tile_x()) * ar32c_tile_y();
+	return 2 * size_t(order[0]) * order[1] * order[2] + size_t(ar32c_tile_x()) * ar32c_tile_y();
 }
 
 void ar32_coefficients(const double* phi, const int order[3], float* b) {
@@ -543,10 +543,7 @@ void ar32_coefficients(const double* phi, const int order[3], float* b) {
 			}
 		}
 	}
-	for (size_t i = 0; i < nh; ++i) {
-		b[2 * P + i] = float(h[i]);
-		b[2 * P + nh + i] = float(h[i] - double(b[2 * P + i]));
-	}
+	for (size_t i = 0; i < nh; ++i) b[2 * P + i] = float(h[i]);
 }
 
 }  // namespace armab
@@ -561,10 +558,8 @@ std::vector<Ar32Surface> ar32_surfaces(Ctx* c, int n, const double* const* phis,
                                        const int* const* orders, const int* const* shapes,
                                        float* const* zetas) {
 	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
-	const size_t nh = size_t(tx) * ty;
 	std::vector<size_t> off(n + 1, 0);
-	for (int k = 0; k < n; ++k)
-		off[k + 1] = off[k] + 2 * size_t(orders[k][0]) * orders[k][1] * orders[k][2] + 2 * nh;
+	for (int k = 0; k < n; ++k) off[k + 1] = off[k] + ar32_coefficient_count(orders[k]);
 	std::vector<float> buf(off[n]);
 	for (int k = 0; k < n; ++k) ar32_coefficients(phis[k], orders[k], buf.data() + off[k]);
 	float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
@@ -586,7 +581,6 @@ std::vector<Ar32Surface> ar32_surfaces(Ctx* c, int n, const double* const* phis,
 		s.phi = dk;
 		s.phi_lo = dk + P;
 		s.h = dk + 2 * P;
-		s.h_lo = dk + 2 * P + nh;
 		s.tiles_x = (s.nx + tx - 1) / tx;
 		s.tiles_y = (s.ny + ty - 1) / ty;
 	}

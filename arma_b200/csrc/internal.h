@@ -167,8 +167,7 @@ struct Ar32Surface {
 	float* zeta;           // device, in place (noise in, surface out)
 	const float* phi;      // device, pt*px*py, hi part of the FP64 coefficients
 	const float* phi_lo;   // device, pt*px*py, phi - hi
-	const float* h;        // device, intra-slice impulse response (TX*TY), hi
-	const float* h_lo;     // device, lo part of h
+	const float* h;        // device, intra-slice impulse response (TX*TY)
 	int tiles_x, tiles_y;  // spatial tile grid
 	int t0 = 0;            // slices [0, t0) hold a finished history (streams)
 };
@@ -316,7 +315,7 @@ void launch_ma_filter(Ctx* c, const double* theta, const int order[3], const int
 uint64_t noise_attempts(size_t n, double margin);
 void require_mt(const arma_mt_params* p);
 // The FP32 tile kernel's coefficient block of one surface: phi hi, phi lo,
-// H hi, H lo (ar32_coefficient_count floats).
+// H (ar32_coefficient_count floats).
 size_t ar32_coefficient_count(const int order[3]);
 void ar32_coefficients(const double* phi, const int order[3], float* out);
 

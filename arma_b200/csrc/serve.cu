@@ -417,7 +417,6 @@ uint64_t arma_server::launch(Slot& sl) {
 		StreamState* st = sl.reqs[k].st;
 		const int cur = int(sl.reqs[k].chunk & 1);
 		const size_t P = size_t(st->pt) * st->px * st->py;
-		const size_t nh = size_t(tx) * ty;
 		Ar32Surface& a = as[k];
 		const bool first = sl.reqs[k].chunk == 0;
 		a.nt = first ? T : st->H + T;
@@ -431,7 +430,6 @@ uint64_t arma_server::launch(Slot& sl) {
 		a.phi = st->coef_d;
 		a.phi_lo = st->coef_d + P;
 		a.h = st->coef_d + 2 * P;
-		a.h_lo = st->coef_d + 2 * P + nh;
 		a.tiles_x = (st->nx + tx - 1) / tx;
 		a.tiles_y = (st->ny + ty - 1) / ty;
 	}
