@@ -7,18 +7,22 @@
 // depends on earlier points of its own time slice as well as on the previous
 // pt-1 slices.  The work is split into spatial tiles of TX x TY points; one
 // CTA owns one tile of one surface for all t and walks the slices in order.
-// For slice t it
-//   1. accumulates the terms on slices t-1 .. t-pt+1 (90% of the work for a
+// For slice t its four compute warps
+//   1. accumulate the terms on slices t-1 .. t-pt+1 (90% of the work for a
 //      10^3 model) from a shared-memory ring that holds those slices for the
 //      tile plus its west/north halo,
-//   2. waits for the three neighbour tiles (x-1, y-1, both) to publish slice t
-//      (a per-tile counter in global memory; bounded spin),
-//   3. loads slice t of the halo and adds the current-slice terms that reach
-//      into it (the in-tile part of the current slice is held at zero),
-//   4. solves the remaining in-tile recursion zeta = S + A0 zeta exactly as a
+//   2.-3. meanwhile a fifth warp publishes slice t-1, clears the ring slot of
+//      slice t, waits for the three neighbour tiles (x-1, y-1, both) to
+//      publish slice t (a per-tile counter in global memory; bounded spin)
+//      and loads slice t of the halo; then the compute warps add the
+//      current-slice terms that reach into the halo (the in-tile part of the
+//      current slice is held at zero),
+//   4. solve the remaining in-tile recursion zeta = S + A0 zeta exactly as a
 //      quarter-plane convolution zeta = H * S, where H is the impulse response
 //      of 1 / (1 - A0(z1,z2)) on the tile (precomputed in FP64),
-//   5. stores the slice to the ring and to global memory and publishes it.
+//   5. store the slice to the ring and to global memory; the fifth warp
+//      publishes it (release store after a fence) off the compute warps'
+//      critical path.
 // The coefficients are carried as hi + lo float pairs (rounding phi to one
 // float perturbs a high-gain recursion far more than FP32 summation does):
 // each (k,i) row of taps is two FP32 FMA chains over one register window, and
@@ -42,7 +46,12 @@ constexpr int TY = 32;            // tile columns (y)
 constexpr int R = 8;              // outputs per thread along y
 constexpr int STRIPS = TY / R;    // threads per tile row
 constexpr int GROUP = TX * STRIPS; // threads covering the tile once
-constexpr int NTHREADS = 2 * GROUP; // two groups split the tap rows
+constexpr int NCOMP = 2 * GROUP;   // compute threads: two groups split the tap rows
+constexpr int NTHREADS = NCOMP + 32; // plus the halo / publication warp
+// named barriers (0 is __syncthreads)
+constexpr int BAR_HALO = 1;        // halo warp -> compute: slot t cleared, halo of t loaded
+constexpr int BAR_COMP = 2;        // compute threads among themselves
+constexpr int BAR_DONE = 3;        // compute -> halo warp: slice t stored
 constexpr int LH = 12;            // left (y) halo columns held in the ring
 constexpr int W = LH + TY;        // ring row width (floats)
 constexpr int SPAD = TY + 8;      // zero padding left of each S row
@@ -72,6 +81,14 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
 __device__ __forceinline__ void cp_async16(float* dst_smem, const float* src) {
 	const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst_smem));
 	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void bar_sync(int id, int n) {
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void bar_arrive(int id, int n) {
+	asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
 
 __device__ __forceinline__ void cp_async_wait_all() {
@@ -175,7 +192,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 	float* sh = slo + pt * px * PYP;             // TX*TY
 	float* ss = sh + TX * TY;                    // TX*SW
 	float* comb = ss + TX * SW;                  // GROUP*R: group 1 partials
-	float* hres = comb + GROUP * R;              // NTHREADS*R: H-phase partials
+	float* hres = comb + GROUP * R;              // NCOMP*R: H-phase partials
 
 	// stage coefficients (rows padded with zeros), H, zero the ring and S pads
 	for (int q = tid; q < pt * px * PYP; q += NTHREADS) {
@@ -205,13 +222,79 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 	}
 	__syncthreads();
 
+	__shared__ int s_ok;
+	if (tid >= NCOMP) {
+		// The halo / publication warp.  For slice t it waits until the compute
+		// threads have stored slice t-1 (which also ends their use of slot t's
+		// previous contents), publishes slice t-1, clears slot t, waits for the
+		// three neighbour tiles to publish slice t and loads slice t's halo,
+		// while the compute threads accumulate the previous slices' terms.
+		const int lane = tid - NCOMP;
+		// 16-byte halo chunks need 16-byte aligned rows in global memory
+		const bool vec_ok = (tk.ny % 4 == 0) &&
+		                    ((reinterpret_cast<uintptr_t>(tk.zeta) & 15) == 0) && ((sst % 4) == 0);
+		const int* fW = (bx > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by : nullptr;
+		const int* fN = (by > 0) ? tk.flags + bx * tk.tiles_y + by - 1 : nullptr;
+		const int* fNW = (bx > 0 && by > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by - 1 : nullptr;
+		int* own_flag = tk.flags + bx * tk.tiles_y + by;
+		for (int t = tk.t0; t < tk.nt; ++t) {
+			if (t > tk.t0) {
+				bar_sync(BAR_DONE, NTHREADS);
+				if (lane == 0) {
+					__threadfence();
+					st_release(own_flag, t);
+				}
+			}
+			float* cur = ring + (t % pt) * slot_sz;
+			const float* zt = tk.zeta + t * sst;
+			for (int q = lane; q < slot_sz; q += 32) cur[q] = 0.0f;
+			__syncwarp();
+			int ok = 1;
+			if (lane == 0) ok = wait_flags(fW, fN, fNW, t + 1, err) ? 1 : 0;
+			ok = __shfl_sync(0xffffffffu, ok, 0);
+			if (ok) {
+				// rows above the tile (all columns) and the left columns of the
+				// tile rows, in 16-byte chunks copied with L2-only asynchronous
+				// copies (scalar loads at ragged edges)
+				const int top = hx * (W / 4);
+				const int nch = top + TX * (LH / 4);
+				for (int q = lane; q < nch; q += 32) {
+					int rr, c4;
+					if (q < top) {
+						rr = q / (W / 4);
+						c4 = q % (W / 4);
+					} else {
+						rr = hx + (q - top) / (LH / 4);
+						c4 = (q - top) % (LH / 4);
+					}
+					const int x = x0 - hx + rr, y = y0 - LH + 4 * c4;
+					if (x < 0 || x >= tk.nx) continue;  // stays zero
+					float* dst = cur + rr * W + 4 * c4;
+					const float* src = zt + (long long)x * tk.ny + y;
+					if (vec_ok && y >= 0 && y + 4 <= tk.ny) {
+						cp_async16(dst, src);
+					} else {
+						for (int e = 0; e < 4; ++e)
+							if (y + e >= 0 && y + e < tk.ny) dst[e] = __ldcg(src + e);
+					}
+				}
+				cp_async_wait_all();
+			}
+			if (lane == 0) s_ok = ok;
+			bar_arrive(BAR_HALO, NTHREADS);
+			if (!ok) return;
+		}
+		if (tk.nt > tk.t0) {
+			bar_sync(BAR_DONE, NTHREADS);
+			if (lane == 0) {
+				__threadfence();
+				st_release(own_flag, tk.nt);
+			}
+		}
+		return;
+	}
+
 	const int gx = x0 + xl;
-	// 16-byte halo chunks need 16-byte aligned rows in global memory
-	const bool vec_ok = (tk.ny % 4 == 0) && ((reinterpret_cast<uintptr_t>(tk.zeta) & 15) == 0) &&
-	                    ((sst % 4) == 0);
-	const int* fW = (bx > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by : nullptr;
-	const int* fN = (by > 0) ? tk.flags + bx * tk.tiles_y + by - 1 : nullptr;
-	const int* fNW = (bx > 0 && by > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by - 1 : nullptr;
 	// H-phase share of this group: rows 0-7 split dx at 4, rows 8-15 at 8, so
 	// every warp runs at most 8 dx iterations
 	const int half = xl >> 3;
@@ -230,10 +313,6 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 			s[r] = (grp == 0 && gx < tk.nx && gy < tk.ny) ? zt[(long long)gx * tk.ny + gy] : 0.0f;
 			c[r] = 0.0f;
 		}
-		// clear the current slot (halo is refilled below; in-tile stays 0 until
-		// the slice is solved)
-		for (int q = tid; q < slot_sz; q += NTHREADS) cur[q] = 0.0f;
-
 		// One (k, i) row of taps at a time, rows alternating between the two
 		// groups: the hi and lo coefficient parts are applied as two FP32 FMA
 		// chains over the same register window, and the row total is
@@ -293,45 +372,12 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 			}
 		};
 
-		// 1. previous slices
+		// 1. previous slices (the halo warp meanwhile prepares slot t)
 		for (int k = 1; k < pt && k <= t; ++k) accumulate_rows(ring + ((t - k) % pt) * slot_sz, k);
-		__syncthreads();  // slot cleared by all threads
 
-		// 2. neighbours' slice t
-		__shared__ int s_ok;
-		if (tid == 0) s_ok = wait_flags(fW, fN, fNW, t + 1, err) ? 1 : 0;
-		__syncthreads();
+		// 2./3. slot t cleared, neighbours' slice t published, halo loaded
+		bar_sync(BAR_HALO, NTHREADS);
 		if (!s_ok) return;
-
-		// 3. halo of slice t: rows above the tile (all columns) and the left
-		//    columns of the tile rows, in 16-byte chunks copied with
-		//    L2-only asynchronous copies (scalar loads at ragged edges)
-		{
-			const int top = hx * (W / 4);
-			const int nch = top + TX * (LH / 4);
-			for (int q = tid; q < nch; q += NTHREADS) {
-				int rr, c4;
-				if (q < top) {
-					rr = q / (W / 4);
-					c4 = q % (W / 4);
-				} else {
-					rr = hx + (q - top) / (LH / 4);
-					c4 = (q - top) % (LH / 4);
-				}
-				const int x = x0 - hx + rr, y = y0 - LH + 4 * c4;
-				if (x < 0 || x >= tk.nx) continue;  // stays zero
-				float* dst = cur + rr * W + 4 * c4;
-				const float* src = zt + (long long)x * tk.ny + y;
-				if (vec_ok && y >= 0 && y + 4 <= tk.ny) {
-					cp_async16(dst, src);
-				} else {
-					for (int e = 0; e < 4; ++e)
-						if (y + e >= 0 && y + e < tk.ny) dst[e] = __ldcg(src + e);
-				}
-			}
-			cp_async_wait_all();
-		}
-		__syncthreads();
 		accumulate_rows(cur, 0);
 
 		// 4. S = noise + all terms outside the unknown in-tile part
@@ -339,7 +385,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 #pragma unroll
 			for (int r = 0; r < R; ++r) comb[lt * R + r] = s[r] - c[r];
 		}
-		__syncthreads();
+		bar_sync(BAR_COMP, NCOMP);
 		if (grp == 0) {
 #pragma unroll
 			for (int r = 0; r < R; ++r) {
@@ -348,13 +394,13 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 				ss[xl * SW + SPAD + yl0 + r] = valid ? (s[r] + (comb[lt * R + r] - c[r])) : 0.0f;
 			}
 		}
-		__syncthreads();
+		bar_sync(BAR_COMP, NCOMP);
 
 		//    zeta = H * S over the quarter plane of the tile
 		h_phase(ss, sh, xl, yl0, dx_lo, dx_hi, hres + tid * R);
 
-		// 5. store the solved slice and publish it
-		__syncthreads();
+		// 5. store the solved slice; the halo warp publishes it
+		bar_sync(BAR_COMP, NCOMP);
 		if (grp == 0) {
 			float* own = cur + hx * W + LH;
 #pragma unroll
@@ -365,11 +411,8 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 				if (gx < tk.nx && gy < tk.ny) zt[(long long)gx * tk.ny + gy] = v;
 			}
 		}
-		__syncthreads();
-		if (tid == 0) {
-			__threadfence();
-			st_release(tk.flags + bx * tk.tiles_y + by, t + 1);
-		}
+		bar_sync(BAR_COMP, NCOMP);  // slice t in the ring for every compute thread
+		bar_arrive(BAR_DONE, NTHREADS);
 	}
 }
 
@@ -413,7 +456,7 @@ size_t smem_bytes(int pt, int px, int py) {
 	const int rows = TX + px - 1;
 	const int pyp = (py + 3) & ~3;
 	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + TX * TY + TX * SW +
-	                        GROUP * R + NTHREADS * R);
+	                        GROUP * R + NCOMP * R);
 }
 
 }  // namespace
