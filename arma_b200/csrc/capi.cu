@@ -283,6 +283,10 @@ int arma_ctx_destroy(arma_ctx* ctx) {
 		for (auto& kv : ctx->c.graphs) cudaGraphExecDestroy(kv.second);
 		for (auto& ch : ctx->chunks) pool_free(&ctx->c, ch.first);
 		cudaStreamSynchronize(ctx->c.stream);
+		if (ctx->c.copy_stream) {
+			cudaStreamSynchronize(ctx->c.copy_stream);
+			cudaStreamDestroy(ctx->c.copy_stream);
+		}
 		cudaFree(ctx->c.d_err);
 		if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
 		delete ctx;
@@ -745,6 +749,8 @@ namespace {
 
 void renorm_surfaces(Ctx* c, arma_surface* s, int n, int precision, const std::vector<void*>& dz,
                      bool host);
+void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<Ar32Surface>& as,
+                           const std::vector<void*>& dz);
 
 void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 	const size_t es = elem_size(precision);
@@ -774,11 +780,91 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 		}
 		std::vector<Ar32Surface> as =
 		    ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
+		if (host && n >= 4) {
+			pipelined_host_output(c, s, n, as, dz);
+			return;
+		}
 		launch_ar32c(c, as, tx, ty, 1);
 		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 		check_device_error(c);
 	}
 	renorm_surfaces(c, s, n, precision, dz, host);
+}
+
+// FP32 surfaces into host buffers with the device->host copies overlapped with
+// the filtering: the batch is split into groups of decreasing work (40, 30,
+// 20, 10 % of the total points x taps); each group's persistent filter launch
+// and renormalisation run on the context's stream, and the group's copies
+// follow on a copy stream while the next group computes, so only the last,
+// smallest group's copies are exposed.
+void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<Ar32Surface>& as,
+                           const std::vector<void*>& dz) {
+	constexpr int G = 4;
+	const double frac[G] = {0.4, 0.3, 0.2, 0.1};
+	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
+	std::vector<double> work(n);
+	double total = 0.0;
+	for (int k = 0; k < n; ++k) {
+		work[k] = double(as[k].nt) * as[k].nx * as[k].ny * as[k].pt * as[k].px * as[k].py;
+		total += work[k];
+	}
+	// largest surfaces first, each to the group furthest below its share
+	std::vector<int> order(n);
+	for (int k = 0; k < n; ++k) order[k] = k;
+	std::sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+	std::vector<std::vector<int>> members(G);
+	double assigned[G] = {0, 0, 0, 0};
+	for (int k : order) {
+		int best = 0;
+		for (int g = 1; g < G; ++g)
+			if (frac[g] * total - assigned[g] > frac[best] * total - assigned[best]) best = g;
+		members[best].push_back(k);
+		assigned[best] += work[k];
+	}
+	if (!c->copy_stream)
+		ARMA_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+	double* d_scale = static_cast<double*>(scratch_take(c, sizeof(double) * n));
+	std::vector<cudaEvent_t> ev;
+	auto release = [&] {
+		for (cudaEvent_t e : ev) cudaEventDestroy(e);
+	};
+	try {
+		for (int g = 0; g < G; ++g) {
+			if (members[g].empty()) continue;
+			std::vector<Ar32Surface> ga;
+			std::vector<RenormSpec> rs;
+			for (int k : members[g]) {
+				ga.push_back(as[k]);
+				if (s[k].acf0 > 0.0)
+					rs.push_back(RenormSpec{dz[k], {s[k].shape[0], s[k].shape[1], s[k].shape[2]},
+					                        s[k].acf0, d_scale + k});
+			}
+			launch_ar32c(c, ga, tx, ty, 1);
+			launch_renorm_batch(c, rs, ARMA_FP32C);
+			cudaEvent_t e;
+			ARMA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+			ev.push_back(e);
+			ARMA_CUDA_TRY(cudaEventRecord(e, c->stream));
+			ARMA_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, e, 0));
+			for (int k : members[g]) {
+				const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
+				ARMA_CUDA_TRY(cudaMemcpyAsync(s[k].d_zeta, dz[k], np * sizeof(float),
+				                              cudaMemcpyDeviceToHost, c->copy_stream));
+			}
+		}
+		std::vector<double> sc(n, 1.0);
+		ARMA_CUDA_TRY(cudaMemcpyAsync(sc.data(), d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost,
+		                              c->stream));
+		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+		ARMA_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
+		check_device_error(c);
+		for (int k = 0; k < n; ++k) s[k].scale = s[k].acf0 > 0.0 ? sc[k] : 1.0;
+	} catch (...) {
+		cudaStreamSynchronize(c->copy_stream);
+		release();
+		throw;
+	}
+	release();
 }
 
 // The variance renormalisation of each surface with acf0 > 0 (and the copy to

@@ -50,6 +50,7 @@ struct Ctx {
 	cudaStream_t stream = nullptr;
 	bool own_stream = false;
 	int* d_err = nullptr;            // device error word
+	cudaStream_t copy_stream = nullptr;  // device->host copies overlapped with compute (lazy)
 	uint64_t launches = 0;           // kernel launches issued
 	int num_sms = 148;
 	// cached CUDA graphs for the FP64 plane sweep, keyed by a string

@@ -218,6 +218,32 @@ def test_batch_host_buffers(ctx):
     assert np.allclose(host, ref, rtol=1e-12, atol=1e-12)
 
 
+def test_batch_host_buffers_fp32_pipelined(ctx):
+    """Six FP32 surfaces into host buffers (the grouped path that overlaps the
+    device->host copies with the filtering) equal the same batch generated
+    into device buffers, bit for bit, scales included."""
+    import torch
+    p = A.mt19937_params()
+    shapes = [(40, 64, 96), (25, 32, 32), (60, 48, 40), (17, 100, 33), (33, 16, 128), (50, 70, 70)]
+    fits = [A.ar_fit_analytic(A.ACF_STANDING if k % 2 else A.ACF_PROPAGATING, (4 + k % 3,) * 3,
+                              1.5, 0.8, [0.05] * 3, [0.5, 0.5]) for k in range(len(shapes))]
+    dev = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh in shapes]
+    sd = [capi.make_surface(sh, f[0], f[1], 1.5, p, 300 + k, b.data_ptr())
+          for k, (sh, f, b) in enumerate(zip(shapes, fits, dev))]
+    sc_dev = ctx.batch_generate(sd, A.FP32C)
+    ctx.synchronize()
+    host = [torch.zeros(sh, dtype=torch.float32).pin_memory() if k % 2 else np.zeros(sh, np.float32)
+            for k, sh in enumerate(shapes)]
+    ptr = [h.data_ptr() if k % 2 else h.ctypes.data for k, h in enumerate(host)]
+    sh_ = [capi.make_surface(sh, f[0], f[1], 1.5, p, 300 + k, q)
+           for k, (sh, f, q) in enumerate(zip(shapes, fits, ptr))]
+    sc_host = ctx.batch_generate(sh_, A.FP32C, host=True)
+    assert sc_host == sc_dev
+    for k in range(len(shapes)):
+        h = host[k].numpy() if k % 2 else host[k]
+        assert np.array_equal(h, dev[k].cpu().numpy()), k
+
+
 def test_errors_are_reported(ctx):
     with pytest.raises(capi.ArmaError):
         ctx.ar_filter(np.zeros((2, 2, 2)), (0, 4, 4), A.FP64, 0)
