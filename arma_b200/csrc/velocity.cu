@@ -11,13 +11,10 @@
 // The work is a list of slices (surface pointer, its length, slice index,
 // time step, output pointer), so one set of launches serves any number of
 // surfaces of one slice shape:
-//   1. factor_waves_kernel one CTA per (slice, axis): the positions are cut
-//                          into one segment per warp; each warp compacts the
-//                          extrema events of 32 positions at a time with a
-//                          ballot and walks them with a segmented first-
-//                          maximum scan, summarising its segment; warp 0
-//                          merges the summaries in order.  No per-event
-//                          global memory.
+//   1. factor_waves_kernel one CTA per (slice, axis): each lane walks a
+//                          piece of one line of the loop order (a column or
+//                          a row) and summarises it; the summaries are joined
+//                          in a tree.  No per-event global memory.
 //   2a. FP32, nx*ny <= 16384: velocity_fused_kernel, one CTA per slice:
 //                          zeta_t into shared memory, in-place mixed-radix
 //                          FFT2 (decimation in frequency: natural in, digit-
@@ -131,15 +128,17 @@ __device__ __forceinline__ void solver_input(const VelSlice<T>& s, int nx, int n
 // p_{r-1})|)^2 / g for every run r >= 1 that closes (the last run never
 // closes); wnmax comes from the smallest k.
 //
-// On the device one CTA of kFwWarps warps handles one (slice, axis): the
-// positions are cut into kFwWarps contiguous segments, each warp walks its
-// segment 32 positions at a time (ballot compaction of the events, a
-// segmented first-maximum scan over the runs) and summarises it; warp 0 then
-// merges the summaries in order.  A segment's first run may continue the
-// previous segment's last run, so pairs that involve its first run are
-// completed during the merge.
-constexpr int kFwWarps = 8;
-constexpr unsigned kFull = 0xffffffffu;
+// On the device one CTA of kFwThreads threads handles one (slice, axis).  The
+// loop order is cut into segments: each line (a column for the x pass, a row
+// for the y pass) in P pieces, enough that every warp has work.  A warp walks
+// 32 neighbouring lines' pieces at once, one lane per piece, each lane keeping
+// the summary of its segment: its runs, the representative periods a join
+// still needs and the extreme k of the pairs it closes.  The summaries are then
+// joined pairwise in a tree (the join is associative: it is the walk itself
+// restarted at a segment boundary) and the pair of the first two runs is added
+// at the end.
+constexpr int kFwThreads = 256;
+constexpr int kFwTile = 35;  // row pitch of the y pass's transposing tile (odd)
 
 struct Run {
 	int sign;       // elevation > 0
@@ -155,8 +154,7 @@ struct SegWalk {
 	double prev_p = 0.0;    // representative period of run m-2
 	Run r0{0, 0.0, 0.0};    // run 0 once closed
 	double r1_p = 0.0;      // run 1 once closed
-	double mn = DBL_MAX, mx = DBL_MIN;  // pairs (r-1, r) with r >= 2, closed (per lane
-	                                    // until the warp reduces them)
+	double mn = DBL_MAX, mx = DBL_MIN;  // pairs (r-1, r) with r >= 2, closed
 };
 
 __device__ __forceinline__ void pair_k(double p0, double p1, double& mn, double& mx) {
@@ -166,171 +164,181 @@ __device__ __forceinline__ void pair_k(double p0, double p1, double& mn, double&
 	if (k > mx) mx = k;
 }
 
-// The first g lanes hold consecutive events (e: elevation, p: period).
-__device__ void walk_events(double e, double p, int g, SegWalk& st) {
-	const int lane = threadIdx.x & 31;
-	const bool valid = lane < g;
+// One event of a thread's own segment, in loop order.
+__device__ __forceinline__ void seg_event(SegWalk& st, double e, double p) {
 	const int s = e > 0.0 ? 1 : 0;
-	const int sprev = __shfl_up_sync(kFull, s, 1);
-	const bool open = st.m > 0;
-	bool b = lane == 0 ? (!open || s != st.open.sign) : (s != sprev);
-	b = b && valid;
-	const unsigned B = __ballot_sync(kFull, b);
-	const unsigned upto = B & (lane == 31 ? kFull : ((2u << lane) - 1u));
-	const int start = upto ? 31 - __clz(upto) : 0;  // first lane of this lane's run
-	// segmented inclusive scan: first maximum of |elevation| within the run
-	double bv = valid ? fabs(e) : 0.0, bp = p;
-	for (int o = 1; o < 32; o <<= 1) {
-		const double ov = __shfl_up_sync(kFull, bv, o);
-		const double op = __shfl_up_sync(kFull, bp, o);
-		if (lane - o >= start && !(bv > ov)) {
-			bv = ov;
-			bp = op;
+	const double ae = fabs(e);
+	if (st.m == 0) {
+		st.open = Run{s, ae, p};
+		st.m = 1;
+	} else if (s == st.open.sign) {
+		if (st.open.best_e < ae) {  // the first maximum stays
+			st.open.best_e = ae;
+			st.open.best_p = p;
 		}
-	}
-	const bool lead = (B & 1u) != 0;  // lane 0 starts a new run
-	if (open && !lead && upto == 0 && !(bv > st.open.best_e)) {
-		bv = st.open.best_e;  // the open run continues: it came first
-		bp = st.open.best_p;
-	}
-	const int first_index = lead ? st.m : st.m - 1;
-	const int run = first_index + __popc(upto & ~1u);
-	const double before = __shfl_sync(kFull, bp, start > 0 ? start - 1 : 0);
-	const double prev = start > 0 ? before : (lead ? st.open.best_p : st.prev_p);
-	// runs closing here: the open one (a new run starts at lane 0) and every
-	// run followed by a boundary inside the group
-	const bool closes = valid && lane + 1 < g && ((B >> (lane + 1)) & 1u);
-	if (open && lead) {
-		const int r = st.m - 1;
+	} else {
+		const int r = st.m - 1;  // the open run closes
 		if (r == 0) st.r0 = st.open;
 		else if (r == 1) st.r1_p = st.open.best_p;
-		else if (lane == 0) pair_k(st.prev_p, st.open.best_p, st.mn, st.mx);
+		else pair_k(st.prev_p, st.open.best_p, st.mn, st.mx);
+		st.prev_p = st.open.best_p;
+		st.open = Run{s, ae, p};
+		++st.m;
 	}
-	if (closes && run >= 2) pair_k(prev, bp, st.mn, st.mx);
-	const unsigned c0 = __ballot_sync(kFull, closes && run == 0);
-	if (c0) {
-		const int src = __ffs(c0) - 1;
-		st.r0.sign = __shfl_sync(kFull, s, src);
-		st.r0.best_e = __shfl_sync(kFull, bv, src);
-		st.r0.best_p = __shfl_sync(kFull, bp, src);
-	}
-	const unsigned c1 = __ballot_sync(kFull, closes && run == 1);
-	if (c1) st.r1_p = __shfl_sync(kFull, bp, __ffs(c1) - 1);
-	// the run open after the group
-	const int last = g - 1;
-	const int lstart = __shfl_sync(kFull, start, last);
-	const double lbefore = __shfl_sync(kFull, bp, lstart > 0 ? lstart - 1 : 0);
-	st.prev_p = lstart > 0 ? lbefore : (lead ? st.open.best_p : st.prev_p);
-	st.open.sign = __shfl_sync(kFull, s, last);
-	st.open.best_e = __shfl_sync(kFull, bv, last);
-	st.open.best_p = __shfl_sync(kFull, bp, last);
-	st.m = __shfl_sync(kFull, run, last) + 1;
 }
 
-// The global walk, continued by one segment summary (lane-uniform).
-struct GlobalWalk {
-	bool open = false;
-	Run cur{0, 0.0, 0.0};
-	double prev_p = 0.0;
-	int index = -1;
-	double mn = DBL_MAX, mx = DBL_MIN;
-};
-
-__device__ void merge_segment(GlobalWalk& G, const SegWalk& S) {
-	if (S.m == 0) return;
-	if (S.mn < G.mn) G.mn = S.mn;
-	if (S.mx > G.mx) G.mx = S.mx;
-	const Run r0 = S.m == 1 ? S.open : S.r0;
-	Run merged;
-	int idx0;
-	double prev0;
-	if (G.open && r0.sign == G.cur.sign) {  // the open run continues
-		merged = r0.best_e > G.cur.best_e ? r0 : G.cur;
-		merged.sign = G.cur.sign;
-		idx0 = G.index;
-		prev0 = G.prev_p;
-	} else {
-		if (G.open && G.index >= 1) pair_k(G.prev_p, G.cur.best_p, G.mn, G.mx);
-		merged = r0;
-		idx0 = G.open ? G.index + 1 : 0;
-		prev0 = G.cur.best_p;
+// The summary of segment A followed by segment B.  B's first run continues
+// A's open run when their signs agree (the first maximum stays A's unless B's
+// is larger); otherwise A's open run closes at the boundary.  Runs with index
+// 0 and 1 keep their representatives for a later join; every other run that
+// closes adds its pair.
+__device__ SegWalk seg_join(const SegWalk& A, const SegWalk& B) {
+	if (A.m == 0) return B;
+	if (B.m == 0) return A;
+	SegWalk C;
+	C.mn = fmin(A.mn, B.mn);
+	C.mx = fmax(A.mx, B.mx);
+	C.r0 = A.r0;
+	C.r1_p = A.r1_p;
+	const Run b0 = B.m == 1 ? B.open : B.r0;
+	if (b0.sign == A.open.sign) {
+		Run R = A.open;  // index A.m - 1
+		if (R.best_e < b0.best_e) {
+			R.best_e = b0.best_e;
+			R.best_p = b0.best_p;
+		}
+		const int rR = A.m - 1;
+		C.m = A.m + B.m - 1;
+		if (B.m == 1) {
+			C.open = R;
+			C.prev_p = A.prev_p;
+			return C;
+		}
+		if (rR == 0) C.r0 = R;
+		else if (rR == 1) C.r1_p = R.best_p;
+		else pair_k(A.prev_p, R.best_p, C.mn, C.mx);
+		if (B.m >= 3) {  // B's run 1 (index rR + 1) closed
+			if (rR == 0) C.r1_p = B.r1_p;
+			else pair_k(R.best_p, B.r1_p, C.mn, C.mx);
+		}
+		C.open = B.open;
+		C.prev_p = B.m == 2 ? R.best_p : B.prev_p;
+		return C;
 	}
-	if (S.m == 1) {
-		G.open = true;
-		G.cur = merged;
-		G.prev_p = prev0;
-		G.index = idx0;
-		return;
+	const int rA = A.m - 1;  // A's open run closes
+	C.m = A.m + B.m;
+	if (rA == 0) C.r0 = A.open;
+	else if (rA == 1) C.r1_p = A.open.best_p;
+	else pair_k(A.prev_p, A.open.best_p, C.mn, C.mx);
+	if (B.m == 1) {
+		C.open = B.open;
+		C.prev_p = A.open.best_p;
+		return C;
 	}
-	if (idx0 >= 1) pair_k(prev0, merged.best_p, G.mn, G.mx);
-	if (S.m >= 3) pair_k(merged.best_p, S.r1_p, G.mn, G.mx);
-	G.open = true;
-	G.cur = S.open;
-	G.prev_p = S.m == 2 ? merged.best_p : S.prev_p;
-	G.index = idx0 + S.m - 1;
+	if (A.m == 1) C.r1_p = b0.best_p;  // B's run 0 (index A.m) closed
+	else pair_k(A.open.best_p, b0.best_p, C.mn, C.mx);
+	if (B.m >= 3) pair_k(b0.best_p, B.r1_p, C.mn, C.mx);  // index A.m + 1 >= 2
+	C.open = B.open;
+	C.prev_p = B.m == 2 ? b0.best_p : B.prev_p;
+	return C;
 }
 
-// One CTA per (slice, axis).  axis 0 loops y outer, x inner over z(x,y);
-// axis 1 (the reference's transposed call) x outer, y inner.  Writes min_k,
-// max_k of the axis.
+// Extremum test and quadratic vertex at position a of a line (z0 = z(a),
+// z1 = z(a-1), z2 = z(a+1)), fed to the segment walk.
+__device__ __forceinline__ void fw_position(SegWalk& st, double z0, double z1, double z2, double dt,
+                                            int t) {
+	const double dw1 = z0 - z1, dw2 = z0 - z2;
+	if (!((dw1 > 0.0) ^ (dw2 > 0.0))) {
+		const double aa = -0.5 * (dw1 + dw2) / (dt * dt);
+		const double bb = dw1 / dt - aa * dt * (2.0 * t - 1.0);
+		const double cc = z0 - t * dt * (aa * t * dt + bb);
+		const double tex = -0.5 * bb / aa;
+		seg_event(st, cc + tex * (bb + aa * tex), tex);
+	}
+}
+
+// Pieces per line: enough (line blocks of 32) x pieces for the CTA's warps,
+// at least 8 positions each.
+__host__ __device__ inline int fw_pieces(int outer, int npos) {
+	const int blocks = (outer + 31) / 32;
+	const int want = (kFwThreads / 32 + blocks - 1) / blocks;
+	return npos < 16 ? 1 : (want < npos / 8 ? want : npos / 8);
+}
+
+// One CTA per (slice, axis).  axis 0 loops y outer, x inner over z(x,y): lane
+// b walks column y = b down x (loads coalesced across the warp); axis 1 (the
+// reference's transposed call) x outer, y inner: lane b walks row x = b, each
+// warp staging 32 rows x 34 columns at a time through shared memory.  Writes
+// min_k, max_k of the axis.
 template <class T>
-__global__ void __launch_bounds__(kFwWarps * 32)
+__global__ void __launch_bounds__(kFwThreads)
 factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* __restrict__ kout) {
-	__shared__ SegWalk seg[kFwWarps];
+	extern __shared__ __align__(16) unsigned char fw_smem[];
 	const int slice = blockIdx.x >> 1, axis = blockIdx.x & 1;
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
 	const VelSlice<T> S = sl[slice];
 	const long long n2 = (long long)nx * ny;
 	const T* z = S.zeta + S.d * n2;
 	const double dt = S.dt;
 	const int t = int(dt * S.d);  // factor_waves(slice, int t, dt): the truncated coordinate
 	const int outer = axis == 0 ? ny : nx;
-	const int inner = (axis == 0 ? nx : ny) - 2;
-	const long long L = inner > 0 ? (long long)outer * inner : 0;
-	auto at = [&](int a, int b) -> double {  // a: inner index, b: outer index
-		return axis == 0 ? double(z[(long long)a * ny + b]) : double(z[(long long)b * ny + a]);
-	};
-	const long long per = (L + kFwWarps - 1) / kFwWarps;
-	const long long q0 = min(L, warp * per), q1 = min(L, q0 + per);
-	SegWalk st;
-	for (long long base = q0; base < q1; base += 32) {
-		const long long q = base + lane;
-		int flag = 0;
-		double period = 0.0, elevation = 0.0;
-		if (q < q1) {
-			const int b = int(q / inner), a = int(q % inner) + 1;
-			const double z0 = at(a, b), z1 = at(a - 1, b), z2 = at(a + 1, b);
-			const double dw1 = z0 - z1, dw2 = z0 - z2;
-			if (!((dw1 > 0.0) ^ (dw2 > 0.0))) {
-				const double aa = -0.5 * (dw1 + dw2) / (dt * dt);
-				const double bb = dw1 / dt - aa * dt * (2.0 * t - 1.0);
-				const double cc = z0 - t * dt * (aa * t * dt + bb);
-				const double tex = -0.5 * bb / aa;
-				period = tex;
-				elevation = cc + tex * (bb + aa * tex);
-				flag = 1;
+	const int npos = (axis == 0 ? nx : ny) - 2;  // positions 1 .. npos of each line
+	const int P = fw_pieces(outer, npos), per = (npos + P - 1) / P;
+	const int nseg = outer * P, blocks = (outer + 31) / 32;
+	SegWalk* seg = reinterpret_cast<SegWalk*>(fw_smem);
+	T* tile = reinterpret_cast<T*>(seg + max(nseg, 1)) + warp * 32 * kFwTile;
+	for (int u = warp; u < blocks * P; u += nwarps) {
+		const int piece = u / blocks, b0 = (u % blocks) * 32, b = b0 + lane;
+		const int a_lo = 1 + piece * per, a_hi = 1 + min(npos, (piece + 1) * per);  // [a_lo, a_hi)
+		SegWalk st;
+		if (axis == 0) {
+			if (b < outer && a_lo < a_hi) {
+				double z1 = double(z[(long long)(a_lo - 1) * ny + b]);
+				double z0 = double(z[(long long)a_lo * ny + b]);
+				for (int a = a_lo; a < a_hi; ++a) {
+					const double z2 = double(z[(long long)(a + 1) * ny + b]);
+					fw_position(st, z0, z1, z2, dt, t);
+					z1 = z0;
+					z0 = z2;
+				}
+			}
+		} else {
+			const int rows = min(32, outer - b0);
+			for (int c0 = a_lo; c0 < a_hi; c0 += 32) {
+				// columns c0-1 .. c0+32 of rows b0 .. b0+rows-1 (those < ny)
+				__syncwarp();
+				for (int r = 0; r < rows; ++r) {
+					const T* zr = z + (long long)(b0 + r) * ny;
+					if (c0 - 1 + lane < ny) tile[r * kFwTile + lane] = zr[c0 - 1 + lane];
+					if (lane < 2 && c0 + 31 + lane < ny) tile[r * kFwTile + 32 + lane] = zr[c0 + 31 + lane];
+				}
+				__syncwarp();
+				if (b < outer) {
+					const T* row = tile + lane * kFwTile;  // row[k] = z(b, c0 - 1 + k)
+					double z1 = double(row[0]), z0 = double(row[1]);
+					const int n = min(32, a_hi - c0);
+					for (int k = 0; k < n; ++k) {
+						const double z2 = double(row[k + 2]);
+						fw_position(st, z0, z1, z2, dt, t);
+						z1 = z0;
+						z0 = z2;
+					}
+				}
 			}
 		}
-		const unsigned mask = __ballot_sync(kFull, flag);
-		if (!mask) continue;
-		const int g = __popc(mask);
-		const int src = lane < g ? int(__fns(mask, 0, lane + 1)) : 0;
-		const double e = __shfl_sync(kFull, elevation, src);
-		const double pp = __shfl_sync(kFull, period, src);
-		walk_events(e, pp, g, st);
+		if (b < outer) seg[b * P + piece] = st;  // loop order: line, then piece
 	}
-	// pairs were accumulated by the lanes that closed them
-	for (int o = 16; o > 0; o >>= 1) {
-		st.mn = fmin(st.mn, __shfl_down_sync(kFull, st.mn, o));
-		st.mx = fmax(st.mx, __shfl_down_sync(kFull, st.mx, o));
-	}
-	if (lane == 0) seg[warp] = st;
 	__syncthreads();
+	for (int stride = 1; stride < nseg; stride <<= 1) {
+		for (int i = threadIdx.x * 2 * stride; i + stride < nseg; i += blockDim.x * 2 * stride)
+			seg[i] = seg_join(seg[i], seg[i + stride]);
+		__syncthreads();
+	}
 	if (threadIdx.x == 0) {
-		GlobalWalk G;
-		for (int w = 0; w < kFwWarps; ++w) merge_segment(G, seg[w]);
-		kout[slice * 4 + axis] = G.mn;      // min_k for this axis
-		kout[slice * 4 + 2 + axis] = G.mx;  // max_k
+		SegWalk all = nseg > 0 ? seg[0] : SegWalk{};
+		if (all.m >= 3) pair_k(all.r0.best_p, all.r1_p, all.mn, all.mx);  // runs 0 and 1
+		kout[slice * 4 + axis] = all.mn;      // min_k for this axis
+		kout[slice * 4 + 2 + axis] = all.mx;  // max_k
 	}
 }
 
@@ -835,7 +843,14 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d_sl, slices.data(), sizeof(VelSlice<T>) * ns,
 	                              cudaMemcpyHostToDevice, c->stream));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d_z, z, sizeof(double) * nz, cudaMemcpyHostToDevice, c->stream));
-	factor_waves_kernel<T><<<2 * ns, kFwWarps * 32, 0, c->stream>>>(d_sl, nx, ny, d_k);
+	{
+		const int nseg = std::max(nx * fw_pieces(nx, ny - 2), ny * fw_pieces(ny, nx - 2));
+		const size_t fw_smem = sizeof(SegWalk) * std::max(nseg, 1) +
+		                       sizeof(T) * (kFwThreads / 32) * 32 * kFwTile;
+		ARMA_CUDA_TRY(cudaFuncSetAttribute(factor_waves_kernel<T>,
+		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(fw_smem)));
+		factor_waves_kernel<T><<<2 * ns, kFwThreads, fw_smem, c->stream>>>(d_sl, nx, ny, d_k);
+	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 	if (sizeof(T) == sizeof(float) && n2 <= kFuseMax) {
