@@ -25,12 +25,15 @@
 //      critical path.
 // The coefficients are carried as hi + lo float pairs (rounding phi to one
 // float perturbs a high-gain recursion far more than FP32 summation does):
-// each (k,i) row of taps is two FP32 FMA chains over one register window, and
-// row totals are combined with Kahan compensation.  H is applied in plain
-// FP32 with Kahan-added partial sums: it acts once per slice on the current
-// slice alone, and its rounding changes the surface by far less than phi's
-// (a lo part for H moved the RMS error by under 1e-7 at 18 % of the filter's
-// time).  Tiles are handed out through a global ticket
+// each (k,i) row of taps feeds two FP32 FMA chains over one register window,
+// continued across the rows of one k plane, and the plane totals are combined
+// with Kahan compensation (per row, the compensation cost 7 % more time for
+// 0.2-1.2e-6 less RMS error).  H is applied in plain FP32, one FMA chain per
+// output over each row of H (up to 32 taps), the row totals Kahan-added: it
+// acts once per slice on the current slice alone, and its rounding changes
+// the surface by far less than phi's (a lo part for H moved the RMS error by
+// under 1e-7 at 18 % of the filter's time; compensating every 8 taps instead
+// of every row, by under 2e-7 at 11 %).  Tiles are handed out through a global ticket
 // counter in dependency order, so a CTA only ever waits on tiles that are
 // already owned by running CTAs.
 #include <algorithm>
@@ -135,6 +138,9 @@ __device__ __noinline__ void h_phase(const float* ss, const float* sh, int xl, i
 	for (int dx = dx_lo; dx <= dx_end; ++dx) {
 		const float* srow = ss + (xl - dx) * SW + SPAD;
 		const float* hrow = sh + dx * TY;
+		float pr[R];
+#pragma unroll
+		for (int r = 0; r < R; ++r) pr[r] = 0.0f;
 		for (int dy0 = 0; dy0 <= yl0; dy0 += R) {
 			// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
 			float w[2 * R];
@@ -159,12 +165,12 @@ __device__ __noinline__ void h_phase(const float* ss, const float* sh, int xl, i
 			}
 #pragma unroll
 			for (int r = 0; r < R; ++r) {
-				float p = 0.0f;
 #pragma unroll
-				for (int dd = 0; dd < R; ++dd) p = fmaf(hv[dd], w[R + r - dd], p);
-				kahan_add(a[r], ac[r], p);
+				for (int dd = 0; dd < R; ++dd) pr[r] = fmaf(hv[dd], w[R + r - dd], pr[r]);
 			}
 		}
+#pragma unroll
+		for (int r = 0; r < R; ++r) kahan_add(a[r], ac[r], pr[r]);
 	}
 #pragma unroll
 	for (int r = 0; r < R; ++r) out[r] = a[r] - ac[r];
@@ -315,11 +321,15 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 		}
 		// One (k, i) row of taps at a time, rows alternating between the two
 		// groups: the hi and lo coefficient parts are applied as two FP32 FMA
-		// chains over the same register window, and the row total is
-		// Kahan-added to the running sum.
+		// chains over the same register window, each chain running across the
+		// rows of the k plane; the plane total is Kahan-added to the running
+		// sum.
 		auto accumulate_rows = [&](const float* slot, int k) {
 			const float* prow = sphi + (k * px) * PYP;
 			const float* lrow = slo + (k * px) * PYP;
+			float pk[R], qk[R];
+#pragma unroll
+			for (int r = 0; r < R; ++r) { pk[r] = 0.0f; qk[r] = 0.0f; }
 			for (int i = (k * px + grp) & 1; i < px; i += 2) {
 				const float* zr = slot + (xl + hx - i) * W + yl0;
 				float win[R + LH];
@@ -352,24 +362,22 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 					}
 #pragma unroll
 					for (int r = 0; r < R; ++r) {
-						float p = 0.0f, q = 0.0f;
 #pragma unroll
 						for (int j = 0; j < PY; ++j) {
-							p = fmaf(ph[j], win[LH + r - j], p);
-							q = fmaf(pl[j], win[LH + r - j], q);
+							pk[r] = fmaf(ph[j], win[LH + r - j], pk[r]);
+							qk[r] = fmaf(pl[j], win[LH + r - j], qk[r]);
 						}
-						kahan_add(s[r], c[r], p + q);
 					}
 				} else {
 #pragma unroll
 					for (int r = 0; r < R; ++r) {
-						float p = 0.0f;
 #pragma unroll
-						for (int j = 0; j < PY; ++j) p = fmaf(ph[j], win[LH + r - j], p);
-						kahan_add(s[r], c[r], p);
+						for (int j = 0; j < PY; ++j) pk[r] = fmaf(ph[j], win[LH + r - j], pk[r]);
 					}
 				}
 			}
+#pragma unroll
+			for (int r = 0; r < R; ++r) kahan_add(s[r], c[r], pk[r] + qk[r]);
 		};
 
 		// 1. previous slices (the halo warp meanwhile prepares slot t)
