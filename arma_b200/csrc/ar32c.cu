@@ -127,7 +127,9 @@ __device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need
 
 // zeta = H * S over the quarter plane of one tile for the output strip
 // (xl, yl0 .. yl0+R-1), dx restricted to [dx_lo, min(dx_hi, xl+1)): writes the
-// Kahan-compensated partial strip to out[0..R).  Shared by every tap-count
+// Kahan-compensated partial strip to out[0..R).  Per row of H the column
+// blocks run from dy0 = yl0 down to 0, so the one block that reaches only the
+// taps dd <= r comes first for every lane and runs as a triangle.  Shared by every tap-count
 // instantiation of run_tile, so its code exists once.
 __device__ __noinline__ void h_phase(const float* ss, const float* sh, int xl, int yl0, int dx_lo,
                                      int dx_hi, float* out) {
@@ -141,7 +143,32 @@ __device__ __noinline__ void h_phase(const float* ss, const float* sh, int xl, i
 		float pr[R];
 #pragma unroll
 		for (int r = 0; r < R; ++r) pr[r] = 0.0f;
-		for (int dy0 = 0; dy0 <= yl0; dy0 += R) {
+		{
+			// the block dy0 = yl0 first (every lane at once): its sources
+			// srow[0 .. R-1] reach only the taps dd <= r
+			float wt[R], hv[R];
+			const float4* sp = reinterpret_cast<const float4*>(srow);
+			const float4* hp = reinterpret_cast<const float4*>(hrow + yl0);
+#pragma unroll
+			for (int q = 0; q < R / 4; ++q) {
+				const float4 v = sp[q];
+				wt[4 * q] = v.x;
+				wt[4 * q + 1] = v.y;
+				wt[4 * q + 2] = v.z;
+				wt[4 * q + 3] = v.w;
+				const float4 u = hp[q];
+				hv[4 * q] = u.x;
+				hv[4 * q + 1] = u.y;
+				hv[4 * q + 2] = u.z;
+				hv[4 * q + 3] = u.w;
+			}
+#pragma unroll
+			for (int r = 0; r < R; ++r) {
+#pragma unroll
+				for (int dd = 0; dd <= r; ++dd) pr[r] = fmaf(hv[dd], wt[r - dd], pr[r]);
+			}
+		}
+		for (int dy0 = yl0 - R; dy0 >= 0; dy0 -= R) {
 			// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
 			float w[2 * R];
 			const float4* sp = reinterpret_cast<const float4*>(srow + yl0 - dy0 - R);
