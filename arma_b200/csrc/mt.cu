@@ -81,38 +81,43 @@ mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	const arma_mt_params p = jb.p;
 	const int n = p.nn, m = p.mm;
 	const int chunk = n - m;
+	const long long count = (long long)jb.count;
+	const long long shift = (long long)jb.first - (long long)jb.offset;  // out index - word
+	uint32_t* const out = jb.out;
 	if (jb.state) {
 		for (int k = threadIdx.x; k < n; k += blockDim.x) ring[k] = jb.state[k];
 	} else if (threadIdx.x == 0) {
 		seed_state(ring, jb.seed, p);
 	}
 	__syncthreads();
-	const unsigned long long end = (unsigned long long)n + jb.count;
 	const uint32_t mask = kRing - 1;
-	auto compute = [&](unsigned long long j0) {
-		for (int t = threadIdx.x; t < chunk; t += blockDim.x) {
-			const unsigned long long j = j0 + t;
-			if (j < end) {
-				const uint32_t y = (ring[(j - n) & mask] & p.umask) |
-				                   (ring[(j - n + 1) & mask] & p.lmask);
-				ring[j & mask] = ring[(j - n + m) & mask] ^ (y >> 1) ^ ((y & 1u) ? p.aaa : 0u);
-			}
-		}
+	// Thread t < n-m owns word t of every chunk: segment word w = s (n-m) + t
+	// at step s, raw word r = n + w at ring position r & mask (positions run
+	// modulo 2^32, a multiple of the ring size), so every index is a running
+	// register sum.  Each step emits the chunk computed by the step before and
+	// computes the next one: raw r + n - m reads raw r (this thread's own
+	// word) and raw r - m, r - m + 1, all written in earlier steps.
+	const int t = threadIdx.x;
+	const bool owner = t < chunk;
+	auto next_word = [&](uint32_t r) {  // raw word r from raw r - n, r - n + 1, r - n + m
+		const uint32_t y = (ring[(r - n) & mask] & p.umask) | (ring[(r - n + 1) & mask] & p.lmask);
+		return ring[(r - n + m) & mask] ^ (y >> 1) ^ ((y & 1u) ? p.aaa : 0u);
 	};
-	unsigned long long j0 = n;
-	compute(j0);
+	uint32_t r = uint32_t(n + t);  // raw position of this thread's current word
+	long long o = shift + t;       // its output index
+	long long rem = count - t;     // words from it to the segment's end
+	if (owner && rem > 0) ring[r & mask] = next_word(r);
 	__syncthreads();
-	while (j0 < end) {
-		for (int t = threadIdx.x; t < chunk; t += blockDim.x) {
-			const unsigned long long j = j0 + t;
-			if (j < end) {
-				const unsigned long long w = jb.first + (j - n);  // output index
-				if (w >= jb.offset) jb.out[w - jb.offset] = temper(ring[j & mask], p);
-			}
+	const long long steps = (count + chunk - 1) / chunk;
+	for (long long st = 0; st < steps; ++st) {
+		if (owner) {
+			if (rem > 0 && o >= 0) out[o] = temper(ring[r & mask], p);
+			if (rem > chunk) ring[(r + chunk) & mask] = next_word(r + chunk);
+			r += chunk;
+			o += chunk;
+			rem -= chunk;
 		}
-		compute(j0 + chunk);
 		__syncthreads();
-		j0 += chunk;
 	}
 }
 
