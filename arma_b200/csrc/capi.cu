@@ -72,8 +72,10 @@ void white_noise(Ctx* c, const arma_mt_params& p, uint32_t seed, double stddev, 
 
 // White noise for many surfaces: all MT streams in one launch (one CTA per
 // stream), the polar transforms enqueued back to back, one host check.
-void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
-                       const std::vector<void*>& dz) {
+// Enqueue the white noise of n surfaces (MT words, then the polar method);
+// returns the device array of accepted pairs per surface.
+long long* white_noise_batch_enqueue(Ctx* c, const arma_surface* s, int n, int precision,
+                                     const std::vector<void*>& dz) {
 	std::vector<MtJob> jobs(n);
 	std::vector<uint64_t> att(n);
 	for (int k = 0; k < n; ++k) {
@@ -92,13 +94,26 @@ void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
 		specs[k] = NoiseSpec{jobs[k].out, 4 * att[k], np, std::sqrt(s[k].var_wn), dz[k]};
 	}
 	enqueue_white_noise_batch(c, specs, precision, d_pairs);
+	return d_pairs;
+}
+
+// True when surface k's accepted pairs do not cover its points (rare: the
+// attempts carry an 8 sigma margin).
+bool noise_short(const arma_surface& s, long long pairs) {
+	const size_t np = size_t(s.shape[0]) * s.shape[1] * s.shape[2];
+	return uint64_t(pairs) * 2 < np;
+}
+
+void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
+                       const std::vector<void*>& dz) {
+	long long* d_pairs = white_noise_batch_enqueue(c, s, n, precision, dz);
 	std::vector<long long> pairs(n);
 	ARMA_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(long long) * n,
 	                              cudaMemcpyDeviceToHost, c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	for (int k = 0; k < n; ++k) {
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
-		if (uint64_t(pairs[k]) * 2 < np)  // rare: not enough accepted attempts
+		if (noise_short(s[k], pairs[k]))  // the sequential generator instead
 			white_noise(c, s[k].mt, s[k].seed, std::sqrt(s[k].var_wn), np, precision, dz[k]);
 	}
 }
@@ -791,17 +806,16 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 }
 
 // FP32 surfaces into host buffers with the device->host copies overlapped with
-// the computation.  The batch is split into groups (10 % of the total points x
-// taps first, then three of 30 %); the first group's white noise, filter and
-// renormalisation run alone, so that its device->host copies (on a copy
-// stream) start early and overlap the noise of all other groups, generated
-// next in one batch; then each further group's filter and renormalisation run
-// on the context's stream while the previous groups' copies drain.  The PCIe
-// copies are the slower stream (about 0.76 ms per % of the bench batch
-// against 0.62 ms of filter), so after the first group they run back to back.
+// the computation.  The batch is split into groups of decreasing work (35, 30,
+// 20, 15 % of the total points x taps); each group's white noise, filter and
+// renormalisation run on the context's stream and its device->host copies on
+// a copy stream, overlapping the next group's computation.  Per % of the bench
+// batch the copies take about 0.76 ms and the computation about 0.9 ms (noise
+// and filter, with the tail of each group's persistent launch), so the copies
+// keep up and only the last, smallest group's are exposed.
 void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz) {
 	constexpr int G = 4;
-	const double frac[G] = {0.10, 0.30, 0.30, 0.30};
+	const double frac[G] = {0.35, 0.30, 0.20, 0.15};
 	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
 	std::vector<double> work(n);
 	double total = 0.0;
@@ -835,15 +849,18 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 	}
 	const std::vector<Ar32Surface> as =
 	    ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
-	auto noise = [&](int g0, int g1) {  // white noise of groups [g0, g1) in one batch
+	// Each group's noise is enqueued without reading its accepted-pair counts
+	// back (a device->host read on the context's stream would queue behind the
+	// previous groups' copies); the counts are checked at the end.
+	std::vector<long long*> d_pairs(G, nullptr);
+	auto noise = [&](int g) {
 		std::vector<arma_surface> sub;
 		std::vector<void*> dsub;
-		for (int g = g0; g < g1; ++g)
-			for (int k : members[g]) {
-				sub.push_back(s[k]);
-				dsub.push_back(dz[k]);
-			}
-		if (!sub.empty()) white_noise_batch(c, sub.data(), int(sub.size()), ARMA_FP32C, dsub);
+		for (int k : members[g]) {
+			sub.push_back(s[k]);
+			dsub.push_back(dz[k]);
+		}
+		d_pairs[g] = white_noise_batch_enqueue(c, sub.data(), int(sub.size()), ARMA_FP32C, dsub);
 	};
 	if (!c->copy_stream)
 		ARMA_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
@@ -854,9 +871,8 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 	};
 	try {
 		for (int g = 0; g < G; ++g) {
-			if (g == 0) noise(0, 1);
-			if (g == 1) noise(1, G);
 			if (members[g].empty()) continue;
+			noise(g);
 			std::vector<Ar32Surface> ga;
 			std::vector<RenormSpec> rs;
 			for (int k : members[g]) {
@@ -885,6 +901,16 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 		ARMA_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
 		check_device_error(c);
 		for (int k = 0; k < n; ++k) s[k].scale = s[k].acf0 > 0.0 ? sc[k] : 1.0;
+		// a surface whose noise ran short is generated again on its own
+		for (int g = 0; g < G; ++g) {
+			if (members[g].empty()) continue;
+			std::vector<long long> pairs(members[g].size());
+			ARMA_CUDA_TRY(cudaMemcpy(pairs.data(), d_pairs[g], sizeof(long long) * pairs.size(),
+			                         cudaMemcpyDeviceToHost));
+			for (size_t q = 0; q < pairs.size(); ++q)
+				if (noise_short(s[members[g][q]], pairs[q]))
+					batch(c, &s[members[g][q]], 1, ARMA_FP32C, true);
+		}
 	} catch (...) {
 		cudaStreamSynchronize(c->copy_stream);
 		release();
