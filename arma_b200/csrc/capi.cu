@@ -766,7 +766,12 @@ void renorm_surfaces(Ctx* c, arma_surface* s, int n, int precision, const std::v
                      bool host);
 void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz);
 
-void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
+// redo: the noise's accepted-pair counts are read back before the filter
+// (white_noise_batch, with its sequential fallback); otherwise the FP32 path
+// enqueues the noise, builds the filter's coefficient tables on the host while
+// the device generates it, and checks the counts at the end, generating a
+// surface whose noise ran short again on its own.
+void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo = false) {
 	const size_t es = elem_size(precision);
 	std::vector<void*> dz(n);
 	for (int k = 0; k < n; ++k) {
@@ -778,31 +783,42 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host) {
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
 		dz[k] = host ? scratch_take(c, np * es) : s[k].d_zeta;
 	}
-	if (host && precision == ARMA_FP32C && n >= 4) {
+	if (host && precision == ARMA_FP32C && n >= 4 && !redo) {
 		pipelined_host_output(c, s, n, dz);
 		return;
 	}
-	white_noise_batch(c, s, n, precision, dz);
 	if (precision == ARMA_FP64) {
+		white_noise_batch(c, s, n, precision, dz);
 		for (int k = 0; k < n; ++k) ar_filter(c, s[k].phi, s[k].order, s[k].shape, precision, dz[k]);
-	} else {
-		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
-		std::vector<const double*> phis(n);
-		std::vector<const int*> ords(n), shps(n);
-		std::vector<float*> zs(n);
-		for (int k = 0; k < n; ++k) {
-			phis[k] = s[k].phi;
-			ords[k] = s[k].order;
-			shps[k] = s[k].shape;
-			zs[k] = static_cast<float*>(dz[k]);
-		}
-		std::vector<Ar32Surface> as =
-		    ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
-		launch_ar32c(c, as, tx, ty, 1);
-		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
-		check_device_error(c);
+		renorm_surfaces(c, s, n, precision, dz, host);
+		return;
 	}
+	long long* d_pairs = nullptr;
+	if (redo) white_noise_batch(c, s, n, precision, dz);
+	else d_pairs = white_noise_batch_enqueue(c, s, n, precision, dz);
+	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
+	std::vector<const double*> phis(n);
+	std::vector<const int*> ords(n), shps(n);
+	std::vector<float*> zs(n);
+	for (int k = 0; k < n; ++k) {
+		phis[k] = s[k].phi;
+		ords[k] = s[k].order;
+		shps[k] = s[k].shape;
+		zs[k] = static_cast<float*>(dz[k]);
+	}
+	std::vector<Ar32Surface> as =
+	    ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
+	launch_ar32c(c, as, tx, ty, 1);
+	std::vector<long long> pairs(n, 0);
+	if (d_pairs)
+		ARMA_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(long long) * n,
+		                              cudaMemcpyDeviceToHost, c->stream));
+	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+	check_device_error(c);
 	renorm_surfaces(c, s, n, precision, dz, host);
+	if (d_pairs)
+		for (int k = 0; k < n; ++k)
+			if (noise_short(s[k], pairs[k])) batch(c, &s[k], 1, precision, host, true);
 }
 
 // FP32 surfaces into host buffers with the device->host copies overlapped with
@@ -909,7 +925,7 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 			                         cudaMemcpyDeviceToHost));
 			for (size_t q = 0; q < pairs.size(); ++q)
 				if (noise_short(s[members[g][q]], pairs[q]))
-					batch(c, &s[members[g][q]], 1, ARMA_FP32C, true);
+					batch(c, &s[members[g][q]], 1, ARMA_FP32C, true, true);
 		}
 	} catch (...) {
 		cudaStreamSynchronize(c->copy_stream);
