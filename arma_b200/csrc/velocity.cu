@@ -354,8 +354,12 @@ __device__ __forceinline__ int rotate_src(int i, int n) {
 __device__ double window_raw(int i, int j, double dkx, double dky, double z, double h) {
 	const double u = dkx * i, v = dky * j;
 	const double l = k2Pi * sqrt(u * u + v * v);
-	const double explz = exp(-l * z);
-	const double exp2lh = exp(-2.0 * l * h);
+	// the exponentials' exact values where the argument is exactly 0 (z = 0)
+	// or -inf (infinite depth) skip the FP64 exp; l = 0 at infinite depth
+	// still gives exp(NaN) = NaN, as in the reference
+	const double az = -l * z, ah = -2.0 * l * h;
+	const double explz = az == 0.0 ? 1.0 : exp(az);
+	const double exp2lh = ah == -INFINITY ? 0.0 : exp(ah);
 	const double num = 1.0 + explz * explz * exp2lh;
 	const double den = explz * (1.0 + exp2lh);
 	return k2Pi * 2.0 * num / den;
