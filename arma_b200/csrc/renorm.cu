@@ -157,16 +157,26 @@ __global__ void finish_batch_kernel(const RenormJob* __restrict__ jobs,
 	else *jb.scale = sqrt(jb.acf0 / (t / double(jb.cnt - 1)));
 }
 
+// Blocks in proportion to each surface's points (kScaleChunk elements per
+// block), so that the largest surfaces do not trail; block b belongs to the
+// last job whose first block is <= b.
+constexpr int kScaleChunk = kThreads * 16;
+
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-scale_batch_kernel(const RenormJob* __restrict__ jobs, int blocks_per_job) {
-	const int s = blockIdx.x / blocks_per_job, b = blockIdx.x % blocks_per_job;
-	const RenormJob& jb = jobs[s];
+scale_batch_kernel(const RenormJob* __restrict__ jobs, const int* __restrict__ first_block,
+                   int njobs) {
+	int lo = 0, hi = njobs - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) / 2;
+		if (first_block[mid] <= int(blockIdx.x)) lo = mid; else hi = mid - 1;
+	}
+	const RenormJob& jb = jobs[lo];
 	T* x = static_cast<T*>(jb.z);
 	const double sc = *jb.scale;
-	for (unsigned long long i = (unsigned long long)b * kThreads + threadIdx.x; i < jb.n;
-	     i += (unsigned long long)blocks_per_job * kThreads)
-		x[i] = T(double(x[i]) * sc);
+	const unsigned long long i0 = (unsigned long long)(blockIdx.x - first_block[lo]) * kScaleChunk;
+	const unsigned long long i1 = min(jb.n, i0 + kScaleChunk);
+	for (unsigned long long i = i0 + threadIdx.x; i < i1; i += kThreads) x[i] = T(double(x[i]) * sc);
 }
 
 }  // namespace
@@ -188,6 +198,15 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 		ARMA_REQUIRE(j.cnt >= 2, ARMA_EINVAL, "surface too small for variance renormalisation");
 	}
 	const int ns = int(jobs.size());
+	std::vector<int> first(ns);
+	int sblocks = 0;
+	for (int k = 0; k < ns; ++k) {
+		first[k] = sblocks;
+		sblocks += int((jobs[k].n + kScaleChunk - 1) / kScaleChunk);
+	}
+	int* d_first = static_cast<int*>(scratch_take(c, sizeof(int) * ns));
+	ARMA_CUDA_TRY(cudaMemcpyAsync(d_first, first.data(), sizeof(int) * ns, cudaMemcpyHostToDevice,
+	                              c->stream));
 	auto* d_jobs = static_cast<RenormJob*>(scratch_take(c, sizeof(RenormJob) * jobs.size()));
 	double* partial = static_cast<double*>(scratch_take(c, sizeof(double) * ns * kBatchBlocks));
 	double* means = static_cast<double*>(scratch_take(c, sizeof(double) * ns));
@@ -199,13 +218,15 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 0, means);
 		partial_batch_kernel<double><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
-		if (apply) scale_batch_kernel<double><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
+		if (apply)
+			scale_batch_kernel<double><<<sblocks, kThreads, 0, c->stream>>>(d_jobs, d_first, ns);
 	} else {
 		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, nullptr, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 0, means);
 		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
-		if (apply) scale_batch_kernel<float><<<ns * 64, kThreads, 0, c->stream>>>(d_jobs, 64);
+		if (apply)
+			scale_batch_kernel<float><<<sblocks, kThreads, 0, c->stream>>>(d_jobs, d_first, ns);
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += apply ? 5 : 4;
