@@ -44,7 +44,7 @@ EXPORTS = (
     "arma_server_poll", "arma_server_stats_get", "arma_server_last_failure",
     "arma_server_profile", "arma_velocity_linear_batch", "arma_validate_process",
     "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf", "arma_velocity_high_amplitude",
-    "arma_ma_fit", "arma_ma_filter", "arma_ma_generate",
+    "arma_ma_fit", "arma_ma_filter", "arma_ma_generate", "arma_ctx_set_noise_margin",
 )
 
 
@@ -200,6 +200,7 @@ def lib():
             "arma_ma_fit": (i, [dp, ip, ip, dp, dp, ip]),
             "arma_ma_filter": (i, [vp, dp, ip, ip, i, vp, vp]),
             "arma_ma_generate": (i, [vp, C.POINTER(Surface), i, i]),
+            "arma_ctx_set_noise_margin": (i, [vp, d]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -383,6 +384,10 @@ class Context:
         n = C.c_uint64()
         _check(lib().arma_ctx_profile(self._h, name.encode(), C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def set_noise_margin(self, margin: float):
+        """Polar-attempt estimate multiplier of the batched calls (default 1)."""
+        _check(lib().arma_ctx_set_noise_margin(self._h, float(margin)))
 
     def profile_reset(self):
         _check(lib().arma_ctx_profile_reset(self._h))

@@ -82,7 +82,7 @@ long long* white_noise_batch_enqueue(Ctx* c, const arma_surface* s, int n, int p
 		ARMA_REQUIRE(s[k].var_wn >= 0.0 && std::isfinite(s[k].var_wn), ARMA_EINVAL,
 		             "variance is less than zero");
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
-		att[k] = noise_attempts(np, 1.0);
+		att[k] = noise_attempts(np, c->noise_margin);
 		jobs[k] = MtJob{s[k].mt, s[k].seed, 0, 4 * att[k],
 		                static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * 4 * att[k]))};
 	}
@@ -339,6 +339,15 @@ int arma_ctx_set_profiling(arma_ctx* ctx, int enabled) {
 	return guard([&] {
 		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
 		ctx->c.profiling = enabled != 0;
+	});
+}
+
+int arma_ctx_set_noise_margin(arma_ctx* ctx, double margin) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
+		ARMA_REQUIRE(margin > 0.0 && std::isfinite(margin), ARMA_EINVAL,
+		             "noise margin must be positive");
+		ctx->c.noise_margin = margin;
 	});
 }
 

@@ -51,6 +51,7 @@ struct Ctx {
 	bool own_stream = false;
 	int* d_err = nullptr;            // device error word
 	cudaStream_t copy_stream = nullptr;  // device->host copies overlapped with compute (lazy)
+	double noise_margin = 1.0;           // polar-attempt estimate multiplier of the batched calls
 	uint64_t launches = 0;           // kernel launches issued
 	int num_sms = 148;
 	// cached CUDA graphs for the FP64 plane sweep, keyed by a string

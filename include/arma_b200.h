@@ -86,6 +86,13 @@ int arma_ctx_launch_count(arma_ctx* ctx, uint64_t* count);
 int arma_ctx_set_profiling(arma_ctx* ctx, int enabled);
 int arma_ctx_profile(arma_ctx* ctx, const char* name, double* ms, uint64_t* launches);
 int arma_ctx_profile_reset(arma_ctx* ctx);
+/* Multiplier (> 0, default 1) of the polar-attempt estimate (expected count
+ * plus 8 sigma) with which the batched generation calls (arma_batch_generate,
+ * arma_batch_generate_host, arma_ma_generate) draw each surface's dcmt words.
+ * No counterpart in the reference, which draws one word at a time.  A
+ * surface whose noise runs short is generated again on its own, so the
+ * results do not depend on it; values below 1 make that path likely. */
+int arma_ctx_set_noise_margin(arma_ctx* ctx, double margin);
 
 /* ------------------------------------------------- A6: dcmt parameter sets */
 /* Replaces read_parallel_mt_config / read_parallel_mts

@@ -244,6 +244,52 @@ def test_batch_host_buffers_fp32_pipelined(ctx):
         assert np.array_equal(h, dev[k].cpu().numpy()), k
 
 
+def test_short_noise_regeneration_is_exact(ctx):
+    """With a polar-attempt margin of 0.5 every surface's noise runs short; the
+    batched calls then generate such a surface again on its own (device
+    buffers, the pipelined host-buffer path, the FP64 path and the MA model)
+    and the results equal those at the default margin bit for bit."""
+    import torch
+    p = A.mt19937_params()
+    shapes = [(30, 32, 48), (20, 64, 32), (25, 40, 40), (18, 33, 70), (22, 16, 64)]
+    fits = [A.ar_fit_analytic(A.ACF_STANDING, (3 + k % 2,) * 3, 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+            for k in range(len(shapes))]
+
+    def run():
+        out = []
+        for prec, dt in ((A.FP32C, torch.float32), (A.FP64, torch.float64)):
+            dev = [torch.empty(sh, dtype=dt, device="cuda") for sh in shapes]
+            sd = [capi.make_surface(sh, f[0], f[1], 1.5, p, 500 + k, b.data_ptr())
+                  for k, (sh, f, b) in enumerate(zip(shapes, fits, dev))]
+            sc = ctx.batch_generate(sd, prec)
+            ctx.synchronize()
+            out.append(([b.cpu().numpy() for b in dev], sc))
+        host = [np.zeros(sh, np.float32) for sh in shapes]
+        sh_ = [capi.make_surface(sh, f[0], f[1], 1.5, p, 500 + k, h.ctypes.data)
+               for k, (sh, f, h) in enumerate(zip(shapes, fits, host))]
+        out.append(([h.copy() for h in host], ctx.batch_generate(sh_, A.FP32C, host=True)))
+        theta, var, _ = A.ma_fit(np.exp(-np.add.outer(np.add.outer(np.arange(6), np.arange(6)),
+                                                       np.arange(6)) * 0.7), (3, 3, 3))
+        ma = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh in shapes[:2]]
+        sm = [capi.make_surface(sh, theta, var, 1.0, p, 700 + k, b.data_ptr())
+              for k, (sh, b) in enumerate(zip(shapes[:2], ma))]
+        out.append(([b.cpu().numpy() for b in ma], ctx.ma_generate(sm, A.FP32C)))
+        return out
+
+    base = run()
+    try:
+        ctx.set_noise_margin(0.5)
+        short = run()
+    finally:
+        ctx.set_noise_margin(1.0)
+    for (za, sa), (zb, sb) in zip(base, short):
+        assert sa == sb
+        for a, b in zip(za, zb):
+            assert np.array_equal(a, b)
+    with pytest.raises(capi.ArmaError):
+        ctx.set_noise_margin(0.0)
+
+
 def test_errors_are_reported(ctx):
     with pytest.raises(capi.ArmaError):
         ctx.ar_filter(np.zeros((2, 2, 2)), (0, 4, 4), A.FP64, 0)
