@@ -7,7 +7,8 @@ Tolerances (stated per test):
   * FP64 AR filter: bit-exact with the oracle given the same noise (same
     summation order, explicitly rounded operations).
   * FP32 compensated AR filter: RMS error <= 1e-5 relative to the FP64 result
-    on the same noise; max-abs error reported.
+    on the same noise (the precision target of the FP32 form); max-abs error
+    reported.
   * renormalisation: 1e-12 relative.
   * NIT bisection: 2e-6 absolute (bisection tolerance 1e-6); NIT LUT: 5e-5.
 """
