@@ -60,6 +60,12 @@ constexpr int W = LH + TY;        // ring row width (floats)
 constexpr int SPAD = TY + 8;      // zero padding left of each S row
 constexpr int SW = SPAD + TY + 4; // S row width (padded against bank conflicts)
 constexpr int MAXO = 13;          // max order per axis supported (py <= LH+1)
+constexpr int HS = TY + 4;        // H row stride in shared memory (bank spread)
+constexpr int HCH = 3;            // rows of H per H work unit
+constexpr int HPAIR = 51;         // H work units per strip pair: sum_x ceil((x+1)/HCH)
+constexpr int HUNITS = 2 * HPAIR; // H work units per tile slice (<= NCOMP)
+constexpr int PS = 2 * R + 4;     // partial record stride (bank spread)
+static_assert(TX == 16 && TY == 4 * R && HUNITS <= NCOMP, "H work-unit table assumes 16 x 4R tiles");
 constexpr long long kSpinLimit = 1ll << 24;
 
 struct Task {
@@ -125,82 +131,109 @@ __device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need
 	return false;
 }
 
-// zeta = H * S over the quarter plane of one tile for the output strip
-// (xl, yl0 .. yl0+R-1), dx restricted to [dx_lo, min(dx_hi, xl+1)): writes the
-// Kahan-compensated partial strip to out[0..R).  Per row of H the column
-// blocks run from dy0 = yl0 down to 0, so the one block that reaches only the
-// taps dd <= r comes first for every lane and runs as a triangle.  Shared by every tap-count
-// instantiation of run_tile, so its code exists once.
-__device__ __noinline__ void h_phase(const float* ss, const float* sh, int xl, int yl0, int dx_lo,
-                                     int dx_hi, float* out) {
-	float a[R], ac[R];
-#pragma unroll
-	for (int r = 0; r < R; ++r) { a[r] = 0.0f; ac[r] = 0.0f; }
-	const int dx_end = min(dx_hi - 1, xl);
-	for (int dx = dx_lo; dx <= dx_end; ++dx) {
-		const float* srow = ss + (xl - dx) * SW + SPAD;
-		const float* hrow = sh + dx * TY;
-		float pr[R];
-#pragma unroll
-		for (int r = 0; r < R; ++r) pr[r] = 0.0f;
-		{
-			// the block dy0 = yl0 first (every lane at once): its sources
-			// srow[0 .. R-1] reach only the taps dd <= r
-			float wt[R], hv[R];
-			const float4* sp = reinterpret_cast<const float4*>(srow);
-			const float4* hp = reinterpret_cast<const float4*>(hrow + yl0);
-#pragma unroll
-			for (int q = 0; q < R / 4; ++q) {
-				const float4 v = sp[q];
-				wt[4 * q] = v.x;
-				wt[4 * q + 1] = v.y;
-				wt[4 * q + 2] = v.z;
-				wt[4 * q + 3] = v.w;
-				const float4 u = hp[q];
-				hv[4 * q] = u.x;
-				hv[4 * q + 1] = u.y;
-				hv[4 * q + 2] = u.z;
-				hv[4 * q + 3] = u.w;
-			}
-#pragma unroll
-			for (int r = 0; r < R; ++r) {
-#pragma unroll
-				for (int dd = 0; dd <= r; ++dd) pr[r] = fmaf(hv[dd], wt[r - dd], pr[r]);
-			}
-		}
-		for (int dy0 = yl0 - R; dy0 >= 0; dy0 -= R) {
-			// sources srow[yl0 - dy0 - 8 .. yl0 - dy0 + 7]
-			float w[2 * R];
-			const float4* sp = reinterpret_cast<const float4*>(srow + yl0 - dy0 - R);
-#pragma unroll
-			for (int q = 0; q < 2 * R / 4; ++q) {
-				const float4 v = sp[q];
-				w[4 * q] = v.x;
-				w[4 * q + 1] = v.y;
-				w[4 * q + 2] = v.z;
-				w[4 * q + 3] = v.w;
-			}
-			float hv[R];
-			const float4* hp = reinterpret_cast<const float4*>(hrow + dy0);
-#pragma unroll
-			for (int q = 0; q < R / 4; ++q) {
-				const float4 v = hp[q];
-				hv[4 * q] = v.x;
-				hv[4 * q + 1] = v.y;
-				hv[4 * q + 2] = v.z;
-				hv[4 * q + 3] = v.w;
-			}
-#pragma unroll
-			for (int r = 0; r < R; ++r) {
-#pragma unroll
-				for (int dd = 0; dd < R; ++dd) pr[r] = fmaf(hv[dd], w[R + r - dd], pr[r]);
-			}
-		}
-#pragma unroll
-		for (int r = 0; r < R; ++r) kahan_add(a[r], ac[r], pr[r]);
+// zeta = H * S over the quarter plane of one tile, cut into work units of
+// equal cost.  Row x of the output needs the x+1 rows dx = 0..x of H, each a
+// causal 1-D convolution along y; the four 8-column strips of a row cost 1, 2,
+// 3 and 4 blocks of R x R taps (the first block of each a triangle), so the
+// strips are paired (3, 0) and (2, 1): either pair costs two triangles and
+// three full blocks per row of H.  A unit is one strip pair of one output row
+// over at most HCH consecutive rows of H; units are numbered pair-major, then
+// by row, then by dx chunk, so row x's units start at HPAIR * pair +
+// h_rowbase(x).  Unit u writes its Kahan-compensated partial (strip X in
+// slots 0..R-1, strip Y in R..2R-1) to part[u * PS ..].  Lanes of one warp
+// work on different rows of H at once: H rows are HS floats apart in shared
+// memory so that their 16-byte loads fall in different banks.
+__device__ __forceinline__ int h_rowbase(int x) {
+	// sum over x' < x of ceil((x'+1) / HCH), for HCH = 3
+	const int q = x / 3, r = x % 3;
+	return x + 3 * q * (q - 1) / 2 + r * q;
+}
+
+__device__ __forceinline__ void load_row(float* d, const float* s, int n4) {
+#pragma unroll 4
+	for (int q = 0; q < n4; ++q) {
+		const float4 v = reinterpret_cast<const float4*>(s)[q];
+		d[4 * q] = v.x;
+		d[4 * q + 1] = v.y;
+		d[4 * q + 2] = v.z;
+		d[4 * q + 3] = v.w;
 	}
+}
+
+// acc[r] += sum_dd hv[dd] src[R + r - dd]: one full R x R block of taps
+__device__ __forceinline__ void h_block(float* acc, const float* src, const float* hrow) {
+	float w[2 * R], hv[R];
+	load_row(w, src, 2 * R / 4);
+	load_row(hv, hrow, R / 4);
 #pragma unroll
-	for (int r = 0; r < R; ++r) out[r] = a[r] - ac[r];
+	for (int r = 0; r < R; ++r) {
+#pragma unroll
+		for (int dd = 0; dd < R; ++dd) acc[r] = fmaf(hv[dd], w[R + r - dd], acc[r]);
+	}
+}
+
+__device__ __noinline__ void h_unit(const float* ss, const float* sh, int u, float* part) {
+	const int pair = u >= HPAIR ? 1 : 0;
+	const int v = u - pair * HPAIR;
+	int x = 0;
+	while (x + 1 < TX && h_rowbase(x + 1) <= v) ++x;
+	const int dx0 = HCH * (v - h_rowbase(x));
+	const int dx1 = min(dx0 + HCH, x + 1);
+	const int yx = pair ? 2 * R : 3 * R;  // first column of strip X
+	const int yy = pair ? R : 0;          // first column of strip Y
+	const int w3 = pair ? 0 : 2 * R;      // sources of the third block
+	float aX[R], cX[R], aY[R], cY[R];
+#pragma unroll
+	for (int r = 0; r < R; ++r) { aX[r] = 0.0f; cX[r] = 0.0f; aY[r] = 0.0f; cY[r] = 0.0f; }
+	for (int dx = dx0; dx < dx1; ++dx) {
+		const float* srow = ss + (x - dx) * SW + SPAD;
+		const float* hrow = sh + dx * HS;
+		float pX[R], pY[R], wt[R], hv[R];
+		// triangle of strip X: its block dy0 = yx reaches sources srow[0 .. r]
+		load_row(wt, srow, R / 4);
+		load_row(hv, hrow + yx, R / 4);
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+			pX[r] = 0.0f;
+#pragma unroll
+			for (int dd = 0; dd <= r; ++dd) pX[r] = fmaf(hv[dd], wt[r - dd], pX[r]);
+		}
+		// strip X's blocks dy0 = yx - R and yx - 2R
+		h_block(pX, srow, hrow + yx - R);
+		h_block(pX, srow + R, hrow + yx - 2 * R);
+		// third block: strip 3's dy0 = 0 (pair 0) or strip 1's dy0 = 0 (pair 1),
+		// accumulated in pY, whose strip has no other term yet
+#pragma unroll
+		for (int r = 0; r < R; ++r) pY[r] = pair ? 0.0f : pX[r];
+		h_block(pY, srow + w3, hrow);
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+			pX[r] = pair ? pX[r] : pY[r];
+			pY[r] = pair ? pY[r] : 0.0f;
+		}
+		// triangle of strip Y
+		load_row(hv, hrow + yy, R / 4);
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+#pragma unroll
+			for (int dd = 0; dd <= r; ++dd) pY[r] = fmaf(hv[dd], wt[r - dd], pY[r]);
+		}
+#pragma unroll
+		for (int r = 0; r < R; ++r) {
+			kahan_add(aX[r], cX[r], pX[r]);
+			kahan_add(aY[r], cY[r], pY[r]);
+		}
+	}
+	float* out = part + u * PS;
+#pragma unroll
+	for (int q4 = 0; q4 < R / 4; ++q4) {
+		reinterpret_cast<float4*>(out)[q4] =
+		    make_float4(aX[4 * q4] - cX[4 * q4], aX[4 * q4 + 1] - cX[4 * q4 + 1],
+		                aX[4 * q4 + 2] - cX[4 * q4 + 2], aX[4 * q4 + 3] - cX[4 * q4 + 3]);
+		reinterpret_cast<float4*>(out + R)[q4] =
+		    make_float4(aY[4 * q4] - cY[4 * q4], aY[4 * q4 + 1] - cY[4 * q4 + 1],
+		                aY[4 * q4 + 2] - cY[4 * q4 + 2], aY[4 * q4 + 3] - cY[4 * q4 + 3]);
+	}
 }
 
 template <int PY>
@@ -222,10 +255,10 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 	float* ring = smem;                          // pt slots
 	float* sphi = ring + pt * slot_sz;           // pt*px*PYP (hi)
 	float* slo = sphi + pt * px * PYP;           // pt*px*PYP (lo)
-	float* sh = slo + pt * px * PYP;             // TX*TY
-	float* ss = sh + TX * TY;                    // TX*SW
-	float* comb = ss + TX * SW;                  // GROUP*R: group 1 partials
-	float* hres = comb + GROUP * R;              // NCOMP*R: H-phase partials
+	float* sh = slo + pt * px * PYP;             // TX*HS
+	float* ss = sh + TX * HS;                    // TX*SW
+	float* part = ss + TX * SW;                  // HUNITS*PS: H-unit partials
+	float* comb = part;                          // GROUP*R: group 1 partials (before H)
 
 	// stage coefficients (rows padded with zeros), H, zero the ring and S pads
 	for (int q = tid; q < pt * px * PYP; q += NTHREADS) {
@@ -239,7 +272,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 		for (int j = 0; j < PY; ++j) nz = nz || tk.phi_lo[ki * PY + j] != 0.0f;
 		s_lo[ki] = nz ? 1 : 0;
 	}
-	for (int q = tid; q < TX * TY; q += NTHREADS) sh[q] = tk.h[q];
+	for (int q = tid; q < TX * TY; q += NTHREADS) sh[(q / TY) * HS + q % TY] = tk.h[q];
 	for (int q = tid; q < pt * slot_sz; q += NTHREADS) ring[q] = 0.0f;
 	for (int q = tid; q < TX * SW; q += NTHREADS) ss[q] = 0.0f;
 	__syncthreads();
@@ -328,11 +361,6 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 	}
 
 	const int gx = x0 + xl;
-	// H-phase share of this group: rows 0-7 split dx at 4, rows 8-15 at 8, so
-	// every warp runs at most 8 dx iterations
-	const int half = xl >> 3;
-	const int dx_lo = grp == 0 ? 0 : (half ? 8 : 4);
-	const int dx_hi = grp == 0 ? (half ? 8 : 4) : TX;
 
 	for (int t = tk.t0; t < tk.nt; ++t) {
 		float* cur = ring + (t % pt) * slot_sz;
@@ -431,19 +459,38 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 		}
 		bar_sync(BAR_COMP, NCOMP);
 
-		//    zeta = H * S over the quarter plane of the tile
-		h_phase(ss, sh, xl, yl0, dx_lo, dx_hi, hres + tid * R);
+		//    zeta = H * S over the quarter plane of the tile, in work units
+		if (tid < HUNITS) h_unit(ss, sh, tid, part);
 
-		// 5. store the solved slice; the halo warp publishes it
+		// 5. sum each output's unit partials (Kahan, in dx order), store the
+		//    solved slice; the halo warp publishes it
 		bar_sync(BAR_COMP, NCOMP);
-		if (grp == 0) {
-			float* own = cur + hx * W + LH;
+		{
+			// this thread's outputs: row ox, columns oy0 .. oy0+3
+			const int ox = tid / (2 * STRIPS);
+			const int ostrip = (tid / 2) % STRIPS;
+			const int oy0 = ostrip * R + (tid % 2) * 4;
+			const int opart = (ostrip == 0 || ostrip == 3 ? 0 : HPAIR) + h_rowbase(ox);
+			const int oslot = (ostrip >= 2 ? 0 : R) + (tid % 2) * 4;
+			const int ogx = x0 + ox;
+			float a[4], ac[4];
 #pragma unroll
-			for (int r = 0; r < R; ++r) {
-				const float v = hres[tid * R + r] + hres[(tid + GROUP) * R + r];
-				own[xl * W + yl0 + r] = v;
-				const int gy = y0 + yl0 + r;
-				if (gx < tk.nx && gy < tk.ny) zt[(long long)gx * tk.ny + gy] = v;
+			for (int e = 0; e < 4; ++e) { a[e] = 0.0f; ac[e] = 0.0f; }
+			const int nch = ox / HCH + 1;
+			for (int ch = 0; ch < nch; ++ch) {
+				const float4 v = *reinterpret_cast<const float4*>(part + (opart + ch) * PS + oslot);
+				kahan_add(a[0], ac[0], v.x);
+				kahan_add(a[1], ac[1], v.y);
+				kahan_add(a[2], ac[2], v.z);
+				kahan_add(a[3], ac[3], v.w);
+			}
+			float* own = cur + hx * W + LH + ox * W + oy0;
+#pragma unroll
+			for (int e = 0; e < 4; ++e) {
+				const float v = a[e] - ac[e];
+				own[e] = v;
+				const int gy = y0 + oy0 + e;
+				if (ogx < tk.nx && gy < tk.ny) zt[(long long)ogx * tk.ny + gy] = v;
 			}
 		}
 		bar_sync(BAR_COMP, NCOMP);  // slice t in the ring for every compute thread
@@ -490,8 +537,8 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
 size_t smem_bytes(int pt, int px, int py) {
 	const int rows = TX + px - 1;
 	const int pyp = (py + 3) & ~3;
-	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + TX * TY + TX * SW +
-	                        GROUP * R + NCOMP * R);
+	return sizeof(float) * (size_t(pt) * rows * W + 2 * size_t(pt) * px * pyp + TX * HS + TX * SW +
+	                        std::max(GROUP * R, HUNITS * PS));
 }
 
 }  // namespace
