@@ -29,11 +29,12 @@
 // continued across the rows of one k plane, and the plane totals are combined
 // with Kahan compensation (per row, the compensation cost 7 % more time for
 // 0.2-1.2e-6 less RMS error).  H is applied in plain FP32, one FMA chain per
-// output over each row of H (up to 32 taps), the row totals Kahan-added: it
-// acts once per slice on the current slice alone, and its rounding changes
-// the surface by far less than phi's (a lo part for H moved the RMS error by
-// under 1e-7 at 18 % of the filter's time; compensating every 8 taps instead
-// of every row, by under 2e-7 at 11 %).  Tiles are handed out through a global ticket
+// output over up to three rows of H (up to 96 taps), the at most six chain
+// totals of an output Kahan-added: it acts once per slice on the current
+// slice alone, and its rounding changes the surface by far less than phi's (a
+// lo part for H moved the RMS error by under 1e-7 at 18 % of the filter's
+// time; Kahan-adding every row of H instead of every three rows, by 4e-8 at
+// 5 %).  Tiles are handed out through a global ticket
 // counter in dependency order, so a CTA only ever waits on tiles that are
 // already owned by running CTAs.
 #include <algorithm>
@@ -139,10 +140,13 @@ __device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need
 // three full blocks per row of H.  A unit is one strip pair of one output row
 // over at most HCH consecutive rows of H; units are numbered pair-major, then
 // by row, then by dx chunk, so row x's units start at HPAIR * pair +
-// h_rowbase(x).  Unit u writes its Kahan-compensated partial (strip X in
-// slots 0..R-1, strip Y in R..2R-1) to part[u * PS ..].  Lanes of one warp
-// work on different rows of H at once: H rows are HS floats apart in shared
-// memory so that their 16-byte loads fall in different banks.
+// h_rowbase(x).  Unit u writes its partial (strip X in slots 0..R-1, strip Y
+// in R..2R-1), one plain FP32 FMA chain per output, to part[u * PS ..]; the
+// partials of an output are Kahan-added afterwards.  Lanes of one warp work
+// on different rows of H at once: H rows are HS floats apart in shared memory
+// so that their 16-byte loads fall in different banks.  The unit is inlined
+// into every tap-count instantiation of run_tile: as a call, the registers
+// the caller keeps across it spilled, and the filter ran 7 % slower.
 __device__ __forceinline__ int h_rowbase(int x) {
 	// sum over x' < x of ceil((x'+1) / HCH), for HCH = 3
 	const int q = x / 3, r = x % 3;
@@ -172,7 +176,7 @@ __device__ __forceinline__ void h_block(float* acc, const float* src, const floa
 	}
 }
 
-__device__ __noinline__ void h_unit(const float* ss, const float* sh, int u, float* part) {
+__device__ __forceinline__ void h_unit(const float* ss, const float* sh, int u, float* part) {
 	const int pair = u >= HPAIR ? 1 : 0;
 	const int v = u - pair * HPAIR;
 	int x = 0;
@@ -182,34 +186,34 @@ __device__ __noinline__ void h_unit(const float* ss, const float* sh, int u, flo
 	const int yx = pair ? 2 * R : 3 * R;  // first column of strip X
 	const int yy = pair ? R : 0;          // first column of strip Y
 	const int w3 = pair ? 0 : 2 * R;      // sources of the third block
-	float aX[R], cX[R], aY[R], cY[R];
+	// one FMA chain per output over the unit's rows of H
+	float pX[R], pY[R];
 #pragma unroll
-	for (int r = 0; r < R; ++r) { aX[r] = 0.0f; cX[r] = 0.0f; aY[r] = 0.0f; cY[r] = 0.0f; }
+	for (int r = 0; r < R; ++r) { pX[r] = 0.0f; pY[r] = 0.0f; }
 	for (int dx = dx0; dx < dx1; ++dx) {
 		const float* srow = ss + (x - dx) * SW + SPAD;
 		const float* hrow = sh + dx * HS;
-		float pX[R], pY[R], wt[R], hv[R];
+		float wt[R], hv[R];
 		// triangle of strip X: its block dy0 = yx reaches sources srow[0 .. r]
 		load_row(wt, srow, R / 4);
 		load_row(hv, hrow + yx, R / 4);
 #pragma unroll
 		for (int r = 0; r < R; ++r) {
-			pX[r] = 0.0f;
 #pragma unroll
 			for (int dd = 0; dd <= r; ++dd) pX[r] = fmaf(hv[dd], wt[r - dd], pX[r]);
 		}
 		// strip X's blocks dy0 = yx - R and yx - 2R
 		h_block(pX, srow, hrow + yx - R);
 		h_block(pX, srow + R, hrow + yx - 2 * R);
-		// third block: strip 3's dy0 = 0 (pair 0) or strip 1's dy0 = 0 (pair 1),
-		// accumulated in pY, whose strip has no other term yet
+		// third block: strip 3's dy0 = 0 (pair 0) or strip 1's dy0 = 0 (pair 1)
+		float q[R];
 #pragma unroll
-		for (int r = 0; r < R; ++r) pY[r] = pair ? 0.0f : pX[r];
-		h_block(pY, srow + w3, hrow);
+		for (int r = 0; r < R; ++r) q[r] = pair ? pY[r] : pX[r];
+		h_block(q, srow + w3, hrow);
 #pragma unroll
 		for (int r = 0; r < R; ++r) {
-			pX[r] = pair ? pX[r] : pY[r];
-			pY[r] = pair ? pY[r] : 0.0f;
+			pX[r] = pair ? pX[r] : q[r];
+			pY[r] = pair ? q[r] : pY[r];
 		}
 		// triangle of strip Y
 		load_row(hv, hrow + yy, R / 4);
@@ -218,21 +222,14 @@ __device__ __noinline__ void h_unit(const float* ss, const float* sh, int u, flo
 #pragma unroll
 			for (int dd = 0; dd <= r; ++dd) pY[r] = fmaf(hv[dd], wt[r - dd], pY[r]);
 		}
-#pragma unroll
-		for (int r = 0; r < R; ++r) {
-			kahan_add(aX[r], cX[r], pX[r]);
-			kahan_add(aY[r], cY[r], pY[r]);
-		}
 	}
 	float* out = part + u * PS;
 #pragma unroll
 	for (int q4 = 0; q4 < R / 4; ++q4) {
 		reinterpret_cast<float4*>(out)[q4] =
-		    make_float4(aX[4 * q4] - cX[4 * q4], aX[4 * q4 + 1] - cX[4 * q4 + 1],
-		                aX[4 * q4 + 2] - cX[4 * q4 + 2], aX[4 * q4 + 3] - cX[4 * q4 + 3]);
+		    make_float4(pX[4 * q4], pX[4 * q4 + 1], pX[4 * q4 + 2], pX[4 * q4 + 3]);
 		reinterpret_cast<float4*>(out + R)[q4] =
-		    make_float4(aY[4 * q4] - cY[4 * q4], aY[4 * q4 + 1] - cY[4 * q4 + 1],
-		                aY[4 * q4 + 2] - cY[4 * q4 + 2], aY[4 * q4 + 3] - cY[4 * q4 + 3]);
+		    make_float4(pY[4 * q4], pY[4 * q4 + 1], pY[4 * q4 + 2], pY[4 * q4 + 3]);
 	}
 }
 
