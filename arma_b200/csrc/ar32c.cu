@@ -67,6 +67,7 @@ constexpr int HPAIR = 51;         // H work units per strip pair: sum_x ceil((x+
 constexpr int HUNITS = 2 * HPAIR; // H work units per tile slice (<= NCOMP)
 constexpr int PS = 2 * R + 4;     // partial record stride (bank spread)
 static_assert(TX == 16 && TY == 4 * R && HUNITS <= NCOMP, "H work-unit table assumes 16 x 4R tiles");
+constexpr int kMaxTapRows = MAXO * (TX + 1);  // (k, i) tap rows per model: pt * px
 constexpr long long kSpinLimit = 1ll << 24;
 
 struct Task {
@@ -502,7 +503,7 @@ ar32c_kernel(const Task* __restrict__ tasks, int ntasks, int total_tickets,
              int* __restrict__ ticket_counter, int* __restrict__ err) {
 	extern __shared__ __align__(16) float smem[];
 	__shared__ int s_ticket;
-	__shared__ unsigned char s_lo[MAXO * (TX + 1)];  // per (k, i) tap row: lo part present
+	__shared__ unsigned char s_lo[kMaxTapRows];  // per (k, i) tap row: lo part present
 	for (;;) {
 		if (threadIdx.x == 0) s_ticket = atomicAdd(ticket_counter, 1);
 		__syncthreads();
@@ -542,6 +543,7 @@ size_t smem_bytes(int pt, int px, int py) {
 
 int ar32c_tile_x() { return TX; }
 int ar32c_tile_y() { return TY; }
+int ar32c_max_tap_rows() { return kMaxTapRows; }
 
 void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int ty, int) {
 	ARMA_REQUIRE(tx == TX && ty == TY, ARMA_EINVAL, "unsupported AR tile shape");
@@ -549,7 +551,8 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 	size_t smem = 0;
 	for (size_t k = 0; k < surfaces.size(); ++k) {
 		const Ar32Surface& s = surfaces[k];
-		ARMA_REQUIRE(s.px <= TX + 1 && s.py <= MAXO && s.pt >= 1 && s.px >= 1 && s.py >= 1,
+		ARMA_REQUIRE(s.px <= TX + 1 && s.py <= MAXO && s.pt >= 1 && s.px >= 1 && s.py >= 1 &&
+		                 s.pt * s.px <= kMaxTapRows,
 		             ARMA_ENOTSUP, "AR order not supported by the FP32 tile kernel");
 		order[k] = int(k);
 		smem = std::max(smem, smem_bytes(s.pt, s.px, s.py));
@@ -665,7 +668,8 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 	if (!phi || !order || !shape || !d_zeta) return fail(ARMA_EINVAL, "null argument");
 	if (shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0)
 		return fail(ARMA_EINVAL, "Bad \"out_grid\": dimensions must be positive");
-	if (order[0] < 1 || order[1] < 1 || order[2] < 1 || order[1] > TX + 1 || order[2] > MAXO)
+	if (order[0] < 1 || order[1] < 1 || order[2] < 1 || order[1] > TX + 1 || order[2] > MAXO ||
+	    order[0] * order[1] > kMaxTapRows)
 		return fail(ARMA_ENOTSUP, "AR order not supported by the FP32 tile kernel");
 	const int P = order[0] * order[1] * order[2];
 	if (P > kStaticMaxTaps)

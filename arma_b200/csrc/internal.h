@@ -177,6 +177,7 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx,
                   int ty, int tt);
 int ar32c_tile_x();
 int ar32c_tile_y();
+int ar32c_max_tap_rows();  // largest pt * px of the FP32 tile kernel
 
 // Variance renormalisation: computes scale on device (d_scale) and applies it.
 void launch_renorm(Ctx* c, void* d_zeta, const int shape[3], int precision,

@@ -734,8 +734,8 @@ int arma_stream_open(arma_server* srv, const arma_stream_spec* spec, uint64_t* s
 		const int* o = spec->order;
 		ARMA_REQUIRE(spec->nx > 0 && spec->ny > 0 && o[0] > 0 && o[1] > 0 && o[2] > 0, ARMA_EINVAL,
 		             "Bad \"stream\": dimensions must be positive");
-		ARMA_REQUIRE(o[1] <= ar32c_tile_x() + 1 && o[2] <= 13, ARMA_ENOTSUP,
-		             "AR order not supported by the FP32 tile kernel");
+		ARMA_REQUIRE(o[1] <= ar32c_tile_x() + 1 && o[2] <= 13 && o[0] * o[1] <= ar32c_max_tap_rows(),
+		             ARMA_ENOTSUP, "AR order not supported by the FP32 tile kernel");
 		ARMA_REQUIRE(o[0] - 1 <= srv->cfg.chunk_slices, ARMA_EINVAL,
 		             "a chunk must be at least as long as the AR history (order t - 1)");
 		ARMA_REQUIRE(spec->var_wn >= 0.0 && std::isfinite(spec->var_wn), ARMA_EINVAL,

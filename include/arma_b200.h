@@ -142,7 +142,9 @@ int arma_white_noise(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed,
  * (ar_generate_surface, src/generator/ar_model_surf.cc:5-36; backend seam
  * AR_model::generate_surface, src/generator/ar_model.hh:102-103).
  * ARMA_FP64 follows the reference's summation order exactly;
- * ARMA_FP32C runs the compensated FP32 tile wavefront. */
+ * ARMA_FP32C runs the compensated FP32 tile wavefront, for orders with
+ * px <= 17, py <= 13 and pt * px <= 221 (others: ARMA_ENOTSUP).  Either
+ * form takes orders of at most 16 per axis. */
 int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3],
                    const int shape[3], int precision, void* d_zeta);
 
@@ -154,7 +156,8 @@ int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3],
  * legacy default stream) on the current device, and all scratch lives in one
  * 64 KiB __device__ array that every GPU loading the library holds until exit.
  * Limits: <= 2048 coefficients and <= 8192 tiles of 16x32 points per slice;
- * larger requests fail with ARMA_EINVAL.  The first call on a device sets up
+ * larger requests fail with ARMA_EINVAL; orders outside the FP32 kernel's
+ * (see arma_ar_filter) with ARMA_ENOTSUP.  The first call on a device sets up
  * the array's address and the kernel's shared-memory limit, so make it before
  * any stream capture.  Calls share the array: calls that overlap on the GPU
  * race and must be serialised by the caller.  Synchronises `stream`. */

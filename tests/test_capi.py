@@ -106,3 +106,13 @@ def test_mt_file_missing():
     with pytest.raises(capi.ArmaError) as e:
         A.mt_file_count("/nonexistent/mt.dat")
     assert e.value.code == -5 and "not found" in str(e.value)
+
+
+@pytest.mark.parametrize("order", [(16, 16, 4), (14, 16, 2), (2, 18, 3), (3, 3, 14)])
+def test_fp32_filter_rejects_unsupported_order_before_device_work(order):
+    """The FP32 tile kernel holds at most 13 x 17 (k, i) tap rows, 17 rows of
+    taps per slice and 13 taps per row; other orders answer ARMA_ENOTSUP
+    from the argument checks (the buffer pointer is never touched)."""
+    with pytest.raises(capi.ArmaError) as e:
+        capi.ar_filter_fp32c_noalloc(0, np.zeros(order), (4, 16, 32), 256)
+    assert e.value.code == -8 and "not supported" in str(e.value)
