@@ -862,7 +862,8 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 		members[best].push_back(k);
 		assigned[best] += work[k];
 	}
-	// the filter's coefficient tables of every surface (host work, one upload)
+	// the filter's coefficient tables of every surface (host work, one
+	// upload), built while the device generates the first group's noise
 	std::vector<const double*> phis(n);
 	std::vector<const int*> ords(n), shps(n);
 	std::vector<float*> zs(n);
@@ -872,8 +873,7 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 		shps[k] = s[k].shape;
 		zs[k] = static_cast<float*>(dz[k]);
 	}
-	const std::vector<Ar32Surface> as =
-	    ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
+	std::vector<Ar32Surface> as;
 	// Each group's noise is enqueued without reading its accepted-pair counts
 	// back (a device->host read on the context's stream would queue behind the
 	// previous groups' copies); the counts are checked at the end.
@@ -898,6 +898,7 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 		for (int g = 0; g < G; ++g) {
 			if (members[g].empty()) continue;
 			noise(g);
+			if (as.empty()) as = ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
 			std::vector<Ar32Surface> ga;
 			std::vector<RenormSpec> rs;
 			for (int k : members[g]) {
