@@ -250,3 +250,44 @@ def test_wave_group_bad_function():
 
 def test_high_amplitude_solver_is_built():
     A.Driver(config(solver_name="high_amplitude"))
+
+
+def test_mutated_configs_parse_or_fail_cleanly():
+    """Robustness of the `.arma` parser: 2000 random edits (deleted,
+    inserted or replaced grammar tokens and extreme numbers) of valid AR, NIT,
+    wave-group MA and high-amplitude configurations either parse or raise
+    ArmaError with a message; none crashes the process."""
+    import random
+    seeds = [
+        config(),
+        config("\torder = (4,4,4)\n\tseed = 3\n\tprecision = fp32c\n\toutput = acf,surface,blitz\n"),
+        config("\ttransform = nit {\n\t\tdistribution = gram_charlier {\n\t\t\tskewness = 2.25\n"
+               "\t\t\tkurtosis = 0.4\n\t\t}\n\t\tcdf_solver = {\n\t\t\tinterval = [-5,5]\n"
+               "\t\t\tabsolute_error = 1e-4\n\t\t\tmax_iterations = 50\n\t\t}\n\t}\n"),
+        config(acf="func = cos\n\t\tamplitude = 2\n\t\talpha = (1,0,0)\n\t\tvelocity = 0.01\n"
+                   "\t\tbeta = (0.1,0)\n\t\tnwaves = (12.5,12.5,12.5)\n\t\tshape = (32,1,1)",
+               model="MA"),
+        config(solver_name="high_amplitude"),
+    ]
+    tokens = ["{", "}", "(", ")", "[", "]", ",", ":", "=", "\n", "#", " ", "-", "1e309", "nan",
+              "inf", "0", "-1", "99999999999", "from", "to", "npoints", "nit", "AR", "MA",
+              "grid", "order", "(0,0,0)", "(1,1)", "((", "\t"]
+    rng = random.Random(2024)
+    parsed = 0
+    for _ in range(2000):
+        s = list(rng.choice(seeds))
+        for _ in range(rng.randint(1, 6)):
+            op, pos = rng.random(), rng.randrange(len(s) + 1)
+            if op < 0.3 and s:
+                del s[min(pos, len(s) - 1)]
+            elif op < 0.6:
+                s.insert(pos, rng.choice(tokens))
+            elif s:
+                s[rng.randrange(len(s))] = rng.choice(tokens)
+        try:
+            with A.Driver("".join(s)) as d:
+                d.info()
+            parsed += 1
+        except A.ArmaError as e:
+            assert str(e)
+    assert 0 < parsed < 2000
