@@ -40,10 +40,16 @@ size_t elem_size(int precision) {
 }  // namespace
 
 // Host-side copy of sgenrand-independent validation of a parameter set.
+// A parameter set is used only if its recurrence and tempering are well
+// formed: besides sizing the generator, the tempering shifts must lie in
+// [1, 31] (the device inverts the tempering by fixed-point iteration, which
+// advances by the shift).
 void require_mt(const arma_mt_params* p) {
 	ARMA_REQUIRE(p, ARMA_EINVAL, "null MT parameter set");
+	auto shift_ok = [](int s) { return s >= 1 && s <= 31; };
 	ARMA_REQUIRE(p->ww == 32 && p->nn > 1 && p->mm > 0 && p->mm < p->nn && p->rr >= 0 &&
-	                 p->rr < 32,
+	                 p->rr < 32 && shift_ok(p->shift0) && shift_ok(p->shift1) &&
+	                 shift_ok(p->shiftB) && shift_ok(p->shiftC),
 	             ARMA_EINVAL, "bad MT parameter set");
 }
 

@@ -116,3 +116,16 @@ def test_fp32_filter_rejects_unsupported_order_before_device_work(order):
     with pytest.raises(capi.ArmaError) as e:
         capi.ar_filter_fp32c_noalloc(0, np.zeros(order), (4, 16, 32), 256)
     assert e.value.code == -8 and "not supported" in str(e.value)
+
+
+@pytest.mark.parametrize("field,value", [("shift0", 0), ("shift1", 0), ("shiftB", -3),
+                                         ("shiftC", 32), ("rr", 32), ("mm", 0)])
+def test_malformed_mt_parameter_set_rejected(tmp_path, field, value):
+    """Tempering shifts outside [1, 31] (the device inverts the tempering by
+    a fixed-point iteration that advances by the shift) and malformed
+    recurrences are rejected wherever a parameter set is used."""
+    p = A.mt19937_params()
+    setattr(p, field, value)
+    with pytest.raises(capi.ArmaError) as e:
+        A.mt_file_write(str(tmp_path / "mt.dat"), [p])
+    assert e.value.code == -1 and "bad MT parameter set" in str(e.value)
