@@ -12,6 +12,7 @@
 //              cubic Lagrange interpolation between nodes and linear
 //              extrapolation beyond the end nodes.  HBM-bound: one read and
 //              one write per value.
+#include <algorithm>
 #include <cmath>
 
 #include "distributions.h"
@@ -98,15 +99,23 @@ void launch_nit_bisection(Ctx* c, int d, const double params[3], double stdev, d
                           void* d_zeta) {
 	ProfScope prof_(c, "nit");
 	upload_gl20(c);
+	// An iteration either moves one end of the bracket to a midpoint strictly
+	// inside it, or leaves the bracket, and so every later iteration, as it
+	// is.  A bracket of finite doubles can be halved at most ~2100 times
+	// (2^1024 down to the subnormal spacing 2^-1074) before its midpoint
+	// rounds to an end, so iterations past 4096 never change the result:
+	// larger counts are cut there, which bounds the kernel's run time without
+	// changing any output.
+	const int iters = std::min(max_iter, 4096);
 	const int grid = grid_for(n, c->num_sms);
 	if (precision == ARMA_FP64)
 		nit_bisection_kernel<double><<<grid, kThreads, 0, c->stream>>>(
 		    static_cast<double*>(d_zeta), n, d, params[0], params[1], params[2], stdev, a, b,
-		    eps, max_iter);
+		    eps, iters);
 	else
 		nit_bisection_kernel<float><<<grid, kThreads, 0, c->stream>>>(
 		    static_cast<float*>(d_zeta), n, d, params[0], params[1], params[2], stdev, a, b,
-		    eps, max_iter);
+		    eps, iters);
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 }

@@ -191,3 +191,19 @@ def test_zeta_bin_is_big_endian(tmp_path):
     p = str(tmp_path / "zeta.bin")
     assert O.write_zeta_bin(p, z) == 0
     assert np.array_equal(np.fromfile(p, dtype=">f8").reshape(2, 3, 4), z)
+
+
+@pytest.mark.parametrize("kind,params", [("gram_charlier", [0.3, 3.2]),
+                                         ("skew_normal", [0.0, 1.0, 1.5])])
+@pytest.mark.parametrize("interval", [(-10.0, 10.0), (-1e300, 1e300), (0.0, 1.0)])
+def test_nit_bisection_settles_within_2200_iterations(kind, params, interval):
+    """The reference's bisection (src/linalg.hh:199-213) with a tolerance it
+    can never meet reaches a fixed bracket within ~2100 halvings of a finite
+    interval, so any iteration count above that gives the same values; the
+    device launcher relies on this when it cuts max_iter at 4096."""
+    rng = np.random.default_rng(0)
+    z = rng.normal(0.0, 1.2, 400)
+    z[:4] = [0.0, 40.0, -40.0, 1e-300]
+    outs = [O.nit_transform(z, 1.2, kind, params, interval=interval, eps=1e-300, max_iter=m)
+            for m in (2200, 4096, 12000)]
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
