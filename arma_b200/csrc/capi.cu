@@ -595,6 +595,8 @@ std::vector<Ar32Surface> ar32_surfaces(Ctx* c, int n, const double* const* phis,
 	std::vector<size_t> off(n + 1, 0);
 	for (int k = 0; k < n; ++k) off[k + 1] = off[k] + ar32_coefficient_count(orders[k]);
 	std::vector<float> buf(off[n]);
+	// independent per surface (FP64 H and the lo-row selection): one thread each
+#pragma omp parallel for schedule(dynamic, 4) if (n >= 8)
 	for (int k = 0; k < n; ++k) ar32_coefficients(phis[k], orders[k], buf.data() + off[k]);
 	float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
 	ARMA_CUDA_TRY(cudaMemcpyAsync(d, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice,
