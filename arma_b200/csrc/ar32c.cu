@@ -38,6 +38,7 @@
 // counter in dependency order, so a CTA only ever waits on tiles that are
 // already owned by running CTAs.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "internal.h"
@@ -623,10 +624,18 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 //
 //   * Limits: at most kStaticMaxTiles (8192) tiles of 16 x 32 points per time
 //     slice and at most kStaticMaxTaps (2048) AR coefficients; larger
-//     requests are rejected with ARMA_EINVAL.
+//     requests are rejected with ARMA_EINVAL.  Orders follow the FP32 filter's
+//     own limits (at most 16 per axis, px <= 17, py <= 13, pt * px <= 221)
+//     and answer ARMA_ENOTSUP beyond them, as arma_ar_filter does.
+//   * The coefficient tables are the ones the context path builds
+//     (ar32_coefficients), so the result is bit-identical to
+//     arma_ar_filter(..., ARMA_FP32C, ...) on the same input.
 //   * The first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress and raises the kernel's shared-memory limit; make
-//     that first call before any stream capture.
+//     cudaGetSymbolAddress (once per device, under a lock).
+//   * Every call reads the device error word back and synchronises the
+//     stream before it returns, and stages its tables from host stack
+//     memory, so it cannot run under stream capture: a capturing stream is
+//     refused with ARMA_EINVAL.
 //   * Every call reuses the same array and leaves the last call's contents in
 //     it; each call clears the counters it relies on.  Calls whose work
 //     overlaps on the GPU (other streams or threads) race on the array and
@@ -638,22 +647,34 @@ namespace {
 constexpr size_t kStaticScratchBytes = 64 * 1024;
 constexpr int kStaticMaxTiles = 8192;
 constexpr int kStaticMaxTaps = 2048;
-// byte offsets inside the array
+// byte offsets inside the array; the coefficient block is hi[P], lo[P], H[TX*TY]
 constexpr size_t kOffTask = 0;
 constexpr size_t kOffTicket = 256;
 constexpr size_t kOffErr = 260;
 constexpr size_t kOffFlags = 512;
-constexpr size_t kOffPhi = kOffFlags + sizeof(int) * kStaticMaxTiles;
-constexpr size_t kOffH = kOffPhi + 2 * sizeof(float) * kStaticMaxTaps;
-constexpr size_t kStaticEnd = kOffH + sizeof(float) * TX * TY;
+constexpr size_t kOffCoef = kOffFlags + sizeof(int) * kStaticMaxTiles;
+constexpr size_t kMaxCoefFloats = 2 * size_t(kStaticMaxTaps) + size_t(TX) * TY;
+constexpr size_t kStaticEnd = kOffCoef + sizeof(float) * kMaxCoefFloats;
 static_assert(kStaticEnd <= kStaticScratchBytes, "static scratch layout overflows");
 static_assert(sizeof(Task) <= kOffTicket, "task record overflows its slot");
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 constexpr int kMaxDevices = 64;
+std::mutex g_static_lock;
 unsigned char* g_static_addr[kMaxDevices] = {nullptr};
-bool g_static_ready[kMaxDevices] = {false};
+
+// The array's device address on the current device (looked up once per
+// device); nullptr when the lookup fails.
+unsigned char* static_scratch(int dev) {
+	std::lock_guard<std::mutex> lk(g_static_lock);
+	if (!g_static_addr[dev]) {
+		void* p = nullptr;
+		if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess) return nullptr;
+		g_static_addr[dev] = static_cast<unsigned char*>(p);
+	}
+	return g_static_addr[dev];
+}
 
 }  // namespace
 }  // namespace armab
@@ -661,15 +682,21 @@ bool g_static_ready[kMaxDevices] = {false};
 extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, const int order[3],
                                             const int shape[3], float* d_zeta) {
 	using namespace armab;
+	// A failed runtime call leaves the runtime's last-error state set; clear it
+	// so that neither this call's launch check nor a later one reads it.
 	auto fail = [](int code, const char* msg) {
+		(void)cudaGetLastError();
 		set_error(msg);
 		return code;
 	};
+	(void)cudaGetLastError();
 	if (!phi || !order || !shape || !d_zeta) return fail(ARMA_EINVAL, "null argument");
 	if (shape[0] <= 0 || shape[1] <= 0 || shape[2] <= 0)
 		return fail(ARMA_EINVAL, "Bad \"out_grid\": dimensions must be positive");
-	if (order[0] < 1 || order[1] < 1 || order[2] < 1 || order[1] > TX + 1 || order[2] > MAXO ||
-	    order[0] * order[1] > kMaxTapRows)
+	if (order[0] < 1 || order[1] < 1 || order[2] < 1 || order[0] > 16 || order[1] > 16 ||
+	    order[2] > 16)
+		return fail(ARMA_ENOTSUP, "AR order above 16 per dimension is not supported on the device");
+	if (order[1] > TX + 1 || order[2] > MAXO || order[0] * order[1] > kMaxTapRows)
 		return fail(ARMA_ENOTSUP, "AR order not supported by the FP32 tile kernel");
 	const int P = order[0] * order[1] * order[2];
 	if (P > kStaticMaxTaps)
@@ -679,33 +706,33 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 		return fail(ARMA_EINVAL,
 		            "allocation-free AR filter: slice needs more than 8192 tiles of 16x32 points");
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+	if (cudaStreamIsCapturing(st, &cap) != cudaSuccess)
+		return fail(ARMA_ECUDA, "cudaStreamIsCapturing failed");
+	if (cap != cudaStreamCaptureStatusNone)
+		return fail(ARMA_EINVAL,
+		            "allocation-free AR filter: the stream is capturing (the call synchronises)");
 	int dev = 0;
 	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
 		return fail(ARMA_ECUDA, "cudaGetDevice failed");
 	const size_t smem = smem_bytes(order[0], order[1], order[2]);
-	if (!g_static_ready[dev]) {
-		void* p = nullptr;
-		if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess)
-			return fail(ARMA_ECUDA, "cudaGetSymbolAddress of the static scratch failed");
-		g_static_addr[dev] = static_cast<unsigned char*>(p);
-		g_static_ready[dev] = true;
-	}
+	int smem_optin = 0;
+	if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+	    cudaSuccess)
+		return fail(ARMA_ECUDA, "shared-memory limit query failed");
+	if (smem > size_t(smem_optin))
+		return fail(ARMA_ENOTSUP, "AR order needs more shared memory than the device has");
+	unsigned char* base = static_scratch(dev);
+	if (!base) return fail(ARMA_ECUDA, "cudaGetSymbolAddress of the static scratch failed");
 	if (cudaFuncSetAttribute(ar32c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                         int(smem)) != cudaSuccess)
 		return fail(ARMA_ECUDA, "cudaFuncSetAttribute failed");
-	unsigned char* base = g_static_addr[dev];
-	float* d_phi = reinterpret_cast<float*>(base + kOffPhi);
-	float* d_h = reinterpret_cast<float*>(base + kOffH);
-	// host-side tables on the stack
-	double h[TX * TY];
-	intra_slice_response(phi, order, TX, TY, h);
-	float hbuf[TX * TY];
-	for (int i = 0; i < TX * TY; ++i) hbuf[i] = float(h[i]);
-	float pbuf[2 * kStaticMaxTaps];
-	for (int i = 0; i < P; ++i) {
-		pbuf[i] = float(phi[i]);
-		pbuf[P + i] = float(phi[i] - double(pbuf[i]));
-	}
+	float* d_coef = reinterpret_cast<float*>(base + kOffCoef);
+	// the context path's tables (hi/lo split, lo-row selection, H), built into
+	// host stack memory: 2P + TX*TY <= kMaxCoefFloats floats
+	float cbuf[kMaxCoefFloats];
+	const size_t ncoef = ar32_coefficient_count(order);
+	ar32_coefficients(phi, order, cbuf);
 	Task t;
 	t.nt = shape[0]; t.nx = shape[1]; t.ny = shape[2];
 	t.pt = order[0]; t.px = order[1]; t.py = order[2];
@@ -713,9 +740,9 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 	t.tiles_x = tiles_x; t.tiles_y = tiles_y;
 	t.ticket_base = 0;
 	t.zeta = d_zeta;
-	t.phi = d_phi;
-	t.phi_lo = d_phi + P;
-	t.h = d_h;
+	t.phi = d_coef;
+	t.phi_lo = d_coef + P;
+	t.h = d_coef + 2 * P;
 	t.flags = reinterpret_cast<int*>(base + kOffFlags);
 	int* d_ticket = reinterpret_cast<int*>(base + kOffTicket);
 	int* d_err = reinterpret_cast<int*>(base + kOffErr);
@@ -725,22 +752,26 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 	        cudaSuccess ||
 	    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
 		return fail(ARMA_ECUDA, "occupancy query failed");
-	if (per_sm <= 0) return fail(ARMA_EINVAL, "AR tile does not fit in shared memory");
+	if (per_sm <= 0) return fail(ARMA_ENOTSUP, "AR tile does not fit in shared memory");
 	const int grid = std::min(ntiles, per_sm * sms);
 	if (cudaMemcpyAsync(base + kOffTask, &t, sizeof(t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-	    cudaMemcpyAsync(d_phi, pbuf, sizeof(float) * 2 * P, cudaMemcpyHostToDevice, st) !=
+	    cudaMemcpyAsync(d_coef, cbuf, sizeof(float) * ncoef, cudaMemcpyHostToDevice, st) !=
 	        cudaSuccess ||
-	    cudaMemcpyAsync(d_h, hbuf, sizeof(hbuf), cudaMemcpyHostToDevice, st) != cudaSuccess ||
 	    cudaMemsetAsync(base + kOffTicket, 0, 8, st) != cudaSuccess ||
-	    cudaMemsetAsync(t.flags, 0, sizeof(int) * ntiles, st) != cudaSuccess)
+	    cudaMemsetAsync(t.flags, 0, sizeof(int) * ntiles, st) != cudaSuccess) {
+		(void)cudaStreamSynchronize(st);  // the staged host buffers are on this stack
 		return fail(ARMA_ECUDA, "staging the allocation-free AR filter failed");
+	}
 	ar32c_kernel<<<grid, NTHREADS, smem, st>>>(reinterpret_cast<const Task*>(base + kOffTask), 1,
 	                                           ntiles, d_ticket, d_err);
-	if (cudaGetLastError() != cudaSuccess) return fail(ARMA_ECUDA, "AR kernel launch failed");
+	const bool launched = cudaGetLastError() == cudaSuccess;
 	int herr = 0;
-	if (cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-	    cudaStreamSynchronize(st) != cudaSuccess)
-		return fail(ARMA_ECUDA, "AR kernel failed");
+	const bool copied =
+	    cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess;
+	// wait in every case: the stream still reads this stack's buffers
+	const bool synced = cudaStreamSynchronize(st) == cudaSuccess;
+	if (!launched) return fail(ARMA_ECUDA, "AR kernel launch failed");
+	if (!copied || !synced) return fail(ARMA_ECUDA, "AR kernel failed");
 	if (herr == DEV_TIMEOUT)
 		return fail(ARMA_ETIMEDOUT, "a bounded device wait gave up (tile dependency not met)");
 	if (herr != DEV_OK) return fail(ARMA_ECUDA, "device-side check failed");

@@ -38,14 +38,15 @@ constexpr double kTwoPi = 6.283185307179586476925286766559;
 }
 
 // ------------------------------------------------------------- lexing helpers
+// Skips blank space and '#' comments (a '#' comments out the rest of its
+// line) up to the next token, which stays unread.
 std::istream& skip_comments(std::istream& in) {
-	char ch = 0;
-	while (in >> std::ws >> ch && ch == '#') {
-		in.ignore(std::numeric_limits<std::streamsize>::max(), '\n');
-		ch = 0;
+	for (;;) {
+		in >> std::ws;
+		if (in.peek() != '#') return in;
+		std::string rest;
+		std::getline(in, rest);
 	}
-	if (ch != 0) in.putback(ch);
-	return in;
 }
 
 bool expect(std::istream& in, char c) {

@@ -19,8 +19,7 @@
  *
  * The reference has no C ABI; its operator API is the C++ generator/solver
  * registry (src/arma_driver.hh:124-134) with the virtual interfaces cited on
- * each entry point below.  The cgo/ctypes-style binding a maintainer would add
- * is shown in INTEGRATION.md.
+ * each entry point below.
  */
 #ifndef ARMA_B200_H
 #define ARMA_B200_H
@@ -157,10 +156,14 @@ int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3],
  * 64 KiB __device__ array that every GPU loading the library holds until exit.
  * Limits: <= 2048 coefficients and <= 8192 tiles of 16x32 points per slice;
  * larger requests fail with ARMA_EINVAL; orders outside the FP32 kernel's
- * (see arma_ar_filter) with ARMA_ENOTSUP.  The first call on a device sets up
- * the array's address and the kernel's shared-memory limit, so make it before
- * any stream capture.  Calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller.  Synchronises `stream`. */
+ * (see arma_ar_filter) with ARMA_ENOTSUP.  Its result is bit-identical to
+ * arma_ar_filter(..., ARMA_FP32C, ...) on the same input (same coefficient
+ * tables, same kernel).  The first call on a device looks up the array's
+ * address (once per device, thread-safe).  Every call stages its tables from
+ * host memory, reads the device error word back and synchronises `stream`,
+ * so it cannot be used under stream capture: a capturing stream is refused
+ * with ARMA_EINVAL.  Calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, const int order[3],
                                  const int shape[3], float* d_zeta);
 

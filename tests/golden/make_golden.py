@@ -110,7 +110,9 @@ def oracle_cases() -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="checkout of the reference (read-only); its src/test/*-test.cc "
+                         "give the known answers")
     args = ap.parse_args()
     ka = os.path.join(HERE, "reference_known_answers.json")
     if os.path.isdir(args.reference):

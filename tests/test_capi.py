@@ -108,11 +108,14 @@ def test_mt_file_missing():
     assert e.value.code == -5 and "not found" in str(e.value)
 
 
-@pytest.mark.parametrize("order", [(16, 16, 4), (14, 16, 2), (2, 18, 3), (3, 3, 14)])
+@pytest.mark.parametrize("order", [(16, 16, 4), (14, 16, 2), (2, 18, 3), (3, 3, 14), (17, 1, 1),
+                                   (100, 1, 1)])
 def test_fp32_filter_rejects_unsupported_order_before_device_work(order):
     """The FP32 tile kernel holds at most 13 x 17 (k, i) tap rows, 17 rows of
-    taps per slice and 13 taps per row; other orders answer ARMA_ENOTSUP
-    from the argument checks (the buffer pointer is never touched)."""
+    taps per slice and 13 taps per row, and the device filters take at most 16
+    per axis (a long time order such as 100 x 1 x 1 would also need more
+    shared memory than a block has); other orders answer ARMA_ENOTSUP from the
+    argument checks (the buffer pointer is never touched)."""
     with pytest.raises(capi.ArmaError) as e:
         capi.ar_filter_fp32c_noalloc(0, np.zeros(order), (4, 16, 32), 256)
     assert e.value.code == -8 and "not supported" in str(e.value)
