@@ -10,6 +10,7 @@ from .capi import (  # noqa: F401
     ArmaError, Context, Driver, MtParams, Server, server_config, Surface, lib, library_path,
     FP64, FP32C, ACF_STANDING, ACF_PROPAGATING,
     NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL, NIT_BISECTION, NIT_LUT,
-    acf_eval, ar_fit, ar_fit_analytic, ar_fit_choi, ma_fit, mt19937_params, mt_file_count,
-    mt_file_read, mt_file_write, poly_roots, validate_process,
+    acf_eval, ar_fit, ar_fit_analytic, ar_fit_choi, ma_fit, mt19937_params, mt_create,
+    mt_equidistribution, mt_file_count, mt_file_read, mt_file_write, mt_is_primitive, poly_roots,
+    validate_process,
 )

@@ -31,6 +31,7 @@ ERRORS = {
 EXPORTS = (
     "arma_version", "arma_last_error", "arma_ctx_create", "arma_ctx_destroy",
     "arma_ctx_set_stream", "arma_ctx_synchronize", "arma_ctx_launch_count",
+    "arma_ctx_transfer_bytes",
     "arma_ctx_set_profiling", "arma_ctx_profile", "arma_ctx_profile_reset",
     "arma_mt_file_count", "arma_mt_file_read", "arma_mt_file_write",
     "arma_mt19937_params", "arma_mt_genrand", "arma_acf_eval", "arma_ar_fit",
@@ -45,6 +46,7 @@ EXPORTS = (
     "arma_server_profile", "arma_velocity_linear_batch", "arma_validate_process",
     "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf", "arma_velocity_high_amplitude",
     "arma_ma_fit", "arma_ma_filter", "arma_ma_generate", "arma_ctx_set_noise_margin",
+    "arma_mt_create", "arma_mt_is_primitive", "arma_mt_equidistribution",
 )
 
 
@@ -155,6 +157,7 @@ def lib():
             "arma_ctx_set_stream": (i, [vp, vp]),
             "arma_ctx_synchronize": (i, [vp]),
             "arma_ctx_launch_count": (i, [vp, C.POINTER(C.c_uint64)]),
+            "arma_ctx_transfer_bytes": (i, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
             "arma_ctx_set_profiling": (i, [vp, i]),
             "arma_ctx_profile": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_uint64)]),
             "arma_ctx_profile_reset": (i, [vp]),
@@ -162,6 +165,9 @@ def lib():
             "arma_mt_file_read": (i, [C.c_char_p, i, mp]),
             "arma_mt_file_write": (i, [C.c_char_p, mp, i]),
             "arma_mt19937_params": (i, [mp]),
+            "arma_mt_create": (i, [i, i, i, C.c_uint32, mp]),
+            "arma_mt_is_primitive": (i, [mp, ip]),
+            "arma_mt_equidistribution": (i, [mp, i, ip]),
             "arma_mt_genrand": (i, [vp, mp, C.c_uint32, C.c_uint64, sz, vp]),
             "arma_acf_eval": (i, [i, d, d, dp, dp, dp, ip, dp]),
             "arma_ar_fit": (i, [dp, ip, ip, i, dp, dp]),
@@ -317,6 +323,27 @@ def mt19937_params() -> MtParams:
     return p
 
 
+def mt_create(p: int, id: int, seed: int, w: int = 32) -> MtParams:
+    """dcmt parameter set of generator `id` with period 2^p - 1
+    (``arma_mt_create``)."""
+    out = MtParams()
+    _check(lib().arma_mt_create(w, p, id, C.c_uint32(seed & 0xffffffff), C.byref(out)))
+    return out
+
+
+def mt_is_primitive(params: MtParams) -> bool:
+    r = C.c_int()
+    _check(lib().arma_mt_is_primitive(C.byref(params), C.byref(r)))
+    return bool(r.value)
+
+
+def mt_equidistribution(params: MtParams, vmax: int = 32):
+    """[k(1), ..., k(vmax)] of the tempered output (``arma_mt_equidistribution``)."""
+    k = (C.c_int * vmax)()
+    _check(lib().arma_mt_equidistribution(C.byref(params), vmax, k))
+    return list(k)
+
+
 def mt_file_count(path: str) -> int:
     n = C.c_int()
     _check(lib().arma_mt_file_count(path.encode(), C.byref(n)))
@@ -374,6 +401,12 @@ class Context:
         n = C.c_uint64()
         _check(lib().arma_ctx_launch_count(self._h, C.byref(n)))
         return n.value
+
+    def transfer_bytes(self):
+        """(host->device, device->host) bytes copied by this context's calls."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().arma_ctx_transfer_bytes(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def set_profiling(self, on: bool = True):
         _check(lib().arma_ctx_set_profiling(self._h, 1 if on else 0))

@@ -588,7 +588,7 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 	}
 	Task* d_tasks = static_cast<Task*>(scratch_take(c, sizeof(Task) * tasks.size()));
 	int* d_ticket = static_cast<int*>(scratch_take(c, sizeof(int)));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_tasks, tasks.data(), sizeof(Task) * tasks.size(),
+	ARMA_CUDA_TRY(copy_async(c, d_tasks, tasks.data(), sizeof(Task) * tasks.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
 	ARMA_CUDA_TRY(cudaMemsetAsync(d_ticket, 0, sizeof(int), c->stream));
 	ARMA_CUDA_TRY(cudaFuncSetAttribute(ar32c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -114,7 +114,7 @@ void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
                        const std::vector<void*>& dz) {
 	long long* d_pairs = white_noise_batch_enqueue(c, s, n, precision, dz);
 	std::vector<long long> pairs(n);
-	ARMA_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(long long) * n,
+	ARMA_CUDA_TRY(copy_async(c, pairs.data(), d_pairs, sizeof(long long) * n,
 	                              cudaMemcpyDeviceToHost, c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	for (int k = 0; k < n; ++k) {
@@ -248,7 +248,7 @@ void resolve_profile(Ctx* c) {
 
 void check_device_error(Ctx* c) {
 	int h = 0;
-	ARMA_CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	ARMA_CUDA_TRY(copy_async(c, &h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	if (h == DEV_TIMEOUT) {
 		ARMA_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
@@ -341,6 +341,14 @@ int arma_ctx_launch_count(arma_ctx* ctx, uint64_t* count) {
 	});
 }
 
+int arma_ctx_transfer_bytes(arma_ctx* ctx, uint64_t* h2d, uint64_t* d2h) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && h2d && d2h, ARMA_EINVAL, "null argument");
+		*h2d = ctx->c.h2d_bytes;
+		*d2h = ctx->c.d2h_bytes;
+	});
+}
+
 int arma_ctx_set_profiling(arma_ctx* ctx, int enabled) {
 	return guard([&] {
 		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
@@ -399,6 +407,37 @@ int arma_mt19937_params(arma_mt_params* p) {
 		p->maskB = 0x9d2c5680u;
 		p->maskC = 0xefc60000u;
 		p->i = 624;
+	});
+}
+
+int arma_mt_create(int w, int p, int id, uint32_t seed, arma_mt_params* out) {
+	return guard([&] {
+		ARMA_REQUIRE(out, ARMA_EINVAL, "null output pointer");
+		ARMA_REQUIRE(w == 32, ARMA_EINVAL, "only w = 32 parameter sets are supported");
+		ARMA_REQUIRE(dcmt::mersenne_exponent(p), ARMA_EINVAL,
+		             "p must be a Mersenne exponent between 521 and 44497");
+		ARMA_REQUIRE(id >= 0 && id < 65536, ARMA_EINVAL, "id must be in [0, 65536)");
+		arma_mt_params r;
+		if (dcmt::create(p, id, seed, &r) != 0)
+			throw Error{ARMA_ENUMERIC, "bad MT: no primitive characteristic polynomial for id " +
+			                               std::to_string(id)};
+		*out = r;
+	});
+}
+
+int arma_mt_is_primitive(const arma_mt_params* p, int* primitive) {
+	return guard([&] {
+		ARMA_REQUIRE(primitive, ARMA_EINVAL, "null output pointer");
+		require_mt(p);
+		*primitive = dcmt::mersenne_exponent(32 * p->nn - p->rr) && dcmt::is_primitive(*p) ? 1 : 0;
+	});
+}
+
+int arma_mt_equidistribution(const arma_mt_params* p, int vmax, int* k_out) {
+	return guard([&] {
+		ARMA_REQUIRE(k_out && vmax >= 1 && vmax <= 32, ARMA_EINVAL, "bad argument");
+		require_mt(p);
+		for (int v = 1; v <= vmax; ++v) k_out[v - 1] = int(dcmt::equidistribution(*p, v));
 	});
 }
 
@@ -599,7 +638,7 @@ std::vector<Ar32Surface> ar32_surfaces(Ctx* c, int n, const double* const* phis,
 #pragma omp parallel for schedule(dynamic, 4) if (n >= 8)
 	for (int k = 0; k < n; ++k) ar32_coefficients(phis[k], orders[k], buf.data() + off[k]);
 	float* d = static_cast<float*>(scratch_take(c, sizeof(float) * buf.size()));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice,
+	ARMA_CUDA_TRY(copy_async(c, d, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice,
 	                              c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));  // buf is pageable and local
 	std::vector<Ar32Surface> out(n);
@@ -628,7 +667,7 @@ void ar_filter(Ctx* c, const double* phi, const int order[3], const int shape[3]
 	const int P = order[0] * order[1] * order[2];
 	if (precision == ARMA_FP64) {
 		double* d_phi = static_cast<double*>(scratch_take(c, sizeof(double) * P));
-		ARMA_CUDA_TRY(cudaMemcpyAsync(d_phi, phi, sizeof(double) * P, cudaMemcpyHostToDevice,
+		ARMA_CUDA_TRY(copy_async(c, d_phi, phi, sizeof(double) * P, cudaMemcpyHostToDevice,
 		                              c->stream));
 		launch_ar64(c, d_phi, order, shape, static_cast<double*>(d_zeta));
 	} else {
@@ -672,7 +711,7 @@ int arma_variance_renorm(arma_ctx* ctx, void* d_zeta, const int shape[3], int pr
 		double* d_scale = static_cast<double*>(scratch_take(&ctx->c, sizeof(double)));
 		launch_renorm(&ctx->c, d_zeta, shape, precision, acf0, d_scale);
 		double s = 0.0;
-		ARMA_CUDA_TRY(cudaMemcpyAsync(&s, d_scale, sizeof(double), cudaMemcpyDeviceToHost,
+		ARMA_CUDA_TRY(copy_async(&ctx->c, &s, d_scale, sizeof(double), cudaMemcpyDeviceToHost,
 		                              ctx->c.stream));
 		ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
 		if (scale_out) *scale_out = s;
@@ -702,9 +741,9 @@ int arma_nit_apply(arma_ctx* ctx, int d, const double params[3], double stdev, i
 			std::vector<float> yf(y.begin(), y.end());
 			double* d_lut = static_cast<double*>(
 			    scratch_take(&ctx->c, sizeof(double) * lut_nodes + sizeof(float) * lut_nodes));
-			ARMA_CUDA_TRY(cudaMemcpyAsync(d_lut, y.data(), sizeof(double) * lut_nodes,
+			ARMA_CUDA_TRY(copy_async(&ctx->c, d_lut, y.data(), sizeof(double) * lut_nodes,
 			                              cudaMemcpyHostToDevice, ctx->c.stream));
-			ARMA_CUDA_TRY(cudaMemcpyAsync(d_lut + lut_nodes, yf.data(), sizeof(float) * lut_nodes,
+			ARMA_CUDA_TRY(copy_async(&ctx->c, d_lut + lut_nodes, yf.data(), sizeof(float) * lut_nodes,
 			                              cudaMemcpyHostToDevice, ctx->c.stream));
 			launch_nit_lut(&ctx->c, d_lut, lut_nodes, x0, dx, n, precision, d_zeta);
 			ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
@@ -828,7 +867,7 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo =
 	launch_ar32c(c, as, tx, ty, 1);
 	std::vector<long long> pairs(n, 0);
 	if (d_pairs)
-		ARMA_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs, sizeof(long long) * n,
+		ARMA_CUDA_TRY(copy_async(c, pairs.data(), d_pairs, sizeof(long long) * n,
 		                              cudaMemcpyDeviceToHost, c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	check_device_error(c);
@@ -924,12 +963,12 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 			ARMA_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, e, 0));
 			for (int k : members[g]) {
 				const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
-				ARMA_CUDA_TRY(cudaMemcpyAsync(s[k].d_zeta, dz[k], np * sizeof(float),
+				ARMA_CUDA_TRY(copy_async(c, s[k].d_zeta, dz[k], np * sizeof(float),
 				                              cudaMemcpyDeviceToHost, c->copy_stream));
 			}
 		}
 		std::vector<double> sc(n, 1.0);
-		ARMA_CUDA_TRY(cudaMemcpyAsync(sc.data(), d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost,
+		ARMA_CUDA_TRY(copy_async(c, sc.data(), d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost,
 		                              c->stream));
 		ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 		ARMA_CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
@@ -968,12 +1007,12 @@ void renorm_surfaces(Ctx* c, arma_surface* s, int n, int precision, const std::v
 	if (host) {
 		for (int k = 0; k < n; ++k) {
 			const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
-			ARMA_CUDA_TRY(cudaMemcpyAsync(s[k].d_zeta, dz[k], np * es, cudaMemcpyDeviceToHost,
+			ARMA_CUDA_TRY(copy_async(c, s[k].d_zeta, dz[k], np * es, cudaMemcpyDeviceToHost,
 			                              c->stream));
 		}
 	}
 	std::vector<double> sc(n, 1.0);
-	ARMA_CUDA_TRY(cudaMemcpyAsync(sc.data(), d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost,
+	ARMA_CUDA_TRY(copy_async(c, sc.data(), d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost,
 	                              c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	for (int k = 0; k < n; ++k) s[k].scale = s[k].acf0 > 0.0 ? sc[k] : 1.0;

@@ -53,6 +53,8 @@ struct Ctx {
 	cudaStream_t copy_stream = nullptr;  // device->host copies overlapped with compute (lazy)
 	double noise_margin = 1.0;           // polar-attempt estimate multiplier of the batched calls
 	uint64_t launches = 0;           // kernel launches issued
+	uint64_t h2d_bytes = 0;          // bytes copied host -> device through copy_async
+	uint64_t d2h_bytes = 0;          // bytes copied device -> host through copy_async
 	int num_sms = 148;
 	// cached CUDA graphs for the FP64 plane sweep, keyed by a string
 	std::map<std::string, cudaGraphExec_t> graphs;
@@ -66,6 +68,15 @@ struct Ctx {
 	std::map<std::string, double> prof_ms;
 	std::map<std::string, long long> prof_count;
 };
+
+// cudaMemcpyAsync that counts the bytes a context moves between host and
+// device (arma_ctx_transfer_bytes).
+inline cudaError_t copy_async(Ctx* c, void* dst, const void* src, size_t bytes,
+                              cudaMemcpyKind kind, cudaStream_t stream) {
+	if (kind == cudaMemcpyHostToDevice) c->h2d_bytes += bytes;
+	if (kind == cudaMemcpyDeviceToHost) c->d2h_bytes += bytes;
+	return cudaMemcpyAsync(dst, src, bytes, kind, stream);
+}
 
 // Records CUDA events around a launch when profiling is on.
 class ProfScope {
@@ -321,6 +332,14 @@ void require_mt(const arma_mt_params* p);
 // H (ar32_coefficient_count floats).
 size_t ar32_coefficient_count(const int order[3]);
 void ar32_coefficients(const double* phi, const int order[3], float* out);
+
+// dcmt parameter-set creation (dcmt.cpp).
+namespace dcmt {
+bool mersenne_exponent(int p);
+bool is_primitive(const arma_mt_params& prm);
+long equidistribution(const arma_mt_params& prm, int v);  // k(v), -1 if undetermined
+int create(int p, int id, uint32_t seed, arma_mt_params* out);  // 0, or -1: no primitive set
+}  // namespace dcmt
 
 // Runs f, mapping library exceptions to status codes and the thread's last
 // error message.

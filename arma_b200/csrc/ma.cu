@@ -230,7 +230,7 @@ void ma_filter_impl(Ctx* c, const double* theta, const int order[3], const int s
 	K[0] = T(1);
 	for (size_t q = 1; q < P; ++q) K[q] = T(-theta[q]);
 	T* dK = static_cast<T*>(scratch_take(c, P * sizeof(T)));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(dK, K.data(), P * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+	ARMA_CUDA_TRY(copy_async(c, dK, K.data(), P * sizeof(T), cudaMemcpyHostToDevice, c->stream));
 	ARMA_CUDA_TRY(cudaFuncSetAttribute(ma_fir_kernel<T>,
 	                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kMaSmemLimit));
 	const dim3 grid((shape[2] + 16 * R - 1) / (16 * R), (shape[1] + 15) / 16,

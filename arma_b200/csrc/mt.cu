@@ -74,6 +74,11 @@ __device__ __forceinline__ void seed_state(uint32_t* dst, uint32_t seed, const a
 	}
 }
 
+// W = ceil((n - m) / kThreads) words of every chunk per thread (n - m <=
+// kMaxOwn * kThreads covers every Mersenne exponent up to 44497).
+constexpr int kMaxOwn = 4;
+
+template <int W>
 __global__ void __launch_bounds__(kThreads)
 mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	__shared__ uint32_t ring[kRing];
@@ -91,31 +96,41 @@ mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	}
 	__syncthreads();
 	const uint32_t mask = kRing - 1;
-	// Thread t < n-m owns word t of every chunk: segment word w = s (n-m) + t
-	// at step s, raw word r = n + w at ring position r & mask (positions run
-	// modulo 2^32, a multiple of the ring size), so every index is a running
-	// register sum.  Each step emits the chunk computed by the step before and
-	// computes the next one: raw r + n - m reads raw r (this thread's own
-	// word) and raw r - m, r - m + 1, all written in earlier steps.
-	const int t = threadIdx.x;
-	const bool owner = t < chunk;
+	// Thread t owns words t + i kThreads (i < W, those < n - m) of every chunk:
+	// segment word w = s (n-m) + t + i kThreads at step s, raw word r = n + w
+	// at ring position r & mask (positions run modulo 2^32, a multiple of the
+	// ring size), so every index is a running register sum.  Each step emits
+	// the chunk computed by the step before and computes the next one: raw
+	// r + n - m reads raw r (this thread's own word) and raw r - m, r - m + 1,
+	// all written in earlier steps.
 	auto next_word = [&](uint32_t r) {  // raw word r from raw r - n, r - n + 1, r - n + m
 		const uint32_t y = (ring[(r - n) & mask] & p.umask) | (ring[(r - n + 1) & mask] & p.lmask);
 		return ring[(r - n + m) & mask] ^ (y >> 1) ^ ((y & 1u) ? p.aaa : 0u);
 	};
-	uint32_t r = uint32_t(n + t);  // raw position of this thread's current word
-	long long o = shift + t;       // its output index
-	long long rem = count - t;     // words from it to the segment's end
-	if (owner && rem > 0) ring[r & mask] = next_word(r);
+	uint32_t r[W];
+	long long o[W], rem[W];
+	bool owner[W];
+#pragma unroll
+	for (int i = 0; i < W; ++i) {
+		const int t = threadIdx.x + i * kThreads;
+		owner[i] = t < chunk;
+		r[i] = uint32_t(n + t);  // raw position of this word
+		o[i] = shift + t;        // its output index
+		rem[i] = count - t;      // words from it to the segment's end
+		if (owner[i] && rem[i] > 0) ring[r[i] & mask] = next_word(r[i]);
+	}
 	__syncthreads();
 	const long long steps = (count + chunk - 1) / chunk;
 	for (long long st = 0; st < steps; ++st) {
-		if (owner) {
-			if (rem > 0 && o >= 0) out[o] = temper(ring[r & mask], p);
-			if (rem > chunk) ring[(r + chunk) & mask] = next_word(r + chunk);
-			r += chunk;
-			o += chunk;
-			rem -= chunk;
+#pragma unroll
+		for (int i = 0; i < W; ++i) {
+			if (owner[i]) {
+				if (rem[i] > 0 && o[i] >= 0) out[o[i]] = temper(ring[r[i] & mask], p);
+				if (rem[i] > chunk) ring[(r[i] + chunk) & mask] = next_word(r[i] + chunk);
+				r[i] += chunk;
+				o[i] += chunk;
+				rem[i] -= chunk;
+			}
 		}
 		__syncthreads();
 	}
@@ -286,8 +301,8 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		             "an MT job started from a window has no offset");
 		ARMA_REQUIRE(j.p.nn > 1 && j.p.mm > 0 && j.p.mm < j.p.nn && j.p.ww == 32, ARMA_EINVAL,
 		             "bad MT parameter set");
-		ARMA_REQUIRE(j.p.nn + (j.p.nn - j.p.mm) <= kRing, ARMA_EINVAL,
-		             "MT state too large for the device generator");
+		ARMA_REQUIRE(j.p.nn + (j.p.nn - j.p.mm) <= kRing && j.p.nn - j.p.mm <= kMaxOwn * kThreads,
+		             ARMA_EINVAL, "MT state too large for the device generator");
 	}
 	if (jobs.empty()) return;
 	const unsigned long long J = 1ull << log2_seg;
@@ -328,13 +343,13 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		auto* d_seeds = static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * seeds.size()));
 		auto* d_src = static_cast<const uint32_t**>(scratch_take(c, sizeof(uint32_t*) * src.size()));
 		auto* d_dst = static_cast<uint32_t**>(scratch_take(c, sizeof(uint32_t*) * dst.size()));
-		ARMA_CUDA_TRY(cudaMemcpyAsync(d_ps, ps.data(), sizeof(arma_mt_params) * ps.size(),
+		ARMA_CUDA_TRY(copy_async(c, d_ps, ps.data(), sizeof(arma_mt_params) * ps.size(),
 		                              cudaMemcpyHostToDevice, c->stream));
-		ARMA_CUDA_TRY(cudaMemcpyAsync(d_seeds, seeds.data(), sizeof(uint32_t) * seeds.size(),
+		ARMA_CUDA_TRY(copy_async(c, d_seeds, seeds.data(), sizeof(uint32_t) * seeds.size(),
 		                              cudaMemcpyHostToDevice, c->stream));
-		ARMA_CUDA_TRY(cudaMemcpyAsync(d_src, src.data(), sizeof(uint32_t*) * src.size(),
+		ARMA_CUDA_TRY(copy_async(c, d_src, src.data(), sizeof(uint32_t*) * src.size(),
 		                              cudaMemcpyHostToDevice, c->stream));
-		ARMA_CUDA_TRY(cudaMemcpyAsync(d_dst, dst.data(), sizeof(uint32_t*) * dst.size(),
+		ARMA_CUDA_TRY(copy_async(c, d_dst, dst.data(), sizeof(uint32_t*) * dst.size(),
 		                              cudaMemcpyHostToDevice, c->stream));
 		mt_seed_kernel<<<int(ps.size()), 32, 0, c->stream>>>(d_ps, d_seeds, d_src, d_dst);
 		c->launches += 1;
@@ -361,7 +376,7 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 			}
 			if (jj.empty()) continue;
 			auto* d_jj = static_cast<JumpJob*>(scratch_take(c, sizeof(JumpJob) * jj.size()));
-			ARMA_CUDA_TRY(cudaMemcpyAsync(d_jj, jj.data(), sizeof(JumpJob) * jj.size(),
+			ARMA_CUDA_TRY(copy_async(c, d_jj, jj.data(), sizeof(JumpJob) * jj.size(),
 			                              cudaMemcpyHostToDevice, c->stream));
 			// few jumps at this level: split each over several CTAs
 			int parts = int(std::min<size_t>(8, std::max<size_t>(1, (2 * size_t(c->num_sms) +
@@ -392,9 +407,16 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		}
 	}
 	auto* d_seg = static_cast<SegJob*>(scratch_take(c, sizeof(SegJob) * seg.size()));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_seg, seg.data(), sizeof(SegJob) * seg.size(),
+	ARMA_CUDA_TRY(copy_async(c, d_seg, seg.data(), sizeof(SegJob) * seg.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
-	mt_generate_kernel<<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg);
+	int own = 1;  // words per thread and chunk: the largest chunk of the batch
+	for (const MtJob& j : jobs) own = std::max(own, (j.p.nn - j.p.mm + kThreads - 1) / kThreads);
+	switch (own) {
+		case 1: mt_generate_kernel<1><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
+		case 2: mt_generate_kernel<2><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
+		case 3: mt_generate_kernel<3><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
+		default: mt_generate_kernel<4><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
+	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 }
@@ -407,7 +429,7 @@ void launch_mt_window_update(Ctx* c, const std::vector<MtWindowSpec>& specs) {
 		jobs[k] = WindowJob{specs[k].p, specs[k].words, specs[k].n_words, specs[k].attempts,
 		                    specs[k].window, specs[k].position};
 	auto* d_jobs = static_cast<WindowJob*>(scratch_take(c, sizeof(WindowJob) * jobs.size()));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(WindowJob) * jobs.size(),
+	ARMA_CUDA_TRY(copy_async(c, d_jobs, jobs.data(), sizeof(WindowJob) * jobs.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
 	mt_window_kernel<<<int(jobs.size()), 256, 0, c->stream>>>(d_jobs);
 	ARMA_CUDA_TRY(cudaGetLastError());

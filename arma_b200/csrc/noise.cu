@@ -173,7 +173,7 @@ bool launch_white_noise(Ctx* c, const uint32_t* d_words, uint64_t n_words,
 	long long* total = static_cast<long long*>(scratch_take(c, sizeof(long long)));
 	enqueue_white_noise(c, d_words, n_words, stddev, n, precision, d_out, total);
 	long long h_total = 0;
-	ARMA_CUDA_TRY(cudaMemcpyAsync(&h_total, total, sizeof(h_total), cudaMemcpyDeviceToHost, c->stream));
+	ARMA_CUDA_TRY(copy_async(c, &h_total, total, sizeof(h_total), cudaMemcpyDeviceToHost, c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	return uint64_t(h_total) * 2 >= n;
 }
@@ -302,7 +302,7 @@ void enqueue_white_noise_batch(Ctx* c, const std::vector<NoiseSpec>& specs, int 
 	auto* d_jobs = static_cast<NoiseJob*>(scratch_take(c, sizeof(NoiseJob) * jobs.size()));
 	int* counts = static_cast<int*>(scratch_take(c, sizeof(int) * total_blocks));
 	long long* offsets = static_cast<long long*>(scratch_take(c, sizeof(long long) * total_blocks));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(NoiseJob) * jobs.size(),
+	ARMA_CUDA_TRY(copy_async(c, d_jobs, jobs.data(), sizeof(NoiseJob) * jobs.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
 	const int nj = int(jobs.size());
 	noise_count_batch_kernel<<<int(total_blocks), kThreads, 0, c->stream>>>(d_jobs, nj, counts);

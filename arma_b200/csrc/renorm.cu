@@ -205,12 +205,12 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 		sblocks += int((jobs[k].n + kScaleChunk - 1) / kScaleChunk);
 	}
 	int* d_first = static_cast<int*>(scratch_take(c, sizeof(int) * ns));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_first, first.data(), sizeof(int) * ns, cudaMemcpyHostToDevice,
+	ARMA_CUDA_TRY(copy_async(c, d_first, first.data(), sizeof(int) * ns, cudaMemcpyHostToDevice,
 	                              c->stream));
 	auto* d_jobs = static_cast<RenormJob*>(scratch_take(c, sizeof(RenormJob) * jobs.size()));
 	double* partial = static_cast<double*>(scratch_take(c, sizeof(double) * ns * kBatchBlocks));
 	double* means = static_cast<double*>(scratch_take(c, sizeof(double) * ns));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(RenormJob) * jobs.size(),
+	ARMA_CUDA_TRY(copy_async(c, d_jobs, jobs.data(), sizeof(RenormJob) * jobs.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
 	const int g = ns * kBatchBlocks;
 	if (precision == ARMA_FP64) {

@@ -77,6 +77,9 @@ int arma_ctx_set_stream(arma_ctx* ctx, void* cuda_stream);
 int arma_ctx_synchronize(arma_ctx* ctx);
 /* Kernel launches issued through this context since creation (counter). */
 int arma_ctx_launch_count(arma_ctx* ctx, uint64_t* count);
+/* Bytes the context's calls have copied host->device and device->host since
+ * creation (counters): inputs, descriptors, coefficient tables, results. */
+int arma_ctx_transfer_bytes(arma_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
 /* Per-kernel-class device timing: when enabled, CUDA events are recorded on
  * the context's stream around each launch of the named classes ("mt",
  * "noise", "ar64", "ar32c", "renorm", "nit", "velocity").  arma_ctx_profile
@@ -103,6 +106,23 @@ int arma_mt_file_read(const char* path, int index, arma_mt_params* out);
 int arma_mt_file_write(const char* path, const arma_mt_params* sets, int n);
 /* The standard MT19937 parameter set in dcmt form. */
 int arma_mt19937_params(arma_mt_params* out);
+/* Creates the dcmt parameter set of generator `id` (0 <= id < 65536) of period
+ * 2^p - 1, w = 32: replaces get_mt_parameter_id_st(32, p, id, seed), which the
+ * reference's parallel_mt_seq calls (src/parallel_mt.hh:199-203) for
+ * arma-dcmt (src/dcmt.cc:15-33; p = 521 there).  p must be a Mersenne
+ * exponent (521, 607, 1279, 2203, 2281, 3217, 4253, 4423, 9689, 9941, 11213,
+ * 19937, 21701, 23209, 44497).  The result depends only on (p, id, seed).
+ * The id sits in the low 16 bits of aaa; when none of the 2^15 twist vectors
+ * of that id gives a primitive characteristic polynomial the call fails with
+ * ARMA_ENUMERIC (the reference then throws "bad MT"). */
+int arma_mt_create(int w, int p, int id, uint32_t seed, arma_mt_params* out);
+/* *primitive = 1 when the set's characteristic polynomial is primitive
+ * (period 2^p - 1 with p = 32 nn - rr a Mersenne exponent), else 0. */
+int arma_mt_is_primitive(const arma_mt_params* p, int* primitive);
+/* k_out[v-1] = k(v), v = 1..vmax (vmax <= 32): the dimension of
+ * equidistribution of the top v bits of the tempered output (-1 where the
+ * lattice reduction did not close). */
+int arma_mt_equidistribution(const arma_mt_params* p, int vmax, int* k_out);
 /* n tempered words of the stream seeded with `seed` (sgenrand_mt then
  * genrand_mt, src/parallel_mt.hh:236,259), starting at word `offset`. */
 int arma_mt_genrand(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed,
