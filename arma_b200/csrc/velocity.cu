@@ -154,14 +154,26 @@ struct SegWalk {
 	double prev_p = 0.0;    // representative period of run m-2
 	Run r0{0, 0.0, 0.0};    // run 0 once closed
 	double r1_p = 0.0;      // run 1 once closed
-	double mn = DBL_MAX, mx = DBL_MIN;  // pairs (r-1, r) with r >= 2, closed
+	// |period difference| extremes of the pairs (r-1, r) with r >= 2 that
+	// closed; k is a decreasing function of it, evaluated once at the end
+	double dmin = INFINITY, dmax = -INFINITY;
 };
 
-__device__ __forceinline__ void pair_k(double p0, double p1, double& mn, double& mx) {
-	const double w = k2Pi / fabs((p1 - p0) * 2.0);
-	const double k = w * w / kG;
-	if (k < mn) mn = k;
-	if (k > mx) mx = k;
+// The reference forms k = (2 pi / |2 (p1 - p0)|)^2 / g for every pair and
+// keeps min and max k.  Rounded division, squaring and division by g are each
+// monotone, so k is a non-increasing function of d = |p1 - p0| and
+// min k = k(max d), max k = k(min d) exactly; the walk keeps d's extremes and
+// k_of is applied once per axis.  (A NaN period gives a NaN d and a NaN k,
+// which the reference's comparisons skip; so do these.)
+__device__ __forceinline__ void pair_k(double p0, double p1, double& dmin, double& dmax) {
+	const double d = fabs(p1 - p0);
+	if (d < dmin) dmin = d;
+	if (d > dmax) dmax = d;
+}
+
+__device__ __forceinline__ double k_of(double d) {
+	const double w = k2Pi / fabs(d * 2.0);
+	return w * w / kG;
 }
 
 // One event of a thread's own segment, in loop order.
@@ -180,7 +192,7 @@ __device__ __forceinline__ void seg_event(SegWalk& st, double e, double p) {
 		const int r = st.m - 1;  // the open run closes
 		if (r == 0) st.r0 = st.open;
 		else if (r == 1) st.r1_p = st.open.best_p;
-		else pair_k(st.prev_p, st.open.best_p, st.mn, st.mx);
+		else pair_k(st.prev_p, st.open.best_p, st.dmin, st.dmax);
 		st.prev_p = st.open.best_p;
 		st.open = Run{s, ae, p};
 		++st.m;
@@ -196,8 +208,8 @@ __device__ SegWalk seg_join(const SegWalk& A, const SegWalk& B) {
 	if (A.m == 0) return B;
 	if (B.m == 0) return A;
 	SegWalk C;
-	C.mn = fmin(A.mn, B.mn);
-	C.mx = fmax(A.mx, B.mx);
+	C.dmin = fmin(A.dmin, B.dmin);
+	C.dmax = fmax(A.dmax, B.dmax);
 	C.r0 = A.r0;
 	C.r1_p = A.r1_p;
 	const Run b0 = B.m == 1 ? B.open : B.r0;
@@ -216,10 +228,10 @@ __device__ SegWalk seg_join(const SegWalk& A, const SegWalk& B) {
 		}
 		if (rR == 0) C.r0 = R;
 		else if (rR == 1) C.r1_p = R.best_p;
-		else pair_k(A.prev_p, R.best_p, C.mn, C.mx);
+		else pair_k(A.prev_p, R.best_p, C.dmin, C.dmax);
 		if (B.m >= 3) {  // B's run 1 (index rR + 1) closed
 			if (rR == 0) C.r1_p = B.r1_p;
-			else pair_k(R.best_p, B.r1_p, C.mn, C.mx);
+			else pair_k(R.best_p, B.r1_p, C.dmin, C.dmax);
 		}
 		C.open = B.open;
 		C.prev_p = B.m == 2 ? R.best_p : B.prev_p;
@@ -229,39 +241,49 @@ __device__ SegWalk seg_join(const SegWalk& A, const SegWalk& B) {
 	C.m = A.m + B.m;
 	if (rA == 0) C.r0 = A.open;
 	else if (rA == 1) C.r1_p = A.open.best_p;
-	else pair_k(A.prev_p, A.open.best_p, C.mn, C.mx);
+	else pair_k(A.prev_p, A.open.best_p, C.dmin, C.dmax);
 	if (B.m == 1) {
 		C.open = B.open;
 		C.prev_p = A.open.best_p;
 		return C;
 	}
 	if (A.m == 1) C.r1_p = b0.best_p;  // B's run 0 (index A.m) closed
-	else pair_k(A.open.best_p, b0.best_p, C.mn, C.mx);
-	if (B.m >= 3) pair_k(b0.best_p, B.r1_p, C.mn, C.mx);  // index A.m + 1 >= 2
+	else pair_k(A.open.best_p, b0.best_p, C.dmin, C.dmax);
+	if (B.m >= 3) pair_k(b0.best_p, B.r1_p, C.dmin, C.dmax);  // index A.m + 1 >= 2
 	C.open = B.open;
 	C.prev_p = B.m == 2 ? b0.best_p : B.prev_p;
 	return C;
 }
 
 // Extremum test and quadratic vertex at position a of a line (z0 = z(a),
-// z1 = z(a-1), z2 = z(a+1)), fed to the segment walk.
-__device__ __forceinline__ void fw_position(SegWalk& st, double z0, double z1, double z2, double dt,
-                                            int t) {
-	const double dw1 = z0 - z1, dw2 = z0 - z2;
-	if (!((dw1 > 0.0) ^ (dw2 > 0.0))) {
-		const double aa = -0.5 * (dw1 + dw2) / (dt * dt);
-		const double bb = dw1 / dt - aa * dt * (2.0 * t - 1.0);
-		const double cc = z0 - t * dt * (aa * t * dt + bb);
+// z1 = z(a-1), z2 = z(a+1)), fed to the segment walk.  The test needs only
+// the signs of z0 - z1 and z0 - z2, which a rounded subtraction always gets
+// right, so it runs in the input's own precision; the vertex is FP64.
+template <class T>
+__device__ __forceinline__ void fw_position(SegWalk& st, T z0, T z1, T z2, double dt, int t) {
+	if ((z0 - z1 > T(0)) == (z0 - z2 > T(0))) {
+		const double dw1 = double(z0) - double(z1), dw2 = double(z0) - double(z2);
+		double aa, bb, cc;
+		if (dt == 1.0) {  // x / 1 and x * 1 are exact: the same values without two divisions
+			aa = -0.5 * (dw1 + dw2);
+			bb = dw1 - aa * (2.0 * t - 1.0);
+			cc = double(z0) - t * (aa * t + bb);
+		} else {
+			aa = -0.5 * (dw1 + dw2) / (dt * dt);
+			bb = dw1 / dt - aa * dt * (2.0 * t - 1.0);
+			cc = double(z0) - t * dt * (aa * t * dt + bb);
+		}
 		const double tex = -0.5 * bb / aa;
 		seg_event(st, cc + tex * (bb + aa * tex), tex);
 	}
 }
 
-// Pieces per line: enough (line blocks of 32) x pieces for the CTA's warps,
-// at least 8 positions each.
+// Pieces per line: enough (line blocks of 32) x pieces for two units per
+// warp of the CTA, at least 8 positions each.
+constexpr int kFwBatch = 16;
 __host__ __device__ inline int fw_pieces(int outer, int npos) {
 	const int blocks = (outer + 31) / 32;
-	const int want = (kFwThreads / 32 + blocks - 1) / blocks;
+	const int want = (2 * (kFwThreads / 32) + blocks - 1) / blocks;
 	return npos < 16 ? 1 : (want < npos / 8 ? want : npos / 8);
 }
 
@@ -293,13 +315,23 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 		SegWalk st;
 		if (axis == 0) {
 			if (b < outer && a_lo < a_hi) {
-				double z1 = double(z[(long long)(a_lo - 1) * ny + b]);
-				double z0 = double(z[(long long)a_lo * ny + b]);
-				for (int a = a_lo; a < a_hi; ++a) {
-					const double z2 = double(z[(long long)(a + 1) * ny + b]);
-					fw_position(st, z0, z1, z2, dt, t);
-					z1 = z0;
-					z0 = z2;
+				// positions in batches of kFwBatch independent loads, so a lane
+				// has a batch in flight instead of one load per position
+				T z1 = z[(long long)(a_lo - 1) * ny + b];
+				T z0 = z[(long long)a_lo * ny + b];
+				for (int a0 = a_lo; a0 < a_hi; a0 += kFwBatch) {
+					const int n = min(kFwBatch, a_hi - a0);
+					T buf[kFwBatch];
+#pragma unroll
+					for (int k = 0; k < kFwBatch; ++k)
+						if (k < n) buf[k] = z[(long long)(a0 + 1 + k) * ny + b];
+#pragma unroll
+					for (int k = 0; k < kFwBatch; ++k)
+						if (k < n) {
+							fw_position(st, z0, z1, buf[k], dt, t);
+							z1 = z0;
+							z0 = buf[k];
+						}
 				}
 			}
 		} else {
@@ -315,10 +347,10 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 				__syncwarp();
 				if (b < outer) {
 					const T* row = tile + lane * kFwTile;  // row[k] = z(b, c0 - 1 + k)
-					double z1 = double(row[0]), z0 = double(row[1]);
+					T z1 = row[0], z0 = row[1];
 					const int n = min(32, a_hi - c0);
 					for (int k = 0; k < n; ++k) {
-						const double z2 = double(row[k + 2]);
+						const T z2 = row[k + 2];
 						fw_position(st, z0, z1, z2, dt, t);
 						z1 = z0;
 						z0 = z2;
@@ -336,9 +368,11 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 	}
 	if (threadIdx.x == 0) {
 		SegWalk all = nseg > 0 ? seg[0] : SegWalk{};
-		if (all.m >= 3) pair_k(all.r0.best_p, all.r1_p, all.mn, all.mx);  // runs 0 and 1
-		kout[slice * 4 + axis] = all.mn;      // min_k for this axis
-		kout[slice * 4 + 2 + axis] = all.mx;  // max_k
+		if (all.m >= 3) pair_k(all.r0.best_p, all.r1_p, all.dmin, all.dmax);  // runs 0 and 1
+		// min k and max k, starting from DBL_MAX and DBL_MIN as the reference does
+		const bool any = all.dmax >= 0.0;
+		kout[slice * 4 + axis] = any ? fmin(DBL_MAX, k_of(all.dmax)) : DBL_MAX;
+		kout[slice * 4 + 2 + axis] = any ? fmax(DBL_MIN, k_of(all.dmin)) : DBL_MIN;
 	}
 }
 
@@ -675,6 +709,386 @@ velocity_fused_kernel(const VelSlice<float>* __restrict__ sl, int nx, int ny, Ff
 	}
 }
 
+// ---------------------------------------------------------------- 2c. real fused
+// FP32 linear solver (mode 0) on power-of-two slices of up to 32768 points.
+//
+// zeta_t is real and only Re of the inverse is kept (the reference keeps the
+// real part, src/velocity/linear_solver.cc:115), so with F = FFT2(zeta_t)
+// Hermitian,  Re IFFT2(W F) = IFFT2(We F),  We(k) = (W(k) + W(-k)) / 2,  and
+// We F is Hermitian again.  Rows are paired: z(p, y) = u(2p, y) + i u(2p+1, y)
+// (u = zeta_t) is an M x ny complex array, M = nx / 2, whose FFT2 Z gives the
+// spectra E, O of the even and odd rows,
+//     E(a, b) = (Z(a, b) + conj Z(-a, -b)) / 2,  O = (Z - conj Z(-a, -b)) / 2i,
+//     U(a, b) = E + W_nx^a O,  U(a + M, b) = E - W_nx^a O.
+// The filtered spectrum U' = We U is packed back the same way,
+//     E' = S E + D W_nx^a O,  O' = S O + D W_nx^-a E,   S, D = (We(a) +- We(a+M)) / 2,
+// Z'(a, b) = E' + i O' and Z'(-a, -b) = conj E' + i conj O', and the inverse FFT2
+// of Z' holds M ny (phi(2p, y) + i phi(2p+1, y)).  One CTA per slice holds the
+// M x ny array in shared memory (half of a full complex spectrum); the line
+// FFTs run in registers.
+//
+// Line FFT (forward, natural order in and out; the inverse conjugates):
+// N = R1 R2 points by T = N / 16 threads of one warp, 16 points per thread.
+//   step 1: for n2 (thread t, t + T, ...): v[n1] = x[R2 n1 + n2], R1-point DFT,
+//           v[k1] *= W_N^(n2 k1)
+//   exchange through the line's own storage: x[R2 k1 + n2] = v[k1]
+//   step 2: for k1 (thread t, t + T, ...): w[n2] = x[R2 k1 + n2], R2-point DFT,
+//           X[k1 + R1 k2] = w[k2]
+// The threads of a line are consecutive lanes of one warp, so the exchange
+// needs only __syncwarp.
+constexpr int kRealMaxPoints = 32768;  // nx * ny of the real fused path (128 KB of float2)
+
+template <bool INV>
+__device__ __forceinline__ float2 cmul_tw(float2 a, float2 w) {
+	// a * w (forward) or a * conj(w) (inverse)
+	return INV ? make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y)
+	           : make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+
+// t * (-i) forward, t * i inverse
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 t) {
+	return INV ? make_float2(-t.y, t.x) : make_float2(t.y, -t.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4r(float2& a, float2& b, float2& c, float2& d) {
+	const float2 s0 = make_float2(a.x + c.x, a.y + c.y), d0 = make_float2(a.x - c.x, a.y - c.y);
+	const float2 s1 = make_float2(b.x + d.x, b.y + d.y);
+	const float2 d1 = mul_mi<INV>(make_float2(b.x - d.x, b.y - d.y));
+	a = make_float2(s0.x + s1.x, s0.y + s1.y);
+	b = make_float2(d0.x + d1.x, d0.y + d1.y);
+	c = make_float2(s0.x - s1.x, s0.y - s1.y);
+	d = make_float2(d0.x - d1.x, d0.y - d1.y);
+}
+
+// W_16^j, j = 0..15 (exp(-2 pi i j / 16)): the roots of the 16-point DFT
+__device__ __forceinline__ float2 w16(int j) {
+	constexpr float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+	constexpr float h = 0.70710678118654752440f;
+	switch (j & 15) {
+		case 0: return make_float2(1.f, 0.f);
+		case 1: return make_float2(c1, -s1);
+		case 2: return make_float2(h, -h);
+		case 3: return make_float2(s1, -c1);
+		case 4: return make_float2(0.f, -1.f);
+		case 5: return make_float2(-s1, -c1);
+		case 6: return make_float2(-h, -h);
+		case 7: return make_float2(-c1, -s1);
+		case 8: return make_float2(-1.f, 0.f);
+		case 9: return make_float2(-c1, s1);
+		case 10: return make_float2(-h, h);
+		case 11: return make_float2(-s1, c1);
+		case 12: return make_float2(0.f, 1.f);
+		case 13: return make_float2(s1, c1);
+		case 14: return make_float2(h, h);
+		default: return make_float2(c1, s1);
+	}
+}
+
+// In-register R-point DFT of v[0..R), natural order out.
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg(float2* v) {
+	if constexpr (R == 1) {
+	} else if constexpr (R == 2) {
+		const float2 a = v[0], b = v[1];
+		v[0] = make_float2(a.x + b.x, a.y + b.y);
+		v[1] = make_float2(a.x - b.x, a.y - b.y);
+	} else if constexpr (R == 4) {
+		dft4r<INV>(v[0], v[1], v[2], v[3]);
+	} else if constexpr (R == 8) {
+		// radix 2 over two 4-point DFTs of the even and odd samples
+		float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+		float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+		dft4r<INV>(e0, e1, e2, e3);
+		dft4r<INV>(o0, o1, o2, o3);
+		float2 e[4] = {e0, e1, e2, e3}, o[4] = {o0, o1, o2, o3};
+#pragma unroll
+		for (int k = 0; k < 4; ++k) {
+			const float2 t = cmul_tw<INV>(o[k], w16(2 * k));
+			v[k] = make_float2(e[k].x + t.x, e[k].y + t.y);
+			v[k + 4] = make_float2(e[k].x - t.x, e[k].y - t.y);
+		}
+	} else if constexpr (R == 16) {
+		// radix 4: F_r = DFT4(v[r], v[r+4], v[r+8], v[r+12]), then per k1 a
+		// DFT4 over r of W_16^(r k1) F_r[k1] -> X[k1 + 4 k2]
+		float2 f[4][4];
+#pragma unroll
+		for (int r = 0; r < 4; ++r) {
+			f[r][0] = v[r];
+			f[r][1] = v[r + 4];
+			f[r][2] = v[r + 8];
+			f[r][3] = v[r + 12];
+			dft4r<INV>(f[r][0], f[r][1], f[r][2], f[r][3]);
+		}
+#pragma unroll
+		for (int k1 = 0; k1 < 4; ++k1) {
+			float2 a = f[0][k1];
+			float2 b = cmul_tw<INV>(f[1][k1], w16(k1));
+			float2 c = cmul_tw<INV>(f[2][k1], w16(2 * k1));
+			float2 d = cmul_tw<INV>(f[3][k1], w16(3 * k1));
+			dft4r<INV>(a, b, c, d);
+			v[k1] = a;
+			v[k1 + 4] = b;
+			v[k1 + 8] = c;
+			v[k1 + 12] = d;
+		}
+	}
+}
+
+template <int N> struct LineShape;
+template <> struct LineShape<16> { static constexpr int R1 = 16, R2 = 1; };
+template <> struct LineShape<32> { static constexpr int R1 = 8, R2 = 4; };
+template <> struct LineShape<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct LineShape<128> { static constexpr int R1 = 16, R2 = 8; };
+template <> struct LineShape<256> { static constexpr int R1 = 16, R2 = 16; };
+
+// N-point FFT of the line x[0], x[es], ... by thread t of its T = N / 16
+// threads.  tw[j * ts] = W_N^j.  Every lane of the warp must call it the same
+// number of times (the exchange synchronises the warp); `active` = false for
+// lanes without a line.
+template <int N, bool INV>
+__device__ __forceinline__ void line_fft(float2* x, int es, int t, const float2* tw, int ts,
+                                         bool active) {
+	constexpr int R1 = LineShape<N>::R1, R2 = LineShape<N>::R2, T = N / 16;
+	if constexpr (R2 == 1) {
+		float2 v[16];
+		if (active) {
+#pragma unroll
+			for (int k = 0; k < 16; ++k) v[k] = x[k * es];
+			dft_reg<16, INV>(v);
+#pragma unroll
+			for (int k = 0; k < 16; ++k) x[k * es] = v[k];
+		}
+		return;
+	} else {
+		// The exchange position of (k1, n2) is R2 k1 + (n2 + k1) mod R2: a
+		// rotation inside each block of R2, which spreads the step-2 reads of
+		// neighbouring threads over the banks.  The rotated positions were
+		// loaded by other threads in step 1, so every load of the line
+		// completes (warp barrier) before any exchange write.
+		constexpr int S1 = R2 / T, S2 = R1 / T;
+		float2 v[S1][R1];
+		if (active) {
+#pragma unroll
+			for (int s = 0; s < S1; ++s) {
+				const int n2 = t + T * s;
+#pragma unroll
+				for (int n1 = 0; n1 < R1; ++n1) v[s][n1] = x[(R2 * n1 + n2) * es];
+				dft_reg<R1, INV>(v[s]);
+#pragma unroll
+				for (int k1 = 1; k1 < R1; ++k1) v[s][k1] = cmul_tw<INV>(v[s][k1], tw[n2 * k1 * ts]);
+			}
+		}
+		__syncwarp();
+		if (active) {
+#pragma unroll
+			for (int s = 0; s < S1; ++s) {
+				const int n2 = t + T * s;
+#pragma unroll
+				for (int k1 = 0; k1 < R1; ++k1) x[(R2 * k1 + (n2 + k1) % R2) * es] = v[s][k1];
+			}
+		}
+		__syncwarp();
+		float2 w[S2][R2];
+		if (active) {
+#pragma unroll
+			for (int s = 0; s < S2; ++s) {
+				const int k1 = t + T * s;
+#pragma unroll
+				for (int n2 = 0; n2 < R2; ++n2) w[s][n2] = x[(R2 * k1 + (n2 + k1) % R2) * es];
+				dft_reg<R2, INV>(w[s]);
+			}
+		}
+		__syncwarp();
+		if (active) {
+#pragma unroll
+			for (int s = 0; s < S2; ++s) {
+				const int k1 = t + T * s;
+#pragma unroll
+				for (int k2 = 0; k2 < R2; ++k2) x[(k1 + R1 * k2) * es] = w[s][k2];
+			}
+		}
+	}
+}
+
+// FFTs of `nlines` lines of length N: line l at a + l * lstride, elements
+// es apart.  Each line gets T = N / 16 lanes of one warp: consecutive lanes
+// on one line (rows), or, with lines_fastest, consecutive lanes on
+// consecutive lines (columns, whose elements are a row stride apart).  Every
+// warp runs the same number of rounds.
+template <int N, bool INV, int NT, bool LINES_FASTEST>
+__device__ __forceinline__ void lines_fft(float2* a, int nlines, int lstride, int es,
+                                          const float2* tw, int ts) {
+	constexpr int T = N / 16, G = 32 / T;  // G lines per warp
+	constexpr int per_round = NT / T;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int g = warp * G + (LINES_FASTEST ? lane % G : lane / T);
+	const int t = LINES_FASTEST ? lane / G : lane % T;
+	for (int l0 = 0; l0 < nlines; l0 += per_round) {
+		const int l = l0 + g;
+		const bool active = l < nlines;
+		line_fft<N, INV>(a + (active ? l : 0) * lstride, es, t, tw, ts, active);
+	}
+	__syncwarp();
+}
+
+// Row stride of the M x NY array in float2, chosen by counting the bank
+// conflicts of every access of the row and column passes (64-bit accesses,
+// 16 banks of 8 bytes per half warp): NY + NY / 16 keeps the row passes free
+// of conflicts; the column passes of M >= 64 keep at most two-way conflicts.
+template <int M, int NY> struct RealLd {
+	static constexpr int v = NY == 16 ? 17 : NY == 256 ? (M >= 64 ? 264 : 256) : NY + NY / 16;
+};
+
+// Even part of the window at natural-order frequency (kx, ky):
+// (W(k) + W(-k)) / 2 with W evaluated at the rotated grid indices.  Not
+// inlined: the FP64 window code would otherwise hold registers across the
+// FFT kernel's pairing loop.
+__device__ __noinline__ double window_even(int kx, int ky, int nx, int ny, double dkx, double dky,
+                                           double z, double depth) {
+	const int mx = kx == 0 ? 0 : nx - kx, my = ky == 0 ? 0 : ny - ky;
+	const double w1 = window_fixed(rotate_src(kx, nx), rotate_src(ky, ny), nx, ny, dkx, dky, z, depth);
+	const double w2 = window_fixed(rotate_src(mx, nx), rotate_src(my, ny), nx, ny, dkx, dky, z, depth);
+	return 0.5 * (w1 + w2);
+}
+
+template <int M, int NY, int NT>
+__global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1)
+velocity_real_kernel(const VelSlice<float>* __restrict__ sl, const double* __restrict__ kinfo,
+                     const double* __restrict__ zs, int nz, double depth,
+                     float2* __restrict__ spectra) {
+	constexpr int NX = 2 * M, LD = RealLd<M, NY>::v;
+	constexpr int L = NX > NY ? NX : NY;  // twiddle table: W_L^j
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	float2* A = reinterpret_cast<float2*>(smem_raw);  // M rows of LD
+	float2* tw = A + M * LD;                           // L
+	const int s = blockIdx.x;
+	const VelSlice<float> S = sl[s];
+	constexpr int n2 = NX * NY;
+	for (int j = threadIdx.x; j < L; j += NT) {
+		double sn, cs;
+		sincospi(2.0 * j / L, &sn, &cs);
+		tw[j] = make_float2(float(cs), float(-sn));
+	}
+	// zeta_t of rows 2p and 2p + 1 into z(p, y)
+	for (int q = threadIdx.x; q < M * NY; q += NT) {
+		const int p = q / NY, y = q % NY;
+		double re, im;
+		solver_input(S, NX, NY, (long long)(2 * p) * NY + y, re, im);
+		const double r0 = re;
+		solver_input(S, NX, NY, (long long)(2 * p + 1) * NY + y, re, im);
+		A[p * LD + y] = make_float2(float(r0), float(re));
+	}
+	__syncthreads();
+	lines_fft<NY, false, NT, false>(A, M, LD, 1, tw, L / NY);  // rows
+	__syncthreads();
+	lines_fft<M, false, NT, true>(A, NY, 1, LD, tw, L / M);    // columns
+	__syncthreads();
+	float2* spec = spectra ? spectra + (long long)s * M * NY : nullptr;
+	if (spec) {
+		for (int q = threadIdx.x; q < M * NY; q += NT) spec[q] = A[(q / NY) * LD + q % NY];
+		__syncthreads();  // the pairing pass rewrites A
+	}
+	const double wx = 1.0 / kinfo[s * 4 + 0], wy = 1.0 / kinfo[s * 4 + 1];
+	const double dkx = wx / (NX - 1), dky = wy / (NY - 1);
+	const float inv = float(1.0 / double(M * NY));
+	for (int iz = 0; iz < nz; ++iz) {
+		if (iz > 0) {
+			__syncthreads();  // the previous depth's output read A
+			for (int q = threadIdx.x; q < M * NY; q += NT) A[(q / NY) * LD + q % NY] = spec[q];
+			__syncthreads();
+		}
+		const double z = zs[iz];
+		auto We = [&](int kx, int ky) {
+			return window_even(kx, ky, NX, NY, dkx, dky, z, depth);
+		};
+		// one thread per pair {(a, b), (-a, -b)}: b in [0, NY/2], a in [0, M),
+		// with b in {0, NY/2} only a <= M/2 (the others are partners)
+		for (int q = threadIdx.x; q < M * (NY / 2 + 1); q += NT) {
+			const int b = q / M, a = q % M;
+			if ((b == 0 || b == NY / 2) && a > M / 2) continue;
+			const int am = a == 0 ? 0 : M - a, bm = b == 0 ? 0 : NY - b;
+			const float2 z1 = A[a * LD + b], z2 = A[am * LD + bm];
+			// E = (z1 + conj z2) / 2, O = (z1 - conj z2) / 2i
+			const float2 E = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
+			const float2 O = make_float2(0.5f * (z1.y + z2.y), -0.5f * (z1.x - z2.x));
+			const double wa = We(a, b), wb = We(a + M, b);
+			const float Sv = float(0.5 * (wa + wb)), Dv = float(0.5 * (wa - wb));
+			const float2 w = tw[a * (L / NX)];  // W_nx^a
+			const float2 wO = cmul_tw<false>(O, w), wE = cmul_tw<true>(E, w);
+			const float2 E2 = make_float2(Sv * E.x + Dv * wO.x, Sv * E.y + Dv * wO.y);
+			const float2 O2 = make_float2(Sv * O.x + Dv * wE.x, Sv * O.y + Dv * wE.y);
+			A[a * LD + b] = make_float2(E2.x - O2.y, E2.y + O2.x);     // E' + i O'
+			A[am * LD + bm] = make_float2(E2.x + O2.y, -E2.y + O2.x);  // conj E' + i conj O'
+		}
+		__syncthreads();
+		lines_fft<M, true, NT, true>(A, NY, 1, LD, tw, L / M);    // columns
+		__syncthreads();
+		lines_fft<NY, true, NT, false>(A, M, LD, 1, tw, L / NY);  // rows
+		__syncthreads();
+		float* out = S.out + (long long)iz * n2;
+		auto f = [&](int r, int c) -> double {
+			const float2 v = A[(r >> 1) * LD + c];
+			return double((r & 1) ? v.y : v.x) * double(inv);
+		};
+		for (int q = threadIdx.x; q < n2; q += NT) {
+			const int x = q / NY, y = q % NY;
+			if (x > 0 && y > 0) {
+				const float2 v = A[(x >> 1) * LD + y];
+				out[q] = ((x & 1) ? v.y : v.x) * inv;
+			} else {
+				out[q] = float(finish_at(x, y, NX, NY, f));
+			}
+		}
+	}
+}
+
+// The instantiated (M, NY) shapes: M in {16, 32, 64, 128}, NY in {16..256},
+// M * NY <= 16384.
+template <int M, int NY>
+bool launch_real_shape(Ctx* c, const VelSlice<float>* d_sl, int ns, int nx, int ny,
+                       const double* d_k, const double* d_z, int nz, double depth, float2* spectra) {
+	if (nx != 2 * M || ny != NY) return false;
+	if constexpr (M * NY > kRealMaxPoints / 2) {
+		return false;
+	} else {
+		constexpr int NT = M * NY >= 8192 ? 512 : 256;
+		constexpr int L = 2 * M > NY ? 2 * M : NY;
+		const size_t smem = sizeof(float2) * (size_t(M) * RealLd<M, NY>::v + L);
+		ARMA_CUDA_TRY(cudaFuncSetAttribute(velocity_real_kernel<M, NY, NT>,
+		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		velocity_real_kernel<M, NY, NT><<<ns, NT, smem, c->stream>>>(d_sl, d_k, d_z, nz, depth,
+		                                                              spectra);
+		return true;
+	}
+}
+
+template <int M>
+bool launch_real_m(Ctx* c, const VelSlice<float>* d_sl, int ns, int nx, int ny, const double* d_k,
+                   const double* d_z, int nz, double depth, float2* spectra) {
+	return launch_real_shape<M, 16>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
+	       launch_real_shape<M, 32>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
+	       launch_real_shape<M, 64>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
+	       launch_real_shape<M, 128>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
+	       launch_real_shape<M, 256>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra);
+}
+
+bool real_path_supported(int nx, int ny) {
+	auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+	return pow2(nx) && pow2(ny) && nx >= 32 && nx <= 256 && ny >= 16 && ny <= 256 &&
+	       nx * ny <= kRealMaxPoints;
+}
+
+bool launch_velocity_real(Ctx* c, const VelSlice<float>* d_sl, int ns, int nx, int ny,
+                          const double* d_k, const double* d_z, int nz, double depth,
+                          float2* spectra) {
+	return launch_real_m<16>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
+	       launch_real_m<32>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
+	       launch_real_m<64>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
+	       launch_real_m<128>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra);
+}
+
 // Radices of the forward stages: 4s first, then 2, 3, 5, 7, ... (at most
 // kMaxRadix); false when n has a larger prime factor.
 bool make_plan(int n, FftPlan* P) {
@@ -844,9 +1258,9 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	auto* d_sl = static_cast<VelSlice<T>*>(scratch_take(c, sizeof(VelSlice<T>) * ns));
 	double* d_z = static_cast<double*>(scratch_take(c, sizeof(double) * nz));
 	double* d_k = static_cast<double*>(scratch_take(c, sizeof(double) * 4 * ns));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_sl, slices.data(), sizeof(VelSlice<T>) * ns,
+	ARMA_CUDA_TRY(copy_async(c, d_sl, slices.data(), sizeof(VelSlice<T>) * ns,
 	                              cudaMemcpyHostToDevice, c->stream));
-	ARMA_CUDA_TRY(cudaMemcpyAsync(d_z, z, sizeof(double) * nz, cudaMemcpyHostToDevice, c->stream));
+	ARMA_CUDA_TRY(copy_async(c, d_z, z, sizeof(double) * nz, cudaMemcpyHostToDevice, c->stream));
 	{
 		const int nseg = std::max(nx * fw_pieces(nx, ny - 2), ny * fw_pieces(ny, nx - 2));
 		const size_t fw_smem = sizeof(SegWalk) * std::max(nseg, 1) +
@@ -857,6 +1271,18 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
+	bool linear_only = true;
+	for (const auto& v : slices) linear_only = linear_only && v.mode == 0;
+	if (sizeof(T) == sizeof(float) && linear_only && real_path_supported(nx, ny)) {
+		float2* spectra =
+		    nz > 1 ? static_cast<float2*>(scratch_take(c, sizeof(float2) * (n2 / 2) * ns)) : nullptr;
+		ARMA_REQUIRE(launch_velocity_real(c, reinterpret_cast<const VelSlice<float>*>(d_sl), ns, nx,
+		                                  ny, d_k, d_z, nz, depth, spectra),
+		             ARMA_EINVAL, "velocity solver: no real-input kernel for this slice shape");
+		ARMA_CUDA_TRY(cudaGetLastError());
+		c->launches += 1;
+		return;
+	}
 	if (sizeof(T) == sizeof(float) && n2 <= kFuseMax) {
 		const size_t smem = sizeof(float2) * (size_t(nx) * (ny + 1) + nx + ny) + sizeof(int) * (nx + ny);
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(velocity_fused_kernel,
