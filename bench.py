@@ -20,6 +20,7 @@ The CPU baseline is the oracle's restatement of the reference's OpenMP block
 wavefront on a bounded sample of the batch.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --stage velocity|ar|ar64|batch|nit|ma [...]   (one stage alone)
 """
 from __future__ import annotations
 
@@ -76,13 +77,14 @@ def fit_batch(batch):
 
 
 def mt_sets():
-    """The dcmt parameter sets (mt.dat when present, else MT19937 only)."""
+    """The 16 dcmt parameter sets of period 2^19937 - 1 (arma_b200/data/mt.dat,
+    created by ``python -m arma_b200.dcmt -n 16 -p 19937 -s 42``)."""
     import arma_b200 as A
     path = os.path.join(ROOT, "arma_b200", "data", "mt.dat")
-    if os.path.exists(path):
-        n = A.mt_file_count(path)
-        return [A.mt_file_read(path, k) for k in range(n)]
-    return [A.mt19937_params()]
+    n = A.mt_file_count(path)
+    if n != MT_SETS:
+        raise RuntimeError(f"{path}: {n} parameter sets, the workload needs {MT_SETS}")
+    return [A.mt_file_read(path, k) for k in range(n)]
 
 
 def points(batch):
@@ -167,19 +169,29 @@ class ClockSampler:
 
 # --------------------------------------------------------------------- CPU arms
 def cpu_sample(batch, seconds_hint: float):
-    """Pick a bounded sample of the batch for the CPU arms (small surfaces first
-    so the sample covers several orders), about `seconds_hint` of work."""
+    """A bounded sample of the batch with the batch's work mix, about
+    `seconds_hint` of CPU work: surfaces are visited in a seeded random order
+    and each is taken while the sample's flops stay within the budget, so the
+    sample's point-weighted order matches the batch's (reported beside it)."""
     rate = 1.5e9  # flop/s per core, rough planning figure for the scalar loop
     cores = os.cpu_count() or 1
     budget = seconds_hint * rate * cores
+    order = np.random.default_rng(7).permutation(len(batch))
     chosen, acc = [], 0.0
-    for s in sorted(batch, key=lambda s: np.prod(s["shape"])):
+    for k in order:
+        s = batch[int(k)]
         f = np.prod(s["shape"]) * 2 * (np.prod(s["order"]) - 1)
-        if acc + f > budget and chosen:
-            break
-        chosen.append(s)
-        acc += f
+        if acc + f <= budget:
+            chosen.append(s)
+            acc += f
+    if not chosen:
+        chosen = [min(batch, key=lambda s: np.prod(s["shape"]) * np.prod(s["order"]))]
     return chosen
+
+
+def weighted_taps(batch):
+    """Point-weighted mean number of AR coefficients P of a set of surfaces."""
+    return flops(batch) / (2.0 * points(batch)) + 1.0
 
 
 def run_cpu(sample, sets, nthreads):
@@ -211,17 +223,19 @@ def reference_arm(args):
     pts = points(sample)
     t = max(statistics.median(times), 1e-9)
     v = pts / t
-    desc = (f"{len(sample)} of the {N_SURFACES} surfaces ({pts} points, orders "
-            f"{sorted(set(s['order'] for s in sample))}); OpenMP block wavefront with per-thread "
-            f"MT noise + renormalisation, {cores} threads")
+    desc = (f"{len(sample)} of the {N_SURFACES} surfaces in seeded random order ({pts} points, "
+            f"point-weighted P {weighted_taps(sample):.0f} against {weighted_taps(batch):.0f} for "
+            f"the whole batch); OpenMP block wavefront with per-thread MT noise + "
+            f"renormalisation, {cores} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "batched-256-surfaces", "sample": desc},
+        "flops_per_s": flops(sample) / t,
         "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
-                         "sample": desc},
+                         "sample": desc, "flops_per_s": flops(sample) / t},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -242,7 +256,7 @@ def gpu_arm(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    batch = fit_batch(make_batch(rank)[:args.surfaces])
+    batch = fit_batch(make_batch(rank)[:args.surfaces or N_SURFACES])
     sets = mt_sets()
     ctx = A.Context(local)
     stream = torch.cuda.current_stream()
@@ -298,13 +312,17 @@ def gpu_arm(args):
                  for s, h in zip(batch, host)]
         ctx.batch_generate(surfh, A.FP32C, host=True)
         barrier()
+        h2d0, d2h0 = ctx.transfer_bytes()
         t0 = time.perf_counter()
-        e2e_steps = max(1, min(args.steps, 3))
+        e2e_steps = args.steps
         for _ in range(e2e_steps):
             ctx.batch_generate(surfh, A.FP32C, host=True)
         barrier()
         e2e_t = max_over_ranks(time.perf_counter() - t0)
+        h2d1, d2h1 = ctx.transfer_bytes()
         e2e = world * npts * e2e_steps / e2e_t
+        e2e_h2d = (h2d1 - h2d0) // e2e_steps
+        e2e_d2h = (d2h1 - d2h0) // e2e_steps
         # parity spot check of the host copy against the device result
         assert torch.equal(host[0], bufs32[0].cpu())
     del bufs32
@@ -351,8 +369,11 @@ def gpu_arm(args):
         cores = os.cpu_count() or 1
         t = run_cpu(sample, sets, cores)
         cpu = {"value": points(sample) / t, "unit": "points/s", "cores": cores, "kind": "port",
-               "sample": f"{len(sample)} smallest surfaces of the batch ({points(sample)} points), "
-                         f"OpenMP block wavefront restatement, {t:.1f} s"}
+               "flops_per_s": flops(sample) / t,
+               "sample": f"{len(sample)} surfaces of the batch in seeded random order "
+                         f"({points(sample)} points, point-weighted P {weighted_taps(sample):.0f} "
+                         f"against {weighted_taps(batch):.0f} for the batch), OpenMP block "
+                         f"wavefront restatement, {t:.1f} s"}
 
     full = None
     if not args.skip_full:
@@ -372,6 +393,7 @@ def gpu_arm(args):
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "flops_per_s": flops(batch) * world * args.steps / elapsed,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (compensated), f64 fit",
             "data": "synthetic (seeded numpy draws; no external dataset)",
             "config": {"workload": "batched-256-surfaces",
@@ -379,8 +401,11 @@ def gpu_arm(args):
                        "orders": "{4,6,8,10}^3", "precision": "fp32c",
                        "l2": "inputs larger than L2 (%.1f GB per rank)" % (npts * 4 / 1e9),
                        "parallelism": f"dp{world} (independent surfaces per rank)"},
-            "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": npts * 4} if e2e else None,
+            "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": e2e_h2d,
+                    "d2h_bytes_per_step": e2e_d2h, "steps": e2e_steps,
+                    "copies": "counted by the library (arma_ctx_transfer_bytes): host->device "
+                              "task lists, parameter sets and coefficient tables; device->host "
+                              "surfaces, scales and accepted-pair counts"} if e2e else None,
             "plain_fp64": {"value": plain, "unit": "points/s",
                            "ratio_fp32c_over_fp64": (value / plain) if plain else None},
             "gpu_launches": launches,
@@ -633,6 +658,115 @@ def serve_bench(A, seconds_per_load: float, seed: int = 42):
     }
 
 
+# --------------------------------------------------------------------- stages
+def _timed(ctx, stream, fn, warm=3, reps=5):
+    """Device milliseconds per call of fn (CUDA events on the library's
+    stream, `warm` untimed calls first)."""
+    import torch
+    for _ in range(warm):
+        fn()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_stage(args):
+    """One stage of the path in isolation, for timing and for ncu captures of
+    its kernels (``--stage NAME``); prints one line with the device time.
+
+    velocity  linear velocity solver on every slice of one propagating-wave
+              surface (order 10^3, FP32 compensated) of slices x side x side,
+              nz depth levels in {0, -1, -2, -4, ...}, infinite depth
+    ar        batched FP32 path (MT, noise, AR filter, renormalisation) on
+              `surfaces` standing-wave surfaces of one shape and order
+    ar64      the plain FP64 path on the same
+    batch     the bench batch's first `surfaces` surfaces, FP32 compensated
+    full      the bench's full path (noise + AR + renormalisation, NIT table,
+              velocity at z = 0 on every slice) on the first `surfaces`
+    nit       skew-normal NIT (1024-node table over +-5 sigma, or the per-point
+              bisection with --bisection) in place over one surface
+    ma        MA filter (zeta = eps - theta * eps) of one surface, random
+              coefficients of the given order"""
+    import torch
+    import arma_b200 as A
+    from arma_b200 import capi
+    ctx = A.Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    shape = (args.slices, args.side, args.side)
+    pts = int(np.prod(shape))
+    tag = "fp64" if args.fp64 else "fp32"
+    if args.stage == "velocity":
+        phi, var = A.ar_fit_analytic(A.ACF_PROPAGATING, (10, 10, 10), 1.0, 0.6, [0.04] * 3,
+                                     [0.3, 0.2])
+        prec, dt = (A.FP64, torch.float64) if args.fp64 else (A.FP32C, torch.float32)
+        z = torch.empty(shape, dtype=dt, device="cuda")
+        ctx.batch_generate([capi.make_surface(shape, phi, var, 1.0, A.mt19937_params(), 42,
+                                              z.data_ptr())], prec)
+        zs = [0.0, -1.0, -2.0, -4.0, -8.0, -16.0, -32.0, -64.0][:args.nz]
+        out = torch.empty((args.slices, args.nz, args.side, args.side), dtype=dt, device="cuda")
+        tidx = list(range(args.slices))
+        ms = _timed(ctx, stream, lambda: ctx.velocity_linear(
+            z.data_ptr(), shape, prec, (1.0, 1.0, 1.0), float("inf"), zs, tidx, out.data_ptr()))
+        print(f"velocity {args.slices}x{args.side}x{args.side} nz={args.nz} {tag}: "
+              f"{ms:.3f} ms/call, {pts / ms / 1e6:.2f} G points/s")
+    elif args.stage in ("ar", "ar64"):
+        order = (args.order,) * 3
+        phi, var = A.ar_fit_analytic(A.ACF_STANDING, order, 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+        prec, dt = (A.FP64, torch.float64) if args.stage == "ar64" else (A.FP32C, torch.float32)
+        nsurf = args.surfaces or 8
+        bufs = [torch.empty(shape, dtype=dt, device="cuda") for _ in range(nsurf)]
+        surfs = [capi.make_surface(shape, phi, var, 1.5, A.mt19937_params(), 42 + k, b.data_ptr())
+                 for k, b in enumerate(bufs)]
+        ms = _timed(ctx, stream, lambda: ctx.batch_generate(surfs, prec),
+                    warm=1 if args.stage == "ar64" else 3, reps=1 if args.stage == "ar64" else 5)
+        n = nsurf * pts
+        flop = n * 2.0 * (np.prod(order) - 1)
+        print(f"{args.stage} {nsurf} x {shape} order {order}: {ms:.3f} ms/call, "
+              f"{n / ms / 1e6:.2f} G points/s, {flop / ms / 1e9:.2f} TFLOP/s algorithmic")
+    elif args.stage == "batch":
+        batch = fit_batch(make_batch(0)[:args.surfaces or N_SURFACES])
+        sets = mt_sets()
+        bufs = [torch.empty(b["shape"], dtype=torch.float32, device="cuda") for b in batch]
+        surfs = [capi.make_surface(b["shape"], b["phi"], b["var"], b["acf0"],
+                                   sets[b["mtset"] % len(sets)], b["seed"], z.data_ptr())
+                 for b, z in zip(batch, bufs)]
+        ms = _timed(ctx, stream, lambda: ctx.batch_generate(surfs, A.FP32C))
+        print(f"batch {len(batch)} surfaces ({points(batch)} points): {ms:.3f} ms/call, "
+              f"{points(batch) / ms / 1e6:.2f} G points/s")
+    elif args.stage == "full":
+        batch = fit_batch(make_batch(0)[:args.surfaces or N_SURFACES])
+        r = full_path(A, capi, ctx, batch, mt_sets(), 2, stream)
+        print(f"full {len(batch)} surfaces ({points(batch)} points): {r['ms_per_step']:.2f} ms/step "
+              f"{json.dumps(r['stage_ms'])}")
+    elif args.stage == "nit":
+        z = torch.randn(shape, dtype=torch.float32, device="cuda")
+        method = A.NIT_BISECTION if args.bisection else A.NIT_LUT
+        ms = _timed(ctx, stream, lambda: ctx.nit_apply(
+            A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499], 1.0, method, pts, A.FP32C, z.data_ptr(),
+            interval=(-10.0, 10.0), eps=1e-6, max_iter=100, lut_nodes=1024, lut_range=5.0))
+        print(f"nit {'bisection' if args.bisection else 'lut'} {shape}: {ms:.3f} ms/call, "
+              f"{pts * 8 / ms / 1e6:.1f} GB/s of 8 B per point")
+    elif args.stage == "ma":
+        order = tuple(int(v) for v in args.ma_order.split(","))
+        rng = np.random.default_rng(1)
+        theta = rng.normal(0.0, 0.2 / np.sqrt(np.prod(order)), order)
+        prec, dt = (A.FP64, torch.float64) if args.fp64 else (A.FP32C, torch.float32)
+        eps = torch.randn(shape, dtype=dt, device="cuda")
+        z = torch.empty_like(eps)
+        ms = _timed(ctx, stream, lambda: ctx.ma_filter(theta, shape, prec, eps.data_ptr(),
+                                                         z.data_ptr()))
+        flop = pts * 2.0 * int(np.prod(order))
+        print(f"ma {shape} order {order} {tag}: {ms:.3f} ms/call, {pts / ms / 1e6:.2f} G points/s, "
+              f"{flop / ms / 1e9:.2f} TFLOP/s algorithmic")
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -642,7 +776,7 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--surfaces", type=int, default=N_SURFACES,
+    ap.add_argument("--surfaces", type=int, default=None,
                     help="use the first N surfaces of the batch (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-serve", action="store_true")
@@ -650,8 +784,19 @@ def main():
     ap.add_argument("--skip-precision", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=1.5,
                     help="Poisson phase length per load level")
+    ap.add_argument("--stage", choices=["velocity", "ar", "ar64", "batch", "full", "nit", "ma"],
+                    help="time one stage in isolation (profiling runs); see run_stage")
+    ap.add_argument("--side", type=int, default=128)
+    ap.add_argument("--slices", type=int, default=400)
+    ap.add_argument("--nz", type=int, default=4)
+    ap.add_argument("--order", type=int, default=8)
+    ap.add_argument("--ma-order", default="20,10,10")
+    ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--bisection", action="store_true")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.stage:
+        run_stage(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

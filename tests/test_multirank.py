@@ -57,3 +57,74 @@ def test_two_gloo_ranks_shard_by_surface():
     assert not set(seeds[0]) & set(seeds[1])       # independent realisations
     assert v0 == pytest.approx(2 * n0 * 3 / 2.0)   # whole-job points/s at the slowest rank
     assert n0 != n1 or seeds[0] != seeds[1]
+
+
+def _scaled(spec):
+    """A bench surface scaled down for the CPU oracle (same seed, parameter
+    set, order and ACF; shape divided by 16 in t and 8 in x and y)."""
+    nt, nx, ny = spec["shape"]
+    return dict(spec, shape=(max(8, nt // 16), max(4, nx // 8), max(4, ny // 8)))
+
+
+def _generate(spec, sets):
+    """One surface the way every rank's device path makes it: white noise from
+    the surface's own parameter set and seed, the AR filter, renormalisation."""
+    import numpy as np
+    import oracle as O
+    n = int(np.prod(spec["shape"]))
+    p = O.MtParams.from_buffer_copy(sets[spec["mtset"] % len(sets)])
+    eps = O.white_noise(p, spec["seed"], float(np.sqrt(spec["var"])), n).reshape(spec["shape"])
+    z, _ = O.variance_renorm(O.ar_filter(eps, spec["phi"]), spec["acf0"])
+    return z
+
+
+def _shard_rank(rank, world, port, q):
+    import hashlib
+    import sys
+    from datetime import timedelta
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        sets = bench.mt_sets()
+        batch = bench.fit_batch([_scaled(s) for s in bench.make_batch(rank, 4)])
+        mine = [(s["seed"], s["mtset"], hashlib.sha256(_generate(s, sets).tobytes()).hexdigest())
+                for s in batch]
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        q.put((rank, gathered))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_surfaces_equal_a_one_rank_run():
+    """Two gloo ranks each generate their own surfaces (the CPU oracle standing
+    in for the device path).  The union of what they produce equals the same
+    surfaces generated one after another in this single process, and no seed
+    repeats across ranks."""
+    import hashlib
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=300) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    gathered = res[0][1]
+    assert gathered == res[1][1]  # both ranks hold the same view
+    sets = bench.mt_sets()
+    for rank in range(2):
+        batch = bench.fit_batch([_scaled(s) for s in bench.make_batch(rank, 4)])
+        one = [(s["seed"], s["mtset"], hashlib.sha256(_generate(s, sets).tobytes()).hexdigest())
+               for s in batch]
+        assert [tuple(x) for x in gathered[rank]] == one
+    seeds = [x[0] for r in gathered for x in r]
+    assert len(seeds) == len(set(seeds))
