@@ -35,7 +35,6 @@ namespace {
 
 constexpr int kRingBits = 12;
 constexpr int kRing = 1 << kRingBits;  // ring of raw words, >= nn + (nn-mm)
-constexpr int kThreads = 256;
 constexpr int kLevels = 16;            // jump tables for J * 2^l, l < 16
 constexpr int kJumpThreads = 640;
 
@@ -74,12 +73,15 @@ __device__ __forceinline__ void seed_state(uint32_t* dst, uint32_t seed, const a
 	}
 }
 
-// W = ceil((n - m) / kThreads) words of every chunk per thread (n - m <=
-// kMaxOwn * kThreads covers every Mersenne exponent up to 44497).
+// The block has one thread per word of a chunk of n - m words, rounded up
+// to whole warps (up to kGenMaxThreads); longer chunks give each thread W =
+// ceil((n - m) / blockDim) words (n - m <= kMaxOwn * kGenMaxThreads covers
+// every Mersenne exponent up to 44497 several times over).
+constexpr int kGenMaxThreads = 1024;
 constexpr int kMaxOwn = 4;
 
 template <int W>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kGenMaxThreads)
 mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	__shared__ uint32_t ring[kRing];
 	const SegJob& jb = jobs[blockIdx.x];
@@ -96,8 +98,8 @@ mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	}
 	__syncthreads();
 	const uint32_t mask = kRing - 1;
-	// Thread t owns words t + i kThreads (i < W, those < n - m) of every chunk:
-	// segment word w = s (n-m) + t + i kThreads at step s, raw word r = n + w
+	// Thread t owns words t + i B (B = blockDim, i < W, those < n - m) of every
+	// chunk: segment word w = s (n-m) + t + i B at step s, raw word r = n + w
 	// at ring position r & mask (positions run modulo 2^32, a multiple of the
 	// ring size), so every index is a running register sum.  Each step emits
 	// the chunk computed by the step before and computes the next one: raw
@@ -112,7 +114,7 @@ mt_generate_kernel(const SegJob* __restrict__ jobs) {
 	bool owner[W];
 #pragma unroll
 	for (int i = 0; i < W; ++i) {
-		const int t = threadIdx.x + i * kThreads;
+		const int t = threadIdx.x + i * int(blockDim.x);
 		owner[i] = t < chunk;
 		r[i] = uint32_t(n + t);  // raw position of this word
 		o[i] = shift + t;        // its output index
@@ -301,7 +303,8 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		             "an MT job started from a window has no offset");
 		ARMA_REQUIRE(j.p.nn > 1 && j.p.mm > 0 && j.p.mm < j.p.nn && j.p.ww == 32, ARMA_EINVAL,
 		             "bad MT parameter set");
-		ARMA_REQUIRE(j.p.nn + (j.p.nn - j.p.mm) <= kRing && j.p.nn - j.p.mm <= kMaxOwn * kThreads,
+		ARMA_REQUIRE(j.p.nn + (j.p.nn - j.p.mm) <= kRing &&
+		                 j.p.nn - j.p.mm <= kMaxOwn * kGenMaxThreads,
 		             ARMA_EINVAL, "MT state too large for the device generator");
 	}
 	if (jobs.empty()) return;
@@ -409,13 +412,16 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 	auto* d_seg = static_cast<SegJob*>(scratch_take(c, sizeof(SegJob) * seg.size()));
 	ARMA_CUDA_TRY(copy_async(c, d_seg, seg.data(), sizeof(SegJob) * seg.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
-	int own = 1;  // words per thread and chunk: the largest chunk of the batch
-	for (const MtJob& j : jobs) own = std::max(own, (j.p.nn - j.p.mm + kThreads - 1) / kThreads);
+	int chunk = 1;  // the largest chunk of the batch
+	for (const MtJob& j : jobs) chunk = std::max(chunk, j.p.nn - j.p.mm);
+	const int threads = std::min(kGenMaxThreads, (chunk + 31) / 32 * 32);
+	const int own = (chunk + threads - 1) / threads;
+	const int grid = int(seg.size());
 	switch (own) {
-		case 1: mt_generate_kernel<1><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
-		case 2: mt_generate_kernel<2><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
-		case 3: mt_generate_kernel<3><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
-		default: mt_generate_kernel<4><<<int(seg.size()), kThreads, 0, c->stream>>>(d_seg); break;
+		case 1: mt_generate_kernel<1><<<grid, threads, 0, c->stream>>>(d_seg); break;
+		case 2: mt_generate_kernel<2><<<grid, threads, 0, c->stream>>>(d_seg); break;
+		case 3: mt_generate_kernel<3><<<grid, threads, 0, c->stream>>>(d_seg); break;
+		default: mt_generate_kernel<4><<<grid, threads, 0, c->stream>>>(d_seg); break;
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;

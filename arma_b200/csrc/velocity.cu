@@ -35,6 +35,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "internal.h"
 
 namespace armab {
@@ -71,13 +73,16 @@ __device__ __forceinline__ double zeta_t(const VelSlice<T>& s, long long n2, lon
 	double r;
 	if (nt - 1 < 2) {
 		r = double(f[d * n2]);
-	} else if (d == 0) {
-		r = 0.5 * (-double(f[2 * n2]) + 4.0 * double(f[n2]) - 3.0 * double(f[0])) / s.dt;
-	} else if (d == nt - 1) {
-		r = 0.5 * (3.0 * double(f[d * n2]) - 4.0 * double(f[(d - 1) * n2]) +
-		           double(f[(d - 2) * n2])) / s.dt;
 	} else {
-		r = 0.5 * (double(f[(d + 1) * n2]) - double(f[(d - 1) * n2])) / s.dt;
+		if (d == 0) {
+			r = 0.5 * (-double(f[2 * n2]) + 4.0 * double(f[n2]) - 3.0 * double(f[0]));
+		} else if (d == nt - 1) {
+			r = 0.5 * (3.0 * double(f[d * n2]) - 4.0 * double(f[(d - 1) * n2]) +
+			           double(f[(d - 2) * n2]));
+		} else {
+			r = 0.5 * (double(f[(d + 1) * n2]) - double(f[(d - 1) * n2]));
+		}
+		if (s.dt != 1.0) r /= s.dt;  // a division by 1 is exact: skipped
 	}
 	return -r;
 }
@@ -255,32 +260,107 @@ __device__ SegWalk seg_join(const SegWalk& A, const SegWalk& B) {
 	return C;
 }
 
+// Segment summaries in shared memory as a structure of arrays (8 double and
+// 3 int arrays of nseg entries), so that neighbouring threads touch
+// neighbouring words.
+constexpr int kSegBytes = 8 * 8 + 3 * 4;
+// bytes of n summaries, rounded up to 16 so that the staging tile after them
+// is aligned for any element type
+__host__ __device__ inline size_t seg_region_bytes(int n) {
+	return (size_t(kSegBytes) * size_t(n) + 15) & ~size_t(15);
+}
+
+struct SegStore {
+	double *oe, *op, *prev, *r0e, *r0p, *r1p, *dmin, *dmax;
+	int *m, *osign, *r0s;
+	__device__ SegStore(unsigned char* base, int n) {
+		double* d = reinterpret_cast<double*>(base);
+		oe = d; op = d + n; prev = d + 2 * n; r0e = d + 3 * n; r0p = d + 4 * n; r1p = d + 5 * n;
+		dmin = d + 6 * n; dmax = d + 7 * n;
+		int* q = reinterpret_cast<int*>(d + 8 * n);
+		m = q; osign = q + n; r0s = q + 2 * n;
+	}
+	__device__ void put(int i, const SegWalk& w) const {
+		oe[i] = w.open.best_e; op[i] = w.open.best_p; prev[i] = w.prev_p;
+		r0e[i] = w.r0.best_e; r0p[i] = w.r0.best_p; r1p[i] = w.r1_p;
+		dmin[i] = w.dmin; dmax[i] = w.dmax;
+		m[i] = w.m; osign[i] = w.open.sign; r0s[i] = w.r0.sign;
+	}
+	__device__ SegWalk get(int i) const {
+		SegWalk w;
+		w.open = Run{osign[i], oe[i], op[i]};
+		w.r0 = Run{r0s[i], r0e[i], r0p[i]};
+		w.prev_p = prev[i]; w.r1_p = r1p[i]; w.dmin = dmin[i]; w.dmax = dmax[i]; w.m = m[i];
+		return w;
+	}
+};
+
+__device__ __forceinline__ SegWalk seg_shfl_down(const SegWalk& w, int d) {
+	SegWalk o;
+	o.m = __shfl_down_sync(0xffffffffu, w.m, d);
+	o.open.sign = __shfl_down_sync(0xffffffffu, w.open.sign, d);
+	o.open.best_e = __shfl_down_sync(0xffffffffu, w.open.best_e, d);
+	o.open.best_p = __shfl_down_sync(0xffffffffu, w.open.best_p, d);
+	o.prev_p = __shfl_down_sync(0xffffffffu, w.prev_p, d);
+	o.r0.sign = __shfl_down_sync(0xffffffffu, w.r0.sign, d);
+	o.r0.best_e = __shfl_down_sync(0xffffffffu, w.r0.best_e, d);
+	o.r0.best_p = __shfl_down_sync(0xffffffffu, w.r0.best_p, d);
+	o.r1_p = __shfl_down_sync(0xffffffffu, w.r1_p, d);
+	o.dmin = __shfl_down_sync(0xffffffffu, w.dmin, d);
+	o.dmax = __shfl_down_sync(0xffffffffu, w.dmax, d);
+	return o;
+}
+
 // Extremum test and quadratic vertex at position a of a line (z0 = z(a),
-// z1 = z(a-1), z2 = z(a+1)), fed to the segment walk.  The test needs only
-// the signs of z0 - z1 and z0 - z2, which a rounded subtraction always gets
-// right, so it runs in the input's own precision; the vertex is FP64.
+// z1 = z(a-1), z2 = z(a+1)).  The test needs only the signs of z0 - z1 and
+// z0 - z2, which a rounded subtraction always gets right, so it runs in the
+// input's own precision; the vertex (the reference's formula) is FP64.
 template <class T>
-__device__ __forceinline__ void fw_position(SegWalk& st, T z0, T z1, T z2, double dt, int t) {
-	if ((z0 - z1 > T(0)) == (z0 - z2 > T(0))) {
-		const double dw1 = double(z0) - double(z1), dw2 = double(z0) - double(z2);
-		double aa, bb, cc;
-		if (dt == 1.0) {  // x / 1 and x * 1 are exact: the same values without two divisions
-			aa = -0.5 * (dw1 + dw2);
-			bb = dw1 - aa * (2.0 * t - 1.0);
-			cc = double(z0) - t * (aa * t + bb);
-		} else {
-			aa = -0.5 * (dw1 + dw2) / (dt * dt);
-			bb = dw1 / dt - aa * dt * (2.0 * t - 1.0);
-			cc = double(z0) - t * dt * (aa * t * dt + bb);
+__device__ __forceinline__ bool fw_extremum(T z0, T z1, T z2) {
+	return (z0 - z1 > T(0)) == (z0 - z2 > T(0));
+}
+
+template <class T>
+__device__ __forceinline__ void fw_vertex(T z0, T z1, T z2, double dt, int t, double& elev,
+                                          double& tex) {
+	const double dw1 = double(z0) - double(z1), dw2 = double(z0) - double(z2);
+	double aa, bb, cc;
+	if (dt == 1.0) {  // x / 1 and x * 1 are exact: the same values without two divisions
+		aa = -0.5 * (dw1 + dw2);
+		bb = dw1 - aa * (2.0 * t - 1.0);
+		cc = double(z0) - t * (aa * t + bb);
+	} else {
+		aa = -0.5 * (dw1 + dw2) / (dt * dt);
+		bb = dw1 / dt - aa * dt * (2.0 * t - 1.0);
+		cc = double(z0) - t * dt * (aa * t * dt + bb);
+	}
+	tex = -0.5 * bb / aa;
+	elev = cc + tex * (bb + aa * tex);
+}
+
+// n (<= kFwBatch) consecutive positions after (z1, z0), fed to the walk in
+// order; leaves (z1, z0) at the last two values.
+constexpr int kFwBatch = 8;
+template <class T>
+__device__ __forceinline__ void fw_batch(SegWalk& st, T& z1, T& z0, const T* zn, int n, double dt,
+                                         int t) {
+#pragma unroll
+	for (int k = 0; k < kFwBatch; ++k) {
+		if (k < n) {
+			const T z2 = zn[k];
+			if (fw_extremum(z0, z1, z2)) {
+				double e, p;
+				fw_vertex(z0, z1, z2, dt, t, e, p);
+				seg_event(st, e, p);
+			}
+			z1 = z0;
+			z0 = z2;
 		}
-		const double tex = -0.5 * bb / aa;
-		seg_event(st, cc + tex * (bb + aa * tex), tex);
 	}
 }
 
 // Pieces per line: enough (line blocks of 32) x pieces for two units per
 // warp of the CTA, at least 8 positions each.
-constexpr int kFwBatch = 16;
 __host__ __device__ inline int fw_pieces(int outer, int npos) {
 	const int blocks = (outer + 31) / 32;
 	const int want = (2 * (kFwThreads / 32) + blocks - 1) / blocks;
@@ -293,7 +373,7 @@ __host__ __device__ inline int fw_pieces(int outer, int npos) {
 // warp staging 32 rows x 34 columns at a time through shared memory.  Writes
 // min_k, max_k of the axis.
 template <class T>
-__global__ void __launch_bounds__(kFwThreads)
+__global__ void __launch_bounds__(kFwThreads, 2)
 factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* __restrict__ kout) {
 	extern __shared__ __align__(16) unsigned char fw_smem[];
 	const int slice = blockIdx.x >> 1, axis = blockIdx.x & 1;
@@ -307,8 +387,9 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 	const int npos = (axis == 0 ? nx : ny) - 2;  // positions 1 .. npos of each line
 	const int P = fw_pieces(outer, npos), per = (npos + P - 1) / P;
 	const int nseg = outer * P, blocks = (outer + 31) / 32;
-	SegWalk* seg = reinterpret_cast<SegWalk*>(fw_smem);
-	T* tile = reinterpret_cast<T*>(seg + max(nseg, 1)) + warp * 32 * kFwTile;
+	const int nstore = max(nseg, nwarps);  // segments, then the warps' results
+	const SegStore seg(fw_smem, nstore);
+	T* tile = reinterpret_cast<T*>(fw_smem + seg_region_bytes(nstore)) + warp * 32 * kFwTile;
 	for (int u = warp; u < blocks * P; u += nwarps) {
 		const int piece = u / blocks, b0 = (u % blocks) * 32, b = b0 + lane;
 		const int a_lo = 1 + piece * per, a_hi = 1 + min(npos, (piece + 1) * per);  // [a_lo, a_hi)
@@ -325,13 +406,7 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 #pragma unroll
 					for (int k = 0; k < kFwBatch; ++k)
 						if (k < n) buf[k] = z[(long long)(a0 + 1 + k) * ny + b];
-#pragma unroll
-					for (int k = 0; k < kFwBatch; ++k)
-						if (k < n) {
-							fw_position(st, z0, z1, buf[k], dt, t);
-							z1 = z0;
-							z0 = buf[k];
-						}
+					fw_batch(st, z1, z0, buf, n, dt, t);
 				}
 			}
 		} else {
@@ -349,25 +424,35 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 					const T* row = tile + lane * kFwTile;  // row[k] = z(b, c0 - 1 + k)
 					T z1 = row[0], z0 = row[1];
 					const int n = min(32, a_hi - c0);
-					for (int k = 0; k < n; ++k) {
-						const T z2 = row[k + 2];
-						fw_position(st, z0, z1, z2, dt, t);
-						z1 = z0;
-						z0 = z2;
-					}
+					for (int k0 = 0; k0 < n; k0 += kFwBatch)
+						fw_batch(st, z1, z0, row + 2 + k0, min(kFwBatch, n - k0), dt, t);
 				}
 			}
 		}
-		if (b < outer) seg[b * P + piece] = st;  // loop order: line, then piece
+		if (b < outer) seg.put(b * P + piece, st);  // loop order: line, then piece
 	}
 	__syncthreads();
-	for (int stride = 1; stride < nseg; stride <<= 1) {
-		for (int i = threadIdx.x * 2 * stride; i + stride < nseg; i += blockDim.x * 2 * stride)
-			seg[i] = seg_join(seg[i], seg[i + stride]);
-		__syncthreads();
+	// join in loop order: every warp a contiguous range, every lane a
+	// contiguous piece of it folded in sequence, then a shuffle tree over the
+	// lanes (lane l's range precedes lane l + d's), then the warps' results
+	const int per_warp = (nseg + nwarps - 1) / nwarps;
+	const int lo = min(nseg, warp * per_warp), hi = min(nseg, lo + per_warp);
+	const int per_lane = (hi - lo + 31) / 32;
+	SegWalk acc;
+	for (int j = 0; j < per_lane; ++j) {
+		const int i = lo + lane * per_lane + j;
+		if (i < hi) acc = seg_join(acc, seg.get(i));
 	}
+	for (int d = 1; d < 32; d <<= 1) {
+		const SegWalk other = seg_shfl_down(acc, d);
+		if ((lane & (2 * d - 1)) == 0) acc = seg_join(acc, other);
+	}
+	__syncthreads();  // the segment arrays are read; warp results reuse them
+	if (lane == 0) seg.put(warp, acc);
+	__syncthreads();
 	if (threadIdx.x == 0) {
-		SegWalk all = nseg > 0 ? seg[0] : SegWalk{};
+		SegWalk all;
+		for (int w = 0; w < nwarps; ++w) all = seg_join(all, seg.get(w));
 		if (all.m >= 3) pair_k(all.r0.best_p, all.r1_p, all.dmin, all.dmax);  // runs 0 and 1
 		// min k and max k, starting from DBL_MAX and DBL_MIN as the reference does
 		const bool any = all.dmax >= 0.0;
@@ -1004,9 +1089,10 @@ velocity_real_kernel(const VelSlice<float>* __restrict__ sl, const double* __res
 			return window_even(kx, ky, NX, NY, dkx, dky, z, depth);
 		};
 		// one thread per pair {(a, b), (-a, -b)}: b in [0, NY/2], a in [0, M),
-		// with b in {0, NY/2} only a <= M/2 (the others are partners)
+		// with b in {0, NY/2} only a <= M/2 (the others are partners);
+		// consecutive threads on consecutive b (one row of A)
 		for (int q = threadIdx.x; q < M * (NY / 2 + 1); q += NT) {
-			const int b = q / M, a = q % M;
+			const int a = q / (NY / 2 + 1), b = q % (NY / 2 + 1);
 			if ((b == 0 || b == NY / 2) && a > M / 2) continue;
 			const int am = a == 0 ? 0 : M - a, bm = b == 0 ? 0 : NY - b;
 			const float2 z1 = A[a * LD + b], z2 = A[am * LD + bm];
@@ -1074,15 +1160,151 @@ bool launch_real_m(Ctx* c, const VelSlice<float>* d_sl, int ns, int nx, int ny, 
 	       launch_real_shape<M, 256>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra);
 }
 
+// ---------------------------------------------------------------- 2d. real, cluster
+// The same solver for slices whose M x NY array (256 KB at 256 x 256) does not
+// fit one CTA's shared memory: a cluster of two CTAs, each holding H = M / 2
+// pair rows, with the halves exchanged through distributed shared memory.
+//   rows:     local NY-point FFTs of each CTA's pair rows
+//   columns:  the first radix-2 stage (decimation in frequency) across the
+//             halves, y0 = x[i] + x[i+H], y1 = (x[i] - x[i+H]) W_M^i, written
+//             to CTA 0 (y0) and CTA 1 (y1) -- each CTA computes the columns of
+//             its half of NY, reading and writing both halves -- then local
+//             H-point column FFTs: CTA r holds column frequencies 2j + r
+//   pairing:  a and -a have the same parity, so every pair is local
+//   inverse:  local H-point column FFTs, the radix-2 stage mirrored
+//             (x[i] = y0 + W_M^-i y1, x[i+H] = y0 - W_M^-i y1), local row FFTs
+// Cluster barriers separate every step that reads the other CTA's memory from
+// the writes before and after it.
+template <int M, int NY, int NT>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
+velocity_real2_kernel(const VelSlice<float>* __restrict__ sl, const double* __restrict__ kinfo,
+                      const double* __restrict__ zs, int nz, double depth,
+                      float2* __restrict__ spectra) {
+	namespace cg = cooperative_groups;
+	constexpr int NX = 2 * M, H = M / 2, LD = RealLd<H, NY>::v;
+	constexpr int L = NX > NY ? NX : NY;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	cg::cluster_group cl = cg::this_cluster();
+	const int rank = int(cl.block_rank());
+	float2* A = reinterpret_cast<float2*>(smem_raw);  // H rows of LD
+	float2* tw = A + H * LD;                           // L
+	float2* Ar = cl.map_shared_rank(A, rank ^ 1);      // the other half
+	float2* A0 = rank == 0 ? A : Ar;
+	float2* A1 = rank == 0 ? Ar : A;
+	const int s = blockIdx.x / 2;
+	const VelSlice<float> S = sl[s];
+	constexpr int n2 = NX * NY;
+	for (int j = threadIdx.x; j < L; j += NT) {
+		double sn, cs;
+		sincospi(2.0 * j / L, &sn, &cs);
+		tw[j] = make_float2(float(cs), float(-sn));
+	}
+	for (int q = threadIdx.x; q < H * NY; q += NT) {
+		const int i = q / NY, y = q % NY, p = rank * H + i;
+		double re, im;
+		solver_input(S, NX, NY, (long long)(2 * p) * NY + y, re, im);
+		const double r0 = re;
+		solver_input(S, NX, NY, (long long)(2 * p + 1) * NY + y, re, im);
+		A[i * LD + y] = make_float2(float(r0), float(re));
+	}
+	__syncthreads();
+	lines_fft<NY, false, NT, false>(A, H, LD, 1, tw, L / NY);  // rows
+	cl.sync();
+	for (int q = threadIdx.x; q < H * (NY / 2); q += NT) {  // radix-2 across the halves
+		const int i = q / (NY / 2), y = rank * (NY / 2) + q % (NY / 2);
+		const float2 x0 = A0[i * LD + y], x1 = A1[i * LD + y];
+		A0[i * LD + y] = make_float2(x0.x + x1.x, x0.y + x1.y);
+		A1[i * LD + y] = cmul_tw<false>(make_float2(x0.x - x1.x, x0.y - x1.y), tw[i * (L / M)]);
+	}
+	cl.sync();
+	lines_fft<H, false, NT, true>(A, NY, 1, LD, tw, L / H);  // columns, local
+	__syncthreads();
+	float2* spec = spectra ? spectra + (long long)s * M * NY + (long long)rank * H * NY : nullptr;
+	if (spec) {
+		for (int q = threadIdx.x; q < H * NY; q += NT) spec[q] = A[(q / NY) * LD + q % NY];
+		__syncthreads();
+	}
+	const double wx = 1.0 / kinfo[s * 4 + 0], wy = 1.0 / kinfo[s * 4 + 1];
+	const double dkx = wx / (NX - 1), dky = wy / (NY - 1);
+	const float inv = float(1.0 / double(M * NY));
+	for (int iz = 0; iz < nz; ++iz) {
+		if (iz > 0) {
+			cl.sync();  // the previous depth's output read both halves
+			for (int q = threadIdx.x; q < H * NY; q += NT) A[(q / NY) * LD + q % NY] = spec[q];
+			__syncthreads();
+		}
+		const double z = zs[iz];
+		// pairs {(a, b), (-a, -b)} with a = 2j + rank (local row j)
+		for (int q = threadIdx.x; q < H * (NY / 2 + 1); q += NT) {
+			const int j = q / (NY / 2 + 1), b = q % (NY / 2 + 1), a = 2 * j + rank;
+			if ((b == 0 || b == NY / 2) && a > M / 2) continue;
+			const int am = a == 0 ? 0 : M - a, bm = b == 0 ? 0 : NY - b;
+			const int jm = (am - rank) / 2;
+			const float2 z1 = A[j * LD + b], z2 = A[jm * LD + bm];
+			const float2 E = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
+			const float2 O = make_float2(0.5f * (z1.y + z2.y), -0.5f * (z1.x - z2.x));
+			const double wa = window_even(a, b, NX, NY, dkx, dky, z, depth);
+			const double wb = window_even(a + M, b, NX, NY, dkx, dky, z, depth);
+			const float Sv = float(0.5 * (wa + wb)), Dv = float(0.5 * (wa - wb));
+			const float2 w = tw[a * (L / NX)];  // W_nx^a
+			const float2 wO = cmul_tw<false>(O, w), wE = cmul_tw<true>(E, w);
+			const float2 E2 = make_float2(Sv * E.x + Dv * wO.x, Sv * E.y + Dv * wO.y);
+			const float2 O2 = make_float2(Sv * O.x + Dv * wE.x, Sv * O.y + Dv * wE.y);
+			A[j * LD + b] = make_float2(E2.x - O2.y, E2.y + O2.x);
+			A[jm * LD + bm] = make_float2(E2.x + O2.y, -E2.y + O2.x);
+		}
+		__syncthreads();
+		lines_fft<H, true, NT, true>(A, NY, 1, LD, tw, L / H);  // columns, local
+		cl.sync();
+		for (int q = threadIdx.x; q < H * (NY / 2); q += NT) {  // radix-2 across the halves
+			const int i = q / (NY / 2), y = rank * (NY / 2) + q % (NY / 2);
+			const float2 y0 = A0[i * LD + y];
+			const float2 y1 = cmul_tw<true>(A1[i * LD + y], tw[i * (L / M)]);
+			A0[i * LD + y] = make_float2(y0.x + y1.x, y0.y + y1.y);
+			A1[i * LD + y] = make_float2(y0.x - y1.x, y0.y - y1.y);
+		}
+		cl.sync();
+		lines_fft<NY, true, NT, false>(A, H, LD, 1, tw, L / NY);  // rows
+		cl.sync();  // the edge fix of the second half reads the first half's last row
+		float* out = S.out + (long long)iz * n2;
+		auto f = [&](int r, int c) -> double {
+			const int pr = r >> 1;
+			const float2* src = pr < H ? A0 : A1;
+			const float2 v = src[(pr % H) * LD + c];
+			return double((r & 1) ? v.y : v.x) * double(inv);
+		};
+		for (int q = threadIdx.x; q < 2 * H * NY; q += NT) {
+			const int x = rank * 2 * H + q / NY, y = q % NY;
+			float* o = out + (long long)x * NY + y;
+			if (x > 0 && y > 0) {
+				const float2 v = A[((x >> 1) - rank * H) * LD + y];
+				*o = ((x & 1) ? v.y : v.x) * inv;
+			} else {
+				*o = float(finish_at(x, y, NX, NY, f));
+			}
+		}
+	}
+	cl.sync();  // the other CTA may still read this one's shared memory
+}
+
 bool real_path_supported(int nx, int ny) {
 	auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
 	return pow2(nx) && pow2(ny) && nx >= 32 && nx <= 256 && ny >= 16 && ny <= 256 &&
-	       nx * ny <= kRealMaxPoints;
+	       (nx * ny <= kRealMaxPoints || (nx == 256 && ny == 256));
 }
 
 bool launch_velocity_real(Ctx* c, const VelSlice<float>* d_sl, int ns, int nx, int ny,
                           const double* d_k, const double* d_z, int nz, double depth,
                           float2* spectra) {
+	if (nx == 256 && ny == 256) {  // two CTAs per slice
+		constexpr int M = 128, NY = 256, NT = 512, H = M / 2;
+		const size_t smem = sizeof(float2) * (size_t(H) * RealLd<H, NY>::v + 256);
+		ARMA_CUDA_TRY(cudaFuncSetAttribute(velocity_real2_kernel<M, NY, NT>,
+		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		velocity_real2_kernel<M, NY, NT><<<2 * ns, NT, smem, c->stream>>>(d_sl, d_k, d_z, nz, depth,
+		                                                                  spectra);
+		return true;
+	}
 	return launch_real_m<16>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
 	       launch_real_m<32>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
 	       launch_real_m<64>(c, d_sl, ns, nx, ny, d_k, d_z, nz, depth, spectra) ||
@@ -1263,7 +1485,7 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	ARMA_CUDA_TRY(copy_async(c, d_z, z, sizeof(double) * nz, cudaMemcpyHostToDevice, c->stream));
 	{
 		const int nseg = std::max(nx * fw_pieces(nx, ny - 2), ny * fw_pieces(ny, nx - 2));
-		const size_t fw_smem = sizeof(SegWalk) * std::max(nseg, 1) +
+		const size_t fw_smem = seg_region_bytes(std::max(nseg, kFwThreads / 32)) +
 		                       sizeof(T) * (kFwThreads / 32) * 32 * kFwTile;
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(factor_waves_kernel<T>,
 		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(fw_smem)));

@@ -334,6 +334,29 @@ def test_velocity_vs_oracle(ctx, shape, depth, zs, tidx):
         assert np.abs(got - ref).max() <= tol * scale, (prec, np.abs(got - ref).max() / scale)
 
 
+@pytest.mark.parametrize("shape,depth,zs,tidx", [
+    ((4, 256, 256), np.inf, [0.0, -1.0, -2.0], [0, 1, 3]),  # two-CTA cluster kernel
+    ((4, 256, 128), 12.0, [0.0, -1.0], [0, 2, 3]),          # 32768 points in one CTA
+    ((4, 128, 256), np.inf, [0.0], [1, 2]),
+    ((4, 32, 16), 12.0, [0.0, -2.0], [0, 3]),               # the smallest real-input shape
+])
+def test_velocity_real_input_kernels_vs_oracle(ctx, shape, depth, zs, tidx):
+    """The FP32 real-input kernels (power-of-two slices, rows packed in pairs,
+    even part of the window) within 2e-4 of max|phi| of the oracle, with
+    several depths (the spectrum reloaded per depth) and both depth kinds."""
+    phi, var = A.ar_fit_analytic(A.ACF_PROPAGATING, (3, 3, 3), 1.0, 0.6, [0.04] * 3, [0.3, 0.2])
+    eps = O.white_noise(O.mt19937_params(), 5, np.sqrt(var), int(np.prod(shape))).reshape(shape)
+    zeta = O.ar_filter(eps, phi)
+    ref = O.velocity_linear(zeta, (1.0, 1.0, 1.0), depth, zs, tidx)
+    scale = np.abs(ref).max()
+    z = dev(zeta, torch.float32)
+    out = torch.zeros(ref.shape, dtype=torch.float32, device="cuda")
+    ctx.velocity_linear(z.data_ptr(), shape, A.FP32C, (1.0, 1.0, 1.0), depth, zs, tidx,
+                        out.data_ptr())
+    got = out.cpu().numpy().astype(np.float64)
+    assert np.abs(got - ref).max() <= 2e-4 * scale, np.abs(got - ref).max() / scale
+
+
 @pytest.mark.parametrize("offset,n", [(0, 5_000_000), (3_000_000, 1_500_000), (1_048_570, 20)])
 def test_mt_jump_ahead_segments_bit_exact(ctx, offset, n):
     """Streams longer than one 2^20-word segment are split by jump-ahead;
