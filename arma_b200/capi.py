@@ -47,6 +47,7 @@ EXPORTS = (
     "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf", "arma_velocity_high_amplitude",
     "arma_ma_fit", "arma_ma_filter", "arma_ma_generate", "arma_ctx_set_noise_margin",
     "arma_mt_create", "arma_mt_is_primitive", "arma_mt_equidistribution",
+    "arma_batch_generate_nit",
 )
 
 
@@ -80,6 +81,25 @@ class Surface(C.Structure):
         ("acf0", C.c_double), ("mt", MtParams), ("seed", C.c_uint32),
         ("d_zeta", C.c_void_p), ("scale", C.c_double),
     ]
+
+
+class NitTable(C.Structure):
+    """The NIT of one batch surface (``arma_nit_table``); dist < 0: none."""
+
+    _fields_ = [
+        ("dist", C.c_int), ("params", C.c_double * 3), ("stdev", C.c_double),
+        ("lut_nodes", C.c_int), ("lut_range", C.c_double),
+    ]
+
+
+def nit_table(dist=-1, params=(0.0, 0.0, 0.0), stdev=1.0, lut_nodes=1024, lut_range=5.0):
+    t = NitTable()
+    t.dist = dist
+    t.params = (C.c_double * 3)(*(list(params) + [0.0] * (3 - len(params))))
+    t.stdev = stdev
+    t.lut_nodes = lut_nodes
+    t.lut_range = lut_range
+    return t
 
 
 class VelocityJob(C.Structure):
@@ -179,6 +199,7 @@ def lib():
             "arma_velocity_linear": (i, [vp, vp, ip, i, dp, d, dp, i, ip, i, vp]),
             "arma_batch_generate": (i, [vp, C.POINTER(Surface), i, i]),
             "arma_batch_generate_host": (i, [vp, C.POINTER(Surface), i, i]),
+            "arma_batch_generate_nit": (i, [vp, C.POINTER(Surface), i, i, C.POINTER(NitTable)]),
             "arma_ar_filter_fp32c_noalloc": (i, [vp, dp, ip, ip, vp]),
             "arma_driver_open": (i, [C.c_char_p, i, C.POINTER(vp)]),
             "arma_driver_close": (i, [vp]),
@@ -493,6 +514,15 @@ class Context:
         arr = (Surface * len(surfaces))(*surfaces)
         fn = lib().arma_batch_generate_host if host else lib().arma_batch_generate
         _check(fn(self._h, arr, len(surfaces), precision))
+        for k, s in enumerate(surfaces):
+            s.scale = arr[k].scale
+        return [arr[k].scale for k in range(len(surfaces))]
+
+    def batch_generate_nit(self, surfaces, precision: int, tables):
+        """``arma_batch_generate_nit``: tables[k] from :func:`nit_table`."""
+        arr = (Surface * len(surfaces))(*surfaces)
+        tab = (NitTable * len(surfaces))(*tables)
+        _check(lib().arma_batch_generate_nit(self._h, arr, len(surfaces), precision, tab))
         for k, s in enumerate(surfaces):
             s.scale = arr[k].scale
         return [arr[k].scale for k in range(len(surfaces))]

@@ -302,6 +302,7 @@ int arma_ctx_destroy(arma_ctx* ctx) {
 			cudaEventDestroy(p.stop);
 		}
 		for (auto& kv : ctx->c.graphs) cudaGraphExecDestroy(kv.second);
+		for (auto& kv : ctx->c.nit_tables) cudaFree(kv.second);
 		for (auto& ch : ctx->chunks) pool_free(&ctx->c, ch.first);
 		cudaStreamSynchronize(ctx->c.stream);
 		if (ctx->c.copy_stream) {
@@ -818,16 +819,36 @@ int arma_velocity_linear_batch(arma_ctx* ctx, const arma_velocity_job* jobs, int
 // ---------------------------------------------------------------- batches
 namespace {
 
+// A surface's NIT table for the fused renormalisation pass (p == nullptr: none).
+struct SurfaceLut {
+	const void* p = nullptr;
+	int nodes = 0;
+	double x0 = 0.0, inv_dx = 0.0;
+};
+
 void renorm_surfaces(Ctx* c, arma_surface* s, int n, int precision, const std::vector<void*>& dz,
-                     bool host);
-void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz);
+                     bool host, const SurfaceLut* luts);
+void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz,
+                           const SurfaceLut* luts);
+
+RenormSpec renorm_spec(const arma_surface& s, void* z, double* d_scale, const SurfaceLut* lut) {
+	RenormSpec r{z, {s.shape[0], s.shape[1], s.shape[2]}, s.acf0, d_scale};
+	if (lut && lut->p) {
+		r.lut = lut->p;
+		r.lut_nodes = lut->nodes;
+		r.lut_x0 = lut->x0;
+		r.lut_inv_dx = lut->inv_dx;
+	}
+	return r;
+}
 
 // redo: the noise's accepted-pair counts are read back before the filter
 // (white_noise_batch, with its sequential fallback); otherwise the FP32 path
 // enqueues the noise, builds the filter's coefficient tables on the host while
 // the device generates it, and checks the counts at the end, generating a
 // surface whose noise ran short again on its own.
-void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo = false) {
+void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo = false,
+           const SurfaceLut* luts = nullptr) {
 	const size_t es = elem_size(precision);
 	std::vector<void*> dz(n);
 	for (int k = 0; k < n; ++k) {
@@ -840,13 +861,13 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo =
 		dz[k] = host ? scratch_take(c, np * es) : s[k].d_zeta;
 	}
 	if (host && precision == ARMA_FP32C && n >= 4 && !redo) {
-		pipelined_host_output(c, s, n, dz);
+		pipelined_host_output(c, s, n, dz, luts);
 		return;
 	}
 	if (precision == ARMA_FP64) {
 		white_noise_batch(c, s, n, precision, dz);
 		for (int k = 0; k < n; ++k) ar_filter(c, s[k].phi, s[k].order, s[k].shape, precision, dz[k]);
-		renorm_surfaces(c, s, n, precision, dz, host);
+		renorm_surfaces(c, s, n, precision, dz, host, luts);
 		return;
 	}
 	long long* d_pairs = nullptr;
@@ -871,10 +892,11 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo =
 		                              cudaMemcpyDeviceToHost, c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	check_device_error(c);
-	renorm_surfaces(c, s, n, precision, dz, host);
+	renorm_surfaces(c, s, n, precision, dz, host, luts);
 	if (d_pairs)
 		for (int k = 0; k < n; ++k)
-			if (noise_short(s[k], pairs[k])) batch(c, &s[k], 1, precision, host, true);
+			if (noise_short(s[k], pairs[k]))
+				batch(c, &s[k], 1, precision, host, true, luts ? luts + k : nullptr);
 }
 
 // FP32 surfaces into host buffers with the device->host copies overlapped with
@@ -885,7 +907,8 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo =
 // batch the copies take about 0.76 ms and the computation about 0.9 ms (noise
 // and filter, with the tail of each group's persistent launch), so the copies
 // keep up and only the last, smallest group's are exposed.
-void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz) {
+void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz,
+                           const SurfaceLut* luts) {
 	constexpr int G = 4;
 	const double frac[G] = {0.35, 0.30, 0.20, 0.15};
 	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
@@ -951,8 +974,7 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 			for (int k : members[g]) {
 				ga.push_back(as[k]);
 				if (s[k].acf0 > 0.0)
-					rs.push_back(RenormSpec{dz[k], {s[k].shape[0], s[k].shape[1], s[k].shape[2]},
-					                        s[k].acf0, d_scale + k});
+					rs.push_back(renorm_spec(s[k], dz[k], d_scale + k, luts ? luts + k : nullptr));
 			}
 			launch_ar32c(c, ga, tx, ty, 1);
 			launch_renorm_batch(c, rs, ARMA_FP32C);
@@ -982,7 +1004,8 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 			                         cudaMemcpyDeviceToHost));
 			for (size_t q = 0; q < pairs.size(); ++q)
 				if (noise_short(s[members[g][q]], pairs[q]))
-					batch(c, &s[members[g][q]], 1, ARMA_FP32C, true, true);
+					batch(c, &s[members[g][q]], 1, ARMA_FP32C, true, true,
+					      luts ? luts + members[g][q] : nullptr);
 		}
 	} catch (...) {
 		cudaStreamSynchronize(c->copy_stream);
@@ -995,14 +1018,12 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 // The variance renormalisation of each surface with acf0 > 0 (and the copy to
 // the host buffers when `host`), then the scales back into s[k].scale.
 void renorm_surfaces(Ctx* c, arma_surface* s, int n, int precision, const std::vector<void*>& dz,
-                     bool host) {
+                     bool host, const SurfaceLut* luts) {
 	const size_t es = elem_size(precision);
 	double* d_scale = static_cast<double*>(scratch_take(c, sizeof(double) * n));
 	std::vector<RenormSpec> rs;
 	for (int k = 0; k < n; ++k)
-		if (s[k].acf0 > 0.0)
-			rs.push_back(RenormSpec{dz[k], {s[k].shape[0], s[k].shape[1], s[k].shape[2]}, s[k].acf0,
-			                        d_scale + k});
+		if (s[k].acf0 > 0.0) rs.push_back(renorm_spec(s[k], dz[k], d_scale + k, luts ? luts + k : nullptr));
 	launch_renorm_batch(c, rs, precision);
 	if (host) {
 		for (int k = 0; k < n; ++k) {
@@ -1036,7 +1057,7 @@ void ma_batch(Ctx* c, arma_surface* s, int n, int precision) {
 	white_noise_batch(c, s, n, precision, eps);
 	for (int k = 0; k < n; ++k)
 		launch_ma_filter(c, s[k].phi, s[k].order, s[k].shape, precision, eps[k], dz[k]);
-	renorm_surfaces(c, s, n, precision, dz, false);
+	renorm_surfaces(c, s, n, precision, dz, false, nullptr);
 }
 
 }  // namespace
@@ -1069,6 +1090,60 @@ int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n, int p
 		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
 		scratch_begin(&ctx->c, 0);
 		batch(&ctx->c, surfaces, n, precision, true);
+	});
+}
+
+namespace {
+// The device NIT table of a specification (FP64 values, then FP32), built once
+// per context and specification.
+const double* nit_table_device(Ctx* c, const arma_nit_table& t, double* x0, double* dx) {
+	ARMA_REQUIRE(t.dist == ARMA_NIT_GRAM_CHARLIER || t.dist == ARMA_NIT_SKEW_NORMAL, ARMA_EINVAL,
+	             "bad distribution");
+	ARMA_REQUIRE(t.stdev > 0.0 && t.lut_nodes >= 4 && t.lut_range > 0.0, ARMA_EINVAL,
+	             "bad NIT table");
+	const double lo = -t.lut_range * t.stdev;
+	*x0 = lo;
+	*dx = (t.lut_range * t.stdev - lo) / (t.lut_nodes - 1);
+	std::vector<double> key{double(t.dist), t.params[0], t.params[1], t.params[2], t.stdev,
+	                        double(t.lut_nodes), t.lut_range};
+	auto it = c->nit_tables.find(key);
+	if (it != c->nit_tables.end()) return it->second;
+	double bx0, bdx;
+	std::vector<double> y;
+	nit_build_lut(t.dist, t.params, t.stdev, t.lut_nodes, t.lut_range, &bx0, &bdx, y);
+	std::vector<float> yf(y.begin(), y.end());
+	double* d = nullptr;
+	ARMA_CUDA_TRY(cudaMalloc(&d, (sizeof(double) + sizeof(float)) * t.lut_nodes));
+	ARMA_CUDA_TRY(cudaMemcpy(d, y.data(), sizeof(double) * t.lut_nodes, cudaMemcpyHostToDevice));
+	ARMA_CUDA_TRY(cudaMemcpy(d + t.lut_nodes, yf.data(), sizeof(float) * t.lut_nodes,
+	                         cudaMemcpyHostToDevice));
+	c->nit_tables.emplace(key, d);
+	return d;
+}
+}  // namespace
+
+int arma_batch_generate_nit(arma_ctx* ctx, arma_surface* surfaces, int n, int precision,
+                            const arma_nit_table* nit) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && surfaces && n > 0, ARMA_EINVAL, "bad argument");
+		elem_size(precision);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		std::vector<SurfaceLut> luts(n);
+		if (nit)
+			for (int k = 0; k < n; ++k) {
+				if (nit[k].dist < 0) continue;
+				ARMA_REQUIRE(surfaces[k].acf0 > 0.0, ARMA_EINVAL,
+				             "NIT needs the variance renormalisation (acf0 > 0)");
+				double x0, dx;
+				const double* d = nit_table_device(&ctx->c, nit[k], &x0, &dx);
+				luts[k].p = precision == ARMA_FP64 ? static_cast<const void*>(d)
+				                                   : static_cast<const void*>(d + nit[k].lut_nodes);
+				luts[k].nodes = nit[k].lut_nodes;
+				luts[k].x0 = x0;
+				luts[k].inv_dx = 1.0 / dx;
+			}
+		scratch_begin(&ctx->c, 0);
+		batch(&ctx->c, surfaces, n, precision, false, false, luts.data());
 	});
 }
 

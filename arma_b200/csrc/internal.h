@@ -58,6 +58,8 @@ struct Ctx {
 	int num_sms = 148;
 	// cached CUDA graphs for the FP64 plane sweep, keyed by a string
 	std::map<std::string, cudaGraphExec_t> graphs;
+	// NIT inverse-CDF tables by specification (double table, then float table)
+	std::map<std::vector<double>, double*> nit_tables;
 	// optional per-kernel-class timing with CUDA events on `stream`
 	bool profiling = false;
 	struct Pending {
@@ -68,6 +70,23 @@ struct Ctx {
 	std::map<std::string, double> prof_ms;
 	std::map<std::string, long long> prof_count;
 };
+
+// The NIT table map shared by the standalone NIT kernel and the fused
+// renormalisation: u = (z - x0) / dx, cubic Lagrange interpolation through
+// nodes i-1 .. i+2 inside, linear extrapolation beyond the end nodes.
+template <class T>
+__device__ __forceinline__ T nit_lut_map(T z, const T* __restrict__ y, int nodes, T x0, T inv_dx) {
+	const T u = (z - x0) * inv_dx;
+	if (u <= T(0)) return y[0] + (y[1] - y[0]) * u;
+	if (u >= T(nodes - 1)) return y[nodes - 1] + (y[nodes - 1] - y[nodes - 2]) * (u - T(nodes - 1));
+	int i = int(u);
+	i = min(max(i, 1), nodes - 3);
+	const T s = u - T(i);  // in [-1, 2) relative to node i
+	const T y0 = y[i - 1], y1 = y[i], y2 = y[i + 1], y3 = y[i + 2];
+	const T sm1 = s + T(1), s1 = s - T(1), s2 = s - T(2);
+	return -y0 * s * s1 * s2 * T(1.0 / 6.0) + y1 * sm1 * s1 * s2 * T(0.5) -
+	       y2 * sm1 * s * s2 * T(0.5) + y3 * sm1 * s * s1 * T(1.0 / 6.0);
+}
 
 // cudaMemcpyAsync that counts the bytes a context moves between host and
 // device (arma_ctx_transfer_bytes).
@@ -198,6 +217,11 @@ struct RenormSpec {
 	int shape[3];
 	double acf0;
 	double* d_scale;
+	// optional NIT inverse-CDF table applied right after the scale (same
+	// element type as the surface; nullptr: none)
+	const void* lut = nullptr;
+	int lut_nodes = 0;
+	double lut_x0 = 0.0, lut_inv_dx = 0.0;
 };
 // apply = false only computes the scales.
 void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int precision,

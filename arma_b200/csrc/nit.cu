@@ -14,6 +14,7 @@
 //              one write per value.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 
 #include "distributions.h"
 #include "internal.h"
@@ -48,6 +49,14 @@ nit_bisection_kernel(T* __restrict__ z, unsigned long long n, int d, double p0, 
 	}
 }
 
+// The table map over n values: groups of kLutPer 16-byte vectors per thread,
+// all loaded before any is mapped (the loads in flight together); the ragged
+// head and tail before / after the vectors scalar.
+template <class T> struct LutVec;
+template <> struct LutVec<float> { using type = float4; static constexpr int n = 4; };
+template <> struct LutVec<double> { using type = double2; static constexpr int n = 2; };
+constexpr int kLutPer = 4;
+
 template <class T>
 __global__ void __launch_bounds__(kThreads)
 nit_lut_kernel(T* __restrict__ z, unsigned long long n, const T* __restrict__ lut, int nodes,
@@ -56,26 +65,36 @@ nit_lut_kernel(T* __restrict__ z, unsigned long long n, const T* __restrict__ lu
 	T* y = reinterpret_cast<T*>(smem_raw);
 	for (int i = threadIdx.x; i < nodes; i += kThreads) y[i] = lut[i];
 	__syncthreads();
-	for (unsigned long long idx = blockIdx.x * (unsigned long long)kThreads + threadIdx.x;
-	     idx < n; idx += (unsigned long long)gridDim.x * kThreads) {
-		const T u = (z[idx] - x0) * inv_dx;
-		T r;
-		if (u <= T(0)) {
-			r = y[0] + (y[1] - y[0]) * u;
-		} else if (u >= T(nodes - 1)) {
-			r = y[nodes - 1] + (y[nodes - 1] - y[nodes - 2]) * (u - T(nodes - 1));
-		} else {
-			int i = int(u);
-			i = min(max(i, 1), nodes - 3);
-			const T s = u - T(i);  // in [-1, 2) relative to node i
-			const T y0 = y[i - 1], y1 = y[i], y2 = y[i + 1], y3 = y[i + 2];
-			// cubic Lagrange through nodes i-1, i, i+1, i+2 at offsets -1,0,1,2
-			const T sm1 = s + T(1), s1 = s - T(1), s2 = s - T(2);
-			r = -y0 * s * s1 * s2 * T(1.0 / 6.0) + y1 * sm1 * s1 * s2 * T(0.5) -
-			    y2 * sm1 * s * s2 * T(0.5) + y3 * sm1 * s * s1 * T(1.0 / 6.0);
+	using V = typename LutVec<T>::type;
+	constexpr int W = LutVec<T>::n;
+	// head: values before the first 16-byte boundary
+	const unsigned long long head =
+	    min(n, (unsigned long long)((16 - (reinterpret_cast<uintptr_t>(z) & 15)) & 15) / sizeof(T));
+	const unsigned long long gtid = blockIdx.x * (unsigned long long)kThreads + threadIdx.x;
+	const unsigned long long nthr = (unsigned long long)gridDim.x * kThreads;
+	if (gtid < head) z[gtid] = nit_lut_map(z[gtid], y, nodes, x0, inv_dx);
+	V* zv = reinterpret_cast<V*>(z + head);
+	const unsigned long long nv = (n - head) / W;
+	for (unsigned long long base = gtid; base < nv; base += nthr * kLutPer) {
+		V v[kLutPer];
+#pragma unroll
+		for (int r = 0; r < kLutPer; ++r) {
+			const unsigned long long i = base + r * nthr;
+			if (i < nv) v[r] = zv[i];
 		}
-		z[idx] = r;
+#pragma unroll
+		for (int r = 0; r < kLutPer; ++r) {
+			const unsigned long long i = base + r * nthr;
+			if (i < nv) {
+				T* e = reinterpret_cast<T*>(&v[r]);
+#pragma unroll
+				for (int k = 0; k < W; ++k) e[k] = nit_lut_map(e[k], y, nodes, x0, inv_dx);
+				zv[i] = v[r];
+			}
+		}
 	}
+	for (unsigned long long i = head + nv * W + gtid; i < n; i += nthr)
+		z[i] = nit_lut_map(z[i], y, nodes, x0, inv_dx);
 }
 
 void upload_gl20(Ctx* c) {

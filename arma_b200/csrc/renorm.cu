@@ -114,6 +114,10 @@ struct RenormJob {
 	unsigned long long off, cnt, n;
 	double acf0;
 	double* scale;
+	const void* lut;  // NIT table after the scale, or null
+	int lut_nodes;
+	int vec;          // z is 16-byte aligned: 16-byte accesses
+	double lut_x0, lut_inv_dx;
 };
 
 template <class T>
@@ -162,6 +166,12 @@ __global__ void finish_batch_kernel(const RenormJob* __restrict__ jobs,
 // last job whose first block is <= b.
 constexpr int kScaleChunk = kThreads * 16;
 
+template <class T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
+
+// zeta *= scale, then (when the job has one) the NIT table: one read and one
+// write per value, 16-byte accesses where the surface is aligned.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
 scale_batch_kernel(const RenormJob* __restrict__ jobs, const int* __restrict__ first_block,
@@ -174,9 +184,43 @@ scale_batch_kernel(const RenormJob* __restrict__ jobs, const int* __restrict__ f
 	const RenormJob& jb = jobs[lo];
 	T* x = static_cast<T*>(jb.z);
 	const double sc = *jb.scale;
+	const T* lut = static_cast<const T*>(jb.lut);
+	const int nodes = jb.lut_nodes;
+	const T x0 = T(jb.lut_x0), inv_dx = T(jb.lut_inv_dx);
+	auto map = [&](T v) {
+		v = T(double(v) * sc);
+		return lut ? nit_lut_map(v, lut, nodes, x0, inv_dx) : v;
+	};
 	const unsigned long long i0 = (unsigned long long)(blockIdx.x - first_block[lo]) * kScaleChunk;
 	const unsigned long long i1 = min(jb.n, i0 + kScaleChunk);
-	for (unsigned long long i = i0 + threadIdx.x; i < i1; i += kThreads) x[i] = T(double(x[i]) * sc);
+	if (jb.vec) {
+		// every thread's kPer vectors of the chunk are loaded before any is
+		// mapped, so that they are all in flight at once
+		using V = typename Vec16<T>::type;
+		constexpr int W = Vec16<T>::n;
+		constexpr int kPer = kScaleChunk / (W * kThreads);
+		const unsigned long long nv = (i1 - i0) / W;  // i0 is a multiple of kScaleChunk
+		V* xv = reinterpret_cast<V*>(x + i0);
+		V v[kPer];
+#pragma unroll
+		for (int r = 0; r < kPer; ++r) {
+			const unsigned long long i = threadIdx.x + (unsigned long long)r * kThreads;
+			if (i < nv) v[r] = xv[i];
+		}
+#pragma unroll
+		for (int r = 0; r < kPer; ++r) {
+			const unsigned long long i = threadIdx.x + (unsigned long long)r * kThreads;
+			if (i < nv) {
+				T* e = reinterpret_cast<T*>(&v[r]);
+#pragma unroll
+				for (int k = 0; k < W; ++k) e[k] = map(e[k]);
+				xv[i] = v[r];
+			}
+		}
+		for (unsigned long long i = i0 + nv * W + threadIdx.x; i < i1; i += kThreads) x[i] = map(x[i]);
+	} else {
+		for (unsigned long long i = i0 + threadIdx.x; i < i1; i += kThreads) x[i] = map(x[i]);
+	}
 }
 
 }  // namespace
@@ -195,6 +239,12 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 		j.n = (unsigned long long)nt * nx * ny;
 		j.acf0 = specs[k].acf0;
 		j.scale = specs[k].d_scale;
+		j.lut = specs[k].lut;
+		j.lut_nodes = specs[k].lut_nodes;
+		j.lut_x0 = specs[k].lut_x0;
+		j.lut_inv_dx = specs[k].lut_inv_dx;
+		j.vec = (reinterpret_cast<uintptr_t>(j.z) % 16) == 0;
+		ARMA_REQUIRE(!j.lut || j.lut_nodes >= 4, ARMA_EINVAL, "NIT table needs at least 4 nodes");
 		ARMA_REQUIRE(j.cnt >= 2, ARMA_EINVAL, "surface too small for variance renormalisation");
 	}
 	const int ns = int(jobs.size());

@@ -438,61 +438,59 @@ def gpu_arm(args):
 # --------------------------------------------------------------------- full path
 def full_path(A, capi, ctx, batch, sets, steps, stream):
     """The batched FP32 compensated path end to end on the device: noise, AR
-    filter and renormalisation for every surface (one call), the skew-normal
-    NIT (skewness 0.3: alpha 1.499) through the 1024-node inverse-CDF table,
-    and the linear velocity potential at z = 0 on every slice of every surface
-    (infinite depth), batched by slice shape.  Returns points/s and the
-    per-stage device milliseconds of one step."""
+    filter, renormalisation and the skew-normal NIT (skewness 0.3: alpha
+    1.499; 1024-node inverse-CDF table applied in the renormalisation's scale
+    pass) for every surface in one call, then the linear velocity potential at
+    z = 0 on every slice of every surface (infinite depth), batched by slice
+    shape.  Returns points/s and the per-stage device milliseconds of one
+    step."""
     import torch
     order = sorted(range(len(batch)), key=lambda k: batch[k]["acf0"])
     total = points(batch)
     flat = torch.empty(total, dtype=torch.float32, device="cuda")
     vel = torch.empty(total, dtype=torch.float32, device="cuda")
-    surfs, groups, nit_ranges, off = [], {}, {}, 0
+    surfs, groups, off = [], {}, 0
     for k in order:
         s = batch[k]
         n = int(np.prod(s["shape"]))
         surfs.append(capi.make_surface(s["shape"], s["phi"], s["var"], s["acf0"],
                                        sets[s["mtset"] % len(sets)], s["seed"],
                                        flat[off:].data_ptr()))
-        lo, hi = nit_ranges.get(s["acf0"], (off, off))
-        nit_ranges[s["acf0"]] = (min(lo, off), off + n)
         nt, nx, ny = s["shape"]
         groups.setdefault((nx, ny), []).append(
             (flat[off:].data_ptr(), vel[off:].data_ptr(), nt, list(range(nt)), 1.0))
         off += n
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    # the NIT table applied in the renormalisation's scale pass
+    tables = [A.nit_table(A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499], float(np.sqrt(batch[k]["acf0"])),
+                          1024, 5.0) for k in order]
 
     def step(record):
         if record:
             ev[0].record(stream)
-        ctx.batch_generate(surfs, A.FP32C)
+        ctx.batch_generate_nit(surfs, A.FP32C, tables)
         if record:
             ev[1].record(stream)
-        for acf0, (lo, hi) in nit_ranges.items():
-            ctx.nit_apply(A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499], float(np.sqrt(acf0)), A.NIT_LUT,
-                          hi - lo, A.FP32C, flat[lo:].data_ptr(), lut_nodes=1024, lut_range=5.0)
-        if record:
-            ev[2].record(stream)
         for (nx, ny), jobs in groups.items():
             ctx.velocity_linear_batch(jobs, nx, ny, A.FP32C, float("inf"), [0.0])
         if record:
-            ev[3].record(stream)
+            ev[2].record(stream)
 
     step(False)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    stage = np.zeros(3)
+    stage = np.zeros(2)
     for _ in range(steps):
         step(True)
         torch.cuda.synchronize()
-        stage += [ev[i].elapsed_time(ev[i + 1]) for i in range(3)]
+        stage += [ev[i].elapsed_time(ev[i + 1]) for i in range(2)]
     wall = time.perf_counter() - t0
     dev_ms = float(stage.sum()) / steps
     return {"value": total / (dev_ms / 1e3), "unit": "points/s", "steps": steps,
             "ms_per_step": dev_ms, "wall_ms_per_step": wall / steps * 1e3,
-            "stage_ms": {"noise_ar_renorm": stage[0] / steps, "nit_lut": stage[1] / steps,
-                         "velocity_z0": stage[2] / steps},
+            "stage_ms": {"noise_ar_renorm_nit": stage[0] / steps,
+                         "velocity_z0": stage[1] / steps},
             "workload": "batched-256-surfaces + skew-normal NIT (LUT 1024 nodes) + velocity "
                         "potential at z=0 on every slice (infinite depth)"}
 

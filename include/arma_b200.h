@@ -266,6 +266,28 @@ int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n,
 int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n,
                              int precision);
 
+/* The NIT of one batch surface: the inverse-CDF table of arma_nit_apply's
+ * ARMA_NIT_LUT method (lut_nodes nodes over [-lut_range, lut_range] * stdev,
+ * built in FP64). */
+typedef struct {
+	int dist;          /* ARMA_NIT_GRAM_CHARLIER or ARMA_NIT_SKEW_NORMAL; < 0: none */
+	double params[3];  /* as arma_nit_apply */
+	double stdev;      /* of the Gaussian input (sqrt(acf0) in the reference) */
+	int lut_nodes;
+	double lut_range;
+} arma_nit_table;
+/* arma_batch_generate followed by the NIT of each surface whose nit[k].dist
+ * is >= 0, as Basic_ARMA_model::generate runs them (the variance
+ * renormalisation, then NIT_transform::transform_realisation;
+ * src/generator/basic_arma_model.cc:102-110, src/nonlinear/nit_transform.cc:
+ * 127-168): the table is applied in the renormalisation's scale pass, one read
+ * and one write per value, and the result equals arma_batch_generate followed
+ * by arma_nit_apply(ARMA_NIT_LUT) bit for bit.  A surface with NIT needs
+ * acf0 > 0 (the reference renormalises before the transform).  Tables are
+ * built once per distinct specification and kept by the context. */
+int arma_batch_generate_nit(arma_ctx* ctx, arma_surface* surfaces, int n,
+                            int precision, const arma_nit_table* nit);
+
 /* ------------------------------------------------ A3': Choi solver */
 /* Yule_walker_solver::solve (src/yule_walker.cc:426-539) as called by
  * AR_model::determine_coefficients_choi (src/generator/ar_model.cc:136-152):

@@ -291,6 +291,39 @@ def test_short_noise_regeneration_is_exact(ctx):
         ctx.set_noise_margin(0.0)
 
 
+@pytest.mark.parametrize("prec,dt", [(A.FP32C, "float32"), (A.FP64, "float64")])
+def test_batch_nit_fused_equals_separate_passes(ctx, prec, dt):
+    """The NIT table applied in the renormalisation's scale pass
+    (arma_batch_generate_nit) equals the batch call followed by the
+    standalone table NIT, bit for bit; a surface without NIT is untouched."""
+    p = A.mt19937_params()
+    shapes = [(20, 33, 50), (16, 64, 32), (12, 40, 40), (9, 17, 31), (10, 32, 32)]
+    fits = [A.ar_fit_analytic(A.ACF_STANDING, (3, 3, 2 + k % 2), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+            for k in range(len(shapes))]
+    specs = [(A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499]), (A.NIT_GRAM_CHARLIER, [0.3, 3.2, 0.0]),
+             None, (A.NIT_SKEW_NORMAL, [0.0, 1.0, 1.499]), (A.NIT_GRAM_CHARLIER, [0.3, 3.2, 0.0])]
+    tdt = getattr(torch, dt)
+
+    def surfaces(bufs):
+        return [capi.make_surface(sh, f[0], f[1], 1.5, p, 60 + k, b.data_ptr())
+                for k, (sh, f, b) in enumerate(zip(shapes, fits, bufs))]
+
+    fused = [torch.empty(sh, dtype=tdt, device="cuda") for sh in shapes]
+    tables = [capi.nit_table(sp[0], sp[1], np.sqrt(1.5), 1024, 5.0) if sp else capi.nit_table()
+              for sp in specs]
+    sc1 = ctx.batch_generate_nit(surfaces(fused), prec, tables)
+    sep = [torch.empty(sh, dtype=tdt, device="cuda") for sh in shapes]
+    sc2 = ctx.batch_generate(surfaces(sep), prec)
+    for sp, b in zip(specs, sep):
+        if sp:
+            ctx.nit_apply(sp[0], sp[1], float(np.sqrt(1.5)), A.NIT_LUT, b.numel(), prec, b.data_ptr(),
+                          lut_nodes=1024, lut_range=5.0)
+    ctx.synchronize()
+    assert sc1 == sc2
+    for a, b in zip(fused, sep):
+        assert torch.equal(a, b)
+
+
 def test_errors_are_reported(ctx):
     with pytest.raises(capi.ArmaError):
         ctx.ar_filter(np.zeros((2, 2, 2)), (0, 4, 4), A.FP64, 0)
