@@ -472,7 +472,14 @@ __device__ __forceinline__ int rotate_src(int i, int n) {
 
 __device__ double window_raw(int i, int j, double dkx, double dky, double z, double h) {
 	const double u = dkx * i, v = dky * j;
-	const double l = k2Pi * sqrt(u * u + v * v);
+	const double s2 = u * u + v * v;
+	if (z == 0.0 && h == INFINITY && s2 > 0.0 && s2 <= DBL_MAX) {
+		// l = 2 pi sqrt(s2) is finite and positive: -l z = -0 (exp = 1) and
+		// -2 l h = -inf (exp = 0), so the formula below gives 4 pi 1 / 1
+		// without the square root
+		return k2Pi * 2.0 * 1.0 / 1.0;
+	}
+	const double l = k2Pi * sqrt(s2);
 	// the exponentials' exact values where the argument is exactly 0 (z = 0)
 	// or -inf (infinite depth) skip the FP64 exp; l = 0 at infinite depth
 	// still gives exp(NaN) = NaN, as in the reference
