@@ -361,10 +361,20 @@ __device__ __forceinline__ void fw_batch(SegWalk& st, T& z1, T& z0, const T* zn,
 
 // Pieces per line: enough (line blocks of 32) x pieces for two units per
 // warp of the CTA, at least 8 positions each.
-__host__ __device__ inline int fw_pieces(int outer, int npos) {
+__host__ __device__ inline int fw_pieces(int outer, int npos, int nwarps) {
 	const int blocks = (outer + 31) / 32;
-	const int want = (2 * (kFwThreads / 32) + blocks - 1) / blocks;
+	const int want = (2 * nwarps + blocks - 1) / blocks;
 	return npos < 16 ? 1 : (want < npos / 8 ? want : npos / 8);
+}
+
+// Warps per CTA for slices of nx x ny: up to kFwThreads / 32, no more than
+// the larger axis has work units (line blocks of 32 x pieces of >= 8
+// positions), so that small slices do not hold idle warps and their tiles.
+inline int fw_warps(int nx, int ny) {
+	auto units = [](int outer, int npos) {
+		return ((outer + 31) / 32) * (npos < 16 ? 1 : npos / 8);
+	};
+	return std::max(1, std::min(kFwThreads / 32, std::max(units(ny, nx - 2), units(nx, ny - 2))));
 }
 
 // One CTA per (slice, axis).  axis 0 loops y outer, x inner over z(x,y): lane
@@ -385,7 +395,7 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 	const int t = int(dt * S.d);  // factor_waves(slice, int t, dt): the truncated coordinate
 	const int outer = axis == 0 ? ny : nx;
 	const int npos = (axis == 0 ? nx : ny) - 2;  // positions 1 .. npos of each line
-	const int P = fw_pieces(outer, npos), per = (npos + P - 1) / P;
+	const int P = fw_pieces(outer, npos, nwarps), per = (npos + P - 1) / P;
 	const int nseg = outer * P, blocks = (outer + 31) / 32;
 	const int nstore = max(nseg, nwarps);  // segments, then the warps' results
 	const SegStore seg(fw_smem, nstore);
@@ -1491,12 +1501,13 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	                              cudaMemcpyHostToDevice, c->stream));
 	ARMA_CUDA_TRY(copy_async(c, d_z, z, sizeof(double) * nz, cudaMemcpyHostToDevice, c->stream));
 	{
-		const int nseg = std::max(nx * fw_pieces(nx, ny - 2), ny * fw_pieces(ny, nx - 2));
-		const size_t fw_smem = seg_region_bytes(std::max(nseg, kFwThreads / 32)) +
-		                       sizeof(T) * (kFwThreads / 32) * 32 * kFwTile;
+		const int fwarps = fw_warps(nx, ny);
+		const int nseg = std::max(nx * fw_pieces(nx, ny - 2, fwarps), ny * fw_pieces(ny, nx - 2, fwarps));
+		const size_t fw_smem = seg_region_bytes(std::max(nseg, fwarps)) +
+		                       sizeof(T) * size_t(fwarps) * 32 * kFwTile;
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(factor_waves_kernel<T>,
 		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(fw_smem)));
-		factor_waves_kernel<T><<<2 * ns, kFwThreads, fw_smem, c->stream>>>(d_sl, nx, ny, d_k);
+		factor_waves_kernel<T><<<2 * ns, 32 * fwarps, fw_smem, c->stream>>>(d_sl, nx, ny, d_k);
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
