@@ -47,7 +47,7 @@ EXPORTS = (
     "arma_poly_roots", "arma_ar_fit_choi", "arma_driver_acf", "arma_velocity_high_amplitude",
     "arma_ma_fit", "arma_ma_filter", "arma_ma_generate", "arma_ctx_set_noise_margin",
     "arma_mt_create", "arma_mt_is_primitive", "arma_mt_equidistribution",
-    "arma_batch_generate_nit",
+    "arma_batch_generate_nit", "arma_ctx_get_tuning", "arma_ctx_set_tuning", "arma_autotune",
 )
 
 
@@ -81,6 +81,18 @@ class Surface(C.Structure):
         ("acf0", C.c_double), ("mt", MtParams), ("seed", C.c_uint32),
         ("d_zeta", C.c_void_p), ("scale", C.c_double),
     ]
+
+
+class Tuning(C.Structure):
+    """``arma_tuning``: result-invariant speed settings of the batched calls."""
+
+    _fields_ = [
+        ("mt_log2_segment", C.c_int), ("ar_ctas_per_sm", C.c_int),
+        ("host_groups", C.c_int), ("host_first", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class NitTable(C.Structure):
@@ -200,6 +212,9 @@ def lib():
             "arma_batch_generate": (i, [vp, C.POINTER(Surface), i, i]),
             "arma_batch_generate_host": (i, [vp, C.POINTER(Surface), i, i]),
             "arma_batch_generate_nit": (i, [vp, C.POINTER(Surface), i, i, C.POINTER(NitTable)]),
+            "arma_ctx_get_tuning": (i, [vp, C.POINTER(Tuning)]),
+            "arma_ctx_set_tuning": (i, [vp, C.POINTER(Tuning)]),
+            "arma_autotune": (i, [vp, C.POINTER(Surface), i, i, i, C.POINTER(Tuning), dp]),
             "arma_ar_filter_fp32c_noalloc": (i, [vp, dp, ip, ip, vp]),
             "arma_driver_open": (i, [C.c_char_p, i, C.POINTER(vp)]),
             "arma_driver_close": (i, [vp]),
@@ -517,6 +532,23 @@ class Context:
         for k, s in enumerate(surfaces):
             s.scale = arr[k].scale
         return [arr[k].scale for k in range(len(surfaces))]
+
+    def tuning(self) -> "Tuning":
+        t = Tuning()
+        _check(lib().arma_ctx_get_tuning(self._h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t: "Tuning") -> None:
+        _check(lib().arma_ctx_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, surfaces, precision: int, host: bool = False):
+        """``arma_autotune``: (chosen Tuning, ms per call or -1 when cached)."""
+        arr = (Surface * len(surfaces))(*surfaces)
+        t = Tuning()
+        ms = C.c_double()
+        _check(lib().arma_autotune(self._h, arr, len(surfaces), precision, int(host), C.byref(t),
+                                   C.byref(ms)))
+        return t, ms.value
 
     def batch_generate_nit(self, surfaces, precision: int, tables):
         """``arma_batch_generate_nit``: tables[k] from :func:`nit_table`."""

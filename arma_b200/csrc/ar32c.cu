@@ -597,6 +597,7 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 	ARMA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ar32c_kernel, NTHREADS,
 	                                                            smem));
 	ARMA_REQUIRE(per_sm > 0, ARMA_EINVAL, "AR tile does not fit in shared memory");
+	if (c->tuning.ar_ctas_per_sm > 0) per_sm = std::min(per_sm, c->tuning.ar_ctas_per_sm);
 	const int grid = std::min(total, per_sm * c->num_sms);
 	ProfScope prof_(c, "ar32c");
 	ar32c_kernel<<<grid, NTHREADS, smem, c->stream>>>(d_tasks, int(tasks.size()), total, d_ticket,

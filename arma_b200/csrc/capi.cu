@@ -1,6 +1,7 @@
 // C ABI: argument checking, error mapping, context and scratch management,
 // and the orchestration of the device kernels.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -93,7 +94,7 @@ long long* white_noise_batch_enqueue(Ctx* c, const arma_surface* s, int n, int p
 		                static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * 4 * att[k]))};
 	}
 	long long* d_pairs = static_cast<long long*>(scratch_take(c, sizeof(long long) * n));
-	launch_mt_generate_batch(c, jobs);
+	launch_mt_generate_batch(c, jobs, c->tuning.mt_log2_segment);
 	std::vector<NoiseSpec> specs(n);
 	for (int k = 0; k < n; ++k) {
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
@@ -363,6 +364,35 @@ int arma_ctx_set_noise_margin(arma_ctx* ctx, double margin) {
 		ARMA_REQUIRE(margin > 0.0 && std::isfinite(margin), ARMA_EINVAL,
 		             "noise margin must be positive");
 		ctx->c.noise_margin = margin;
+	});
+}
+
+namespace {
+void require_tuning(const arma_tuning* t) {
+	ARMA_REQUIRE(t, ARMA_EINVAL, "null tuning");
+	ARMA_REQUIRE(t->mt_log2_segment >= 16 && t->mt_log2_segment <= 22, ARMA_EINVAL,
+	             "mt_log2_segment must be in [16, 22]");
+	ARMA_REQUIRE(t->ar_ctas_per_sm >= 0 && t->ar_ctas_per_sm <= 32, ARMA_EINVAL,
+	             "ar_ctas_per_sm must be in [0, 32]");
+	ARMA_REQUIRE(t->host_groups >= 1 && t->host_groups <= 16, ARMA_EINVAL,
+	             "host_groups must be in [1, 16]");
+	ARMA_REQUIRE(t->host_first > 0.0 && t->host_first < 1.0, ARMA_EINVAL,
+	             "host_first must be in (0, 1)");
+}
+}  // namespace
+
+int arma_ctx_get_tuning(arma_ctx* ctx, arma_tuning* out) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && out, ARMA_EINVAL, "null argument");
+		*out = ctx->c.tuning;
+	});
+}
+
+int arma_ctx_set_tuning(arma_ctx* ctx, const arma_tuning* t) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null context");
+		require_tuning(t);
+		ctx->c.tuning = *t;
 	});
 }
 
@@ -909,8 +939,9 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo =
 // keep up and only the last, smallest group's are exposed.
 void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz,
                            const SurfaceLut* luts) {
-	constexpr int G = 4;
-	const double frac[G] = {0.35, 0.30, 0.20, 0.15};
+	const int G = std::min(std::max(c->tuning.host_groups, 1), std::max(n, 1));
+	std::vector<double> frac(G, G > 1 ? (1.0 - c->tuning.host_first) / (G - 1) : 1.0);
+	if (G > 1) frac[0] = c->tuning.host_first;
 	const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
 	std::vector<double> work(n);
 	double total = 0.0;
@@ -924,7 +955,7 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 	for (int k = 0; k < n; ++k) order[k] = k;
 	std::sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
 	std::vector<std::vector<int>> members(G);
-	double assigned[G] = {};
+	std::vector<double> assigned(G, 0.0);
 	for (int k : order) {
 		int best = 0;
 		for (int g = 1; g < G; ++g)
@@ -1090,6 +1121,102 @@ int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n, int p
 		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
 		scratch_begin(&ctx->c, 0);
 		batch(&ctx->c, surfaces, n, precision, true);
+	});
+}
+
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::vector<long long>, arma_tuning> g_tune_cache;
+
+// The batch's shape class: precision, output kind, surface count and the
+// sorted multiset of (log2 slice size, length / 32, log2 order size).
+std::vector<long long> tune_key(const arma_surface* s, int n, int precision, int host) {
+	std::vector<long long> cls;
+	for (int k = 0; k < n; ++k) {
+		const double area = double(s[k].shape[1]) * s[k].shape[2];
+		const double P = double(s[k].order[0]) * s[k].order[1] * s[k].order[2];
+		cls.push_back((long long)(std::lround(std::log2(std::max(area, 1.0)))) * 1000000 +
+		              (long long)(s[k].shape[0] / 32) * 100 +
+		              (long long)std::lround(std::log2(std::max(P, 1.0))));
+	}
+	std::sort(cls.begin(), cls.end());
+	std::vector<long long> key{precision, host, n};
+	key.insert(key.end(), cls.begin(), cls.end());
+	return key;
+}
+}  // namespace
+
+int arma_autotune(arma_ctx* ctx, arma_surface* surfaces, int n, int precision, int host,
+                  arma_tuning* best_out, double* best_ms) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && surfaces && n > 0 && best_out && best_ms, ARMA_EINVAL, "bad argument");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		const std::vector<long long> key = tune_key(surfaces, n, precision, host);
+		{
+			std::lock_guard<std::mutex> lk(g_tune_mutex);
+			auto it = g_tune_cache.find(key);
+			if (it != g_tune_cache.end()) {
+				ctx->c.tuning = it->second;
+				*best_out = it->second;
+				*best_ms = -1.0;
+				return;
+			}
+		}
+		auto call = [&] {
+			scratch_begin(&ctx->c, 0);
+			batch(&ctx->c, surfaces, n, precision, host != 0);
+		};
+		// wall-clock time per call (every call synchronises before it returns),
+		// after one untimed call that builds whatever the setting needs once
+		auto time_of = [&](const arma_tuning& t) {
+			ctx->c.tuning = t;
+			call();
+			double best = 1e300;
+			for (int r = 0; r < 2; ++r) {
+				const auto t0 = std::chrono::steady_clock::now();
+				call();
+				const auto t1 = std::chrono::steady_clock::now();
+				best = std::min(best, std::chrono::duration<double, std::milli>(t1 - t0).count());
+			}
+			return best;
+		};
+		arma_tuning cur = ctx->c.tuning;
+		double cur_ms = time_of(cur);
+		auto consider = [&](arma_tuning t) {
+			const double ms = time_of(t);
+			if (ms < cur_ms) {
+				cur = t;
+				cur_ms = ms;
+			}
+		};
+		for (int v : {18, 19, 21})
+			if (v != cur.mt_log2_segment) {
+				arma_tuning t = cur;
+				t.mt_log2_segment = v;
+				consider(t);
+			}
+		if (precision == ARMA_FP32C) {
+			for (int a : {1, 2}) {
+				arma_tuning t = cur;
+				t.ar_ctas_per_sm = a;
+				consider(t);
+			}
+			if (host && n >= 4) {
+				const std::pair<int, double> splits[] = {{4, 0.10}, {6, 0.06}, {8, 0.05},
+				                                         {12, 0.04}, {16, 0.03}};
+				for (const auto& sp : splits) {
+					arma_tuning t = cur;
+					t.host_groups = sp.first;
+					t.host_first = sp.second;
+					consider(t);
+				}
+			}
+		}
+		ctx->c.tuning = cur;
+		*best_out = cur;
+		*best_ms = cur_ms;
+		std::lock_guard<std::mutex> lk(g_tune_mutex);
+		g_tune_cache[key] = cur;
 	});
 }
 

@@ -52,6 +52,7 @@ struct Ctx {
 	int* d_err = nullptr;            // device error word
 	cudaStream_t copy_stream = nullptr;  // device->host copies overlapped with compute (lazy)
 	double noise_margin = 1.0;           // polar-attempt estimate multiplier of the batched calls
+	arma_tuning tuning{20, 0, 4, 0.35};  // result-invariant speed settings (arma_ctx_set_tuning)
 	uint64_t launches = 0;           // kernel launches issued
 	uint64_t h2d_bytes = 0;          // bytes copied host -> device through copy_async
 	uint64_t d2h_bytes = 0;          // bytes copied device -> host through copy_async

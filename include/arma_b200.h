@@ -88,6 +88,29 @@ int arma_ctx_transfer_bytes(arma_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
 int arma_ctx_set_profiling(arma_ctx* ctx, int enabled);
 int arma_ctx_profile(arma_ctx* ctx, const char* name, double* ms, uint64_t* launches);
 int arma_ctx_profile_reset(arma_ctx* ctx);
+/* Settings of the batched calls that change their speed but never their
+ * results (no counterpart in the reference):
+ *   mt_log2_segment  the dcmt stream of a surface is cut into segments of
+ *                    2^v words generated by one CTA each, v in [16, 22]
+ *                    (default 20); shorter segments give more CTAs and more
+ *                    jump-ahead work;
+ *   ar_ctas_per_sm   CTAs of the persistent FP32 filter launch per SM, 0 =
+ *                    as many as fit (default);
+ *   host_groups      arma_batch_generate_host (FP32) splits the batch into
+ *                    this many groups, 1..16 (default 4), whose device->host
+ *                    copies overlap the next groups' computation;
+ *   host_first       share of the work in the first group, (0, 1) (default
+ *                    0.35); the other groups share the rest equally.
+ * arma_autotune (after the batch calls below) picks them for a batch by
+ * timing. */
+typedef struct {
+	int mt_log2_segment;
+	int ar_ctas_per_sm;
+	int host_groups;
+	double host_first;
+} arma_tuning;
+int arma_ctx_get_tuning(arma_ctx* ctx, arma_tuning* out);
+int arma_ctx_set_tuning(arma_ctx* ctx, const arma_tuning* t);
 /* Multiplier (> 0, default 1) of the polar-attempt estimate (expected count
  * plus 8 sigma) with which the batched generation calls (arma_batch_generate,
  * arma_batch_generate_host, arma_ma_generate) draw each surface's dcmt words.
@@ -265,6 +288,17 @@ int arma_batch_generate(arma_ctx* ctx, arma_surface* surfaces, int n,
  * pointer of doubles); host<->device copies are part of the call. */
 int arma_batch_generate_host(arma_ctx* ctx, arma_surface* surfaces, int n,
                              int precision);
+
+/* Times candidate settings on this batch (arma_batch_generate, or
+ * arma_batch_generate_host with host = 1; the surfaces' buffers are written)
+ * by coordinate descent over the MT segment length, the filter's CTAs per SM
+ * and, for host output, the group split; sets the fastest on the context and
+ * returns it with its time per call.  The choice is cached per batch shape
+ * class (precision, host, surface count and the histogram of slice sizes,
+ * lengths and orders) for the life of the process: a later call on the same
+ * class sets the cached setting without timing. */
+int arma_autotune(arma_ctx* ctx, arma_surface* surfaces, int n, int precision, int host,
+                  arma_tuning* best, double* best_ms);
 
 /* The NIT of one batch surface: the inverse-CDF table of arma_nit_apply's
  * ARMA_NIT_LUT method (lut_nodes nodes over [-lut_range, lut_range] * stdev,

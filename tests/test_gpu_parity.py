@@ -12,6 +12,8 @@ Tolerances (stated per test):
   * renormalisation: 1e-12 relative.
   * NIT bisection: 2e-6 absolute (bisection tolerance 1e-6); NIT LUT: 5e-5.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -21,6 +23,8 @@ import oracle as O
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def assert_noise_close(got, ref):
@@ -322,6 +326,61 @@ def test_batch_nit_fused_equals_separate_passes(ctx, prec, dt):
     assert sc1 == sc2
     for a, b in zip(fused, sep):
         assert torch.equal(a, b)
+
+
+def test_tuning_settings_do_not_change_results(ctx):
+    """The MT segment length, the filter's CTAs per SM and the host-output
+    group split change the speed only: the same batch comes out bit for bit
+    equal under several settings, into device and into host buffers, and the
+    autotuner's choice (cached per shape class) is one of them."""
+    import torch
+    sets = [A.mt_file_read(os.path.join(ROOT, "arma_b200", "data", "mt.dat"), k) for k in range(3)]
+    shapes = [(60, 64, 96), (25, 32, 32), (90, 48, 64), (17, 100, 33), (33, 16, 128), (50, 70, 70)]
+    fits = [A.ar_fit_analytic(A.ACF_STANDING if k % 2 else A.ACF_PROPAGATING, (4 + k % 3,) * 3,
+                              1.5, 0.8, [0.05] * 3, [0.5, 0.5]) for k in range(len(shapes))]
+    base = ctx.tuning()
+
+    def run(t, host):
+        ctx.set_tuning(t)
+        if host:
+            out = [np.zeros(sh, np.float32) for sh in shapes]
+            ptr = [o.ctypes.data for o in out]
+        else:
+            out = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh in shapes]
+            ptr = [o.data_ptr() for o in out]
+        sf = [capi.make_surface(sh, f[0], f[1], 1.5, sets[k % 3], 900 + k, q)
+              for k, (sh, f, q) in enumerate(zip(shapes, fits, ptr))]
+        sc = ctx.batch_generate(sf, A.FP32C, host=host)
+        ctx.synchronize()
+        return [o if host else o.cpu().numpy() for o in out], sc, sf
+
+    try:
+        ref, ref_sc, _ = run(base, False)
+        variants = []
+        for mt, ar, g, f in [(16, 1, 2, 0.5), (18, 2, 6, 0.06), (22, 0, 16, 0.03)]:
+            t = capi.Tuning()
+            t.mt_log2_segment, t.ar_ctas_per_sm, t.host_groups, t.host_first = mt, ar, g, f
+            variants.append(t)
+        for t in variants:
+            for host in (False, True):
+                got, sc, _ = run(t, host)
+                assert sc == ref_sc
+                for a, b in zip(got, ref):
+                    assert np.array_equal(a, b), (t.as_dict(), host)
+        bad = capi.Tuning()
+        bad.mt_log2_segment, bad.ar_ctas_per_sm, bad.host_groups, bad.host_first = 12, 0, 4, 0.3
+        with pytest.raises(capi.ArmaError):
+            ctx.set_tuning(bad)
+        keep, _, sf = run(base, True)  # the surfaces write into `keep`: it must stay alive
+        chosen, ms = ctx.autotune(sf, A.FP32C, host=True)
+        assert ms > 0.0 and 16 <= chosen.mt_log2_segment <= 22
+        again, ms2 = ctx.autotune(sf, A.FP32C, host=True)
+        assert ms2 == -1.0 and again.as_dict() == chosen.as_dict()
+        del keep
+        got, sc, _ = run(chosen, True)
+        assert sc == ref_sc and all(np.array_equal(a, b) for a, b in zip(got, ref))
+    finally:
+        ctx.set_tuning(base)
 
 
 def test_errors_are_reported(ctx):
