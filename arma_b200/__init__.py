@@ -11,7 +11,7 @@ from .capi import (  # noqa: F401
     library_path, nit_table,
     FP64, FP32C, ACF_STANDING, ACF_PROPAGATING,
     NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL, NIT_BISECTION, NIT_LUT,
-    acf_eval, ar_fit, ar_fit_analytic, ar_fit_choi, ma_fit, mt19937_params, mt_create,
+    acf_eval, auto_covariance, ar_fit, ar_fit_analytic, ar_fit_choi, ma_fit, mt19937_params, mt_create,
     mt_equidistribution, mt_file_count, mt_file_read, mt_file_write, mt_is_primitive, poly_roots,
     validate_process,
 )

@@ -34,7 +34,8 @@ EXPORTS = (
     "arma_ctx_transfer_bytes",
     "arma_ctx_set_profiling", "arma_ctx_profile", "arma_ctx_profile_reset",
     "arma_mt_file_count", "arma_mt_file_read", "arma_mt_file_write",
-    "arma_mt19937_params", "arma_mt_genrand", "arma_acf_eval", "arma_ar_fit",
+    "arma_mt19937_params", "arma_mt_genrand", "arma_acf_eval", "arma_auto_covariance",
+    "arma_ar_fit",
     "arma_ar_fit_analytic", "arma_white_noise", "arma_ar_filter",
     "arma_variance_renorm", "arma_nit_apply", "arma_velocity_linear",
     "arma_batch_generate", "arma_batch_generate_host", "arma_ar_filter_fp32c_noalloc",
@@ -202,6 +203,7 @@ def lib():
             "arma_mt_equidistribution": (i, [mp, i, ip]),
             "arma_mt_genrand": (i, [vp, mp, C.c_uint32, C.c_uint64, sz, vp]),
             "arma_acf_eval": (i, [i, d, d, dp, dp, dp, ip, dp]),
+            "arma_auto_covariance": (i, [dp, ip, dp]),
             "arma_ar_fit": (i, [dp, ip, ip, i, dp, dp]),
             "arma_ar_fit_analytic": (i, [i, d, d, dp, dp, dp, ip, dp, dp]),
             "arma_white_noise": (i, [vp, mp, C.c_uint32, d, sz, i, vp]),
@@ -279,6 +281,14 @@ def acf_eval(kind, shape, amplitude, velocity, alpha, beta, delta=(1.0, 1.0, 1.0
     b, bp = _d(beta)
     dl, dlp = _d(delta)
     _check(lib().arma_acf_eval(kind, amplitude, velocity, ap, bp, dlp, _i3(shape), _dp(out)))
+    return out
+
+
+def auto_covariance(w):
+    """Circular auto-covariance of a 3-D FP64 array (arma::auto_covariance)."""
+    w = np.ascontiguousarray(w, np.float64)
+    out = np.empty_like(w)
+    _check(lib().arma_auto_covariance(_dp(w), _i3(w.shape), _dp(out)))
     return out
 
 

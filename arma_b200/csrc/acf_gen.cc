@@ -12,7 +12,8 @@
 // |y|)) and rescaled to the wave's variance; the ACF is the circular
 // auto-covariance IFFT(|FFT(w)|^2) / n^2 truncated to half of each axis, on a
 // grid of length nwaves per axis.  FP64 on the host; the 3-D transforms are
-// direct DFTs along each axis (sides <= 129).
+// mixed-radix FFTs along each axis (any length; a prime factor p costs p
+// operations per value and level).
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -71,10 +72,35 @@ std::vector<double> sample(const EmpiricalAcf& p, const int n[3]) {
 	return w;
 }
 
+// Unnormalised mixed-radix DFT of x[0], x[stride], ... (n values) into
+// out[0..n): decimation in time by the smallest prime factor p of n, each
+// output combined directly from the p sub-transforms (n p operations per
+// level).  tw[j] = exp(sign 2 pi i j / N) for the full length N; `step` = N / n.
+void fft_rec(const std::complex<double>* x, size_t stride, int n, std::complex<double>* out,
+             std::complex<double>* tmp, const std::vector<std::complex<double>>& tw, int step) {
+	if (n == 1) {
+		out[0] = x[0];
+		return;
+	}
+	int p = 2;
+	while (n % p) p = p * p > n ? n : p + 1;
+	const int m = n / p;
+	for (int r = 0; r < p; ++r) fft_rec(x + r * stride, stride * p, m, tmp + r * m, out, tw, step * p);
+	const int big = int(tw.size());
+	for (int k = 0; k < m; ++k)
+		for (int q = 0; q < p; ++q) {
+			const int kk = q * m + k;
+			std::complex<double> acc = tmp[k];
+			for (int r = 1; r < p; ++r)
+				acc += tmp[r * m + k] * tw[(size_t(r) * kk % n) * step % big];
+			out[kk] = acc;
+		}
+}
+
 // Unnormalised DFT along one axis of an n0 x n1 x n2 complex array.
 void dft_axis(std::vector<std::complex<double>>& a, const int n[3], int axis, int sign) {
 	const int len = n[axis];
-	std::vector<std::complex<double>> tw(len), buf(len);
+	std::vector<std::complex<double>> tw(len), in(len), out(len), tmp(len);
 	for (int k = 0; k < len; ++k) tw[k] = std::polar(1.0, sign * k2Pi * k / len);
 	const size_t stride = axis == 0 ? size_t(n[1]) * n[2] : axis == 1 ? size_t(n[2]) : 1;
 	const int o1 = axis == 0 ? n[1] : n[0], o2 = axis == 2 ? n[1] : n[2];
@@ -84,12 +110,9 @@ void dft_axis(std::vector<std::complex<double>>& a, const int n[3], int axis, in
 			if (axis == 0) base = size_t(u) * n[2] + v;
 			else if (axis == 1) base = size_t(u) * n[1] * n[2] + v;
 			else base = (size_t(u) * n[1] + v) * n[2];
-			for (int q = 0; q < len; ++q) {
-				std::complex<double> acc = 0.0;
-				for (int p = 0; p < len; ++p) acc += a[base + p * stride] * tw[(size_t(p) * q) % len];
-				buf[q] = acc;
-			}
-			for (int q = 0; q < len; ++q) a[base + q * stride] = buf[q];
+			for (int q = 0; q < len; ++q) in[q] = a[base + q * stride];
+			fft_rec(in.data(), 1, len, out.data(), tmp.data(), tw, 1);
+			for (int q = 0; q < len; ++q) a[base + q * stride] = out[q];
 		}
 }
 
@@ -130,12 +153,7 @@ std::vector<double> empirical_acf(const EmpiricalAcf& p, int shape[3], double de
 			}
 	const double sc = std::sqrt(v0 / variance(we));
 	for (double& v : we) v *= sc;
-	// circular auto-covariance IFFT(|FFT(w)|^2) / n^2
-	std::vector<std::complex<double>> c(we.begin(), we.end());
-	for (int a = 0; a < 3; ++a) dft_axis(c, n, a, -1);
-	for (auto& v : c) v = std::norm(v);
-	for (int a = 0; a < 3; ++a) dft_axis(c, n, a, +1);
-	const double nn = double(c.size());
+	const std::vector<double> c = auto_covariance(we, n);
 	for (int a = 0; a < 3; ++a) {
 		shape[a] = n[a] / 2;
 		delta[a] = p.nwaves[a] / std::max(shape[a] - 1, 1);  // Grid(shape, nwaves)
@@ -144,9 +162,22 @@ std::vector<double> empirical_acf(const EmpiricalAcf& p, int shape[3], double de
 	for (int i = 0; i < shape[0]; ++i)
 		for (int j = 0; j < shape[1]; ++j)
 			for (int k = 0; k < shape[2]; ++k)
-				acf[(size_t(i) * shape[1] + j) * shape[2] + k] =
-				    c[(size_t(i) * n[1] + j) * n[2] + k].real() / nn / nn;
+				acf[(size_t(i) * shape[1] + j) * shape[2] + k] = c[(size_t(i) * n[1] + j) * n[2] + k];
 	return acf;
+}
+
+// Circular auto-covariance Re IFFT(|FFT(w)|^2) / n / n over the whole array
+// (auto_covariance, src/arma.cc:81-100): element (i,j,k) is
+// sum w(i1,j1,k1) w((i+i1)%n0, (j+j1)%n1, (k+k1)%n2) / n.
+std::vector<double> auto_covariance(const std::vector<double>& w, const int n[3]) {
+	std::vector<std::complex<double>> c(w.begin(), w.end());
+	for (int a = 0; a < 3; ++a) dft_axis(c, n, a, -1);
+	for (auto& v : c) v = std::norm(v);
+	for (int a = 0; a < 3; ++a) dft_axis(c, n, a, +1);
+	const double nn = double(c.size());
+	std::vector<double> out(c.size());
+	for (size_t q = 0; q < c.size(); ++q) out[q] = c[q].real() / nn / nn;
+	return out;
 }
 
 }  // namespace armab

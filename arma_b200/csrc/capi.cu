@@ -548,6 +548,16 @@ int arma_mt_genrand(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed, uint6
 }
 
 // ---------------------------------------------------------------- fit
+int arma_auto_covariance(const double* in, const int shape[3], double* out) {
+	return guard([&] {
+		ARMA_REQUIRE(in && out && shape, ARMA_EINVAL, "null argument");
+		require_shape(shape, "array");
+		const size_t n = size_t(shape[0]) * shape[1] * shape[2];
+		const std::vector<double> r = auto_covariance(std::vector<double>(in, in + n), shape);
+		std::copy(r.begin(), r.end(), out);
+	});
+}
+
 int arma_acf_eval(int kind, double amplitude, double velocity, const double alpha[3],
                   const double beta[2], const double delta[3], const int shape[3],
                   double* acf) {

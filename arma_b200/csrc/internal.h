@@ -309,6 +309,7 @@ struct EmpiricalAcf {
 	int shape[3] = {16, 16, 16};
 };
 std::vector<double> empirical_acf(const EmpiricalAcf& p, int shape[3], double delta[3]);
+std::vector<double> auto_covariance(const std::vector<double>& w, const int n[3]);
 
 // Choi's order-recursive Yule-Walker solver (choi.cc) on a cubic n^3 ACF:
 // 0 with phi (order[0] x order[1] x order[2]) and the solver's variance, 1 bad

@@ -38,6 +38,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "surface points/s: batched FP32 vs plain FP64 AR on 1 B200; p50/p99 latency"
+
+
+def _load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+PEAKS = _load_peaks()
 N_SURFACES = 256
 MT_SETS = 16
 
@@ -349,12 +360,7 @@ def gpu_arm(args):
         del bufs64
 
     # ---- roofline of the dominant kernel (ar32c)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
+    peaks = PEAKS
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s at the max SM clock
     per_launch_flops = flops(batch)  # one ar32c pass over the batch per step
@@ -498,7 +504,31 @@ def full_path(A, capi, ctx, batch, sets, steps, stream):
         stage += [ev[i].elapsed_time(ev[i + 1]) for i in range(2)]
     wall = time.perf_counter() - t0
     dev_ms = float(stage.sum()) / steps
+    # velocity roofline, algorithmic work per slice of N = nx ny points at nz
+    # depths: 5 N log2 N flop per complex FFT (one forward, nz inverse) + 6 N nz
+    # for the window product; N 4 bytes read and nz N 4 bytes written (FP32)
+    nz, vflop, vbytes = 1, 0.0, 0.0
+    for (nx, ny), jobs in groups.items():
+        n = nx * ny
+        nslices = sum(j[2] for j in jobs)
+        vflop += nslices * (5.0 * n * np.log2(n) * (1 + nz) + 6.0 * n * nz)
+        vbytes += nslices * 4.0 * n * (1 + nz)
+    vel_s = stage[1] / steps / 1e3
+    sm_max = float(PEAKS.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    hbm_peak = float(PEAKS.get("hbm_gbs", 6650.0))
+    v_tf = vflop / vel_s / 1e12
+    v_gb = vbytes / vel_s / 1e9
+    vroof = {"flop_per_step": vflop, "bytes_per_step": vbytes,
+             "fp32": {"achieved": v_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                      "frac": v_tf / fp32_peak},
+             "hbm": {"achieved": v_gb, "peak": hbm_peak, "unit": "GB/s", "frac": v_gb / hbm_peak},
+             "binding": "fp32" if v_tf / fp32_peak > v_gb / hbm_peak else "hbm",
+             "note": "all velocity kernels (zeta_t, FFTs, window, factor_waves) over the "
+                     "algorithmic FFT + window work; peaks as the ar32c roofline (FP32 at the "
+                     "max SM clock) and MEASURED_PEAKS.json's copy bandwidth"}
     return {"value": total / (dev_ms / 1e3), "unit": "points/s", "steps": steps,
+            "velocity_roofline": vroof,
             "ms_per_step": dev_ms, "wall_ms_per_step": wall / steps * 1e3,
             "stage_ms": {"noise_ar_renorm_nit": stage[0] / steps,
                          "velocity_z0": stage[1] / steps},

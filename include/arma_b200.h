@@ -152,6 +152,13 @@ int arma_mt_genrand(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed,
                     uint64_t offset, size_t n, uint32_t* d_out);
 
 /* ------------------------------------------------------ A1-A5: model fit */
+/* Circular auto-covariance of an n0 x n1 x n2 FP64 array (row-major, t
+ * slowest): out(i,j,k) = sum w(i1,j1,k1) w((i+i1)%n0,(j+j1)%n1,(k+k1)%n2) / n,
+ * computed as Re IFFT(|FFT(w)|^2) / n / n in FP64 on the host; replaces
+ * arma::auto_covariance (src/arma.cc:81-100), which the wave-group ACF
+ * generator calls (src/generator/acf_generator.cc:147).  in and out may
+ * alias. */
+int arma_auto_covariance(const double* in, const int shape[3], double* out);
 /* Analytic ACF on the non-negative lag grid (src/acf.hh:18-62). */
 int arma_acf_eval(int kind, double amplitude, double velocity,
                   const double alpha[3], const double beta[2],

@@ -1,6 +1,6 @@
 """Regenerate the committed golden fixtures in this directory.
 
-    python tests/golden/make_golden.py [--reference /path/to/arma]
+    python tests/golden/make_golden.py --reference /path/to/arma
 
 Two kinds of fixtures:
 
