@@ -118,6 +118,7 @@ void white_noise_batch(Ctx* c, const arma_surface* s, int n, int precision,
 	ARMA_CUDA_TRY(copy_async(c, pairs.data(), d_pairs, sizeof(long long) * n,
 	                              cudaMemcpyDeviceToHost, c->stream));
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+	check_device_error(c);
 	for (int k = 0; k < n; ++k) {
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
 		if (noise_short(s[k], pairs[k]))  // the sequential generator instead
@@ -253,7 +254,9 @@ void check_device_error(Ctx* c) {
 	ARMA_CUDA_TRY(cudaStreamSynchronize(c->stream));
 	if (h == DEV_TIMEOUT) {
 		ARMA_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
-		throw Error{ARMA_ETIMEDOUT, "a bounded device wait gave up (tile dependency not met)"};
+		throw Error{ARMA_ETIMEDOUT,
+		            "a bounded device wait gave up (a tile dependency or a noise block's "
+		            "predecessor count never arrived)"};
 	}
 	if (h != DEV_OK) {
 		ARMA_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
@@ -779,13 +782,14 @@ int arma_nit_apply(arma_ctx* ctx, int d, const double params[3], double stdev, i
 			double x0, dx;
 			std::vector<double> y;
 			nit_build_lut(d, params, stdev, lut_nodes, lut_range, &x0, &dx, y);
-			std::vector<float> yf(y.begin(), y.end());
-			double* d_lut = static_cast<double*>(
-			    scratch_take(&ctx->c, sizeof(double) * lut_nodes + sizeof(float) * lut_nodes));
-			ARMA_CUDA_TRY(copy_async(&ctx->c, d_lut, y.data(), sizeof(double) * lut_nodes,
-			                              cudaMemcpyHostToDevice, ctx->c.stream));
-			ARMA_CUDA_TRY(copy_async(&ctx->c, d_lut + lut_nodes, yf.data(), sizeof(float) * lut_nodes,
-			                              cudaMemcpyHostToDevice, ctx->c.stream));
+			const std::vector<double> coef = nit_lut_coefficients(y);
+			const std::vector<float> coef_f(coef.begin(), coef.end());
+			const bool fp64 = precision == ARMA_FP64;
+			const size_t bytes = fp64 ? sizeof(double) * coef.size() : sizeof(float) * coef.size();
+			void* d_lut = scratch_take(&ctx->c, bytes);
+			ARMA_CUDA_TRY(copy_async(&ctx->c, d_lut,
+			                         fp64 ? static_cast<const void*>(coef.data()) : coef_f.data(),
+			                         bytes, cudaMemcpyHostToDevice, ctx->c.stream));
 			launch_nit_lut(&ctx->c, d_lut, lut_nodes, x0, dx, n, precision, d_zeta);
 			ARMA_CUDA_TRY(cudaStreamSynchronize(ctx->c.stream));
 		}
@@ -1248,11 +1252,13 @@ const double* nit_table_device(Ctx* c, const arma_nit_table& t, double* x0, doub
 	double bx0, bdx;
 	std::vector<double> y;
 	nit_build_lut(t.dist, t.params, t.stdev, t.lut_nodes, t.lut_range, &bx0, &bdx, y);
-	std::vector<float> yf(y.begin(), y.end());
+	// the FP64 coefficients, then the FP32 ones (4 (nodes + 1) values each)
+	const std::vector<double> coef = nit_lut_coefficients(y);
+	const std::vector<float> coef_f(coef.begin(), coef.end());
 	double* d = nullptr;
-	ARMA_CUDA_TRY(cudaMalloc(&d, (sizeof(double) + sizeof(float)) * t.lut_nodes));
-	ARMA_CUDA_TRY(cudaMemcpy(d, y.data(), sizeof(double) * t.lut_nodes, cudaMemcpyHostToDevice));
-	ARMA_CUDA_TRY(cudaMemcpy(d + t.lut_nodes, yf.data(), sizeof(float) * t.lut_nodes,
+	ARMA_CUDA_TRY(cudaMalloc(&d, (sizeof(double) + sizeof(float)) * coef.size()));
+	ARMA_CUDA_TRY(cudaMemcpy(d, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice));
+	ARMA_CUDA_TRY(cudaMemcpy(d + coef.size(), coef_f.data(), sizeof(float) * coef.size(),
 	                         cudaMemcpyHostToDevice));
 	c->nit_tables.emplace(key, d);
 	return d;
@@ -1273,8 +1279,9 @@ int arma_batch_generate_nit(arma_ctx* ctx, arma_surface* surfaces, int n, int pr
 				             "NIT needs the variance renormalisation (acf0 > 0)");
 				double x0, dx;
 				const double* d = nit_table_device(&ctx->c, nit[k], &x0, &dx);
-				luts[k].p = precision == ARMA_FP64 ? static_cast<const void*>(d)
-				                                   : static_cast<const void*>(d + nit[k].lut_nodes);
+				luts[k].p = precision == ARMA_FP64
+				                ? static_cast<const void*>(d)
+				                : static_cast<const void*>(d + 4 * size_t(nit[k].lut_nodes + 1));
 				luts[k].nodes = nit[k].lut_nodes;
 				luts[k].x0 = x0;
 				luts[k].inv_dx = 1.0 / dx;

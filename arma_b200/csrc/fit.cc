@@ -186,4 +186,37 @@ void nit_build_lut(int dist, const double params[3], double stdev, int nodes,
 	}
 }
 
+std::vector<double> nit_lut_coefficients(const std::vector<double>& y) {
+	const int nodes = int(y.size());
+	std::vector<double> c(4 * size_t(nodes + 1), 0.0);
+	// Lagrange basis on the nodes s = -1, 0, 1, 2 (values y[i-1 .. i+2]) with
+	// s = t + d: basis m is prod_{q != m} (t - e_q) / den_m, e_q = s_q - d.
+	const int sq[4] = {-1, 0, 1, 2};
+	const double den[4] = {-6.0, 2.0, -2.0, 6.0};
+	for (int j = 0; j + 1 < nodes; ++j) {
+		const int i = std::min(std::max(j, 1), nodes - 3);
+		const int d = j - i;
+		double* out = &c[4 * size_t(j)];
+		for (int m = 0; m < 4; ++m) {
+			double e[3];
+			int r = 0;
+			for (int q = 0; q < 4; ++q)
+				if (q != m) e[r++] = double(sq[q] - d);
+			// (t - a)(t - b)(t - c) = t^3 - (a+b+c) t^2 + (ab+bc+ca) t - abc
+			const double w = y[size_t(i - 1 + m)] / den[m];
+			out[0] += -e[0] * e[1] * e[2] * w;
+			out[1] += (e[0] * e[1] + e[1] * e[2] + e[2] * e[0]) * w;
+			out[2] += -(e[0] + e[1] + e[2]) * w;
+			out[3] += w;
+		}
+	}
+	double* lo = &c[4 * size_t(nodes - 1)];
+	lo[0] = y[0];
+	lo[1] = y[1] - y[0];
+	double* hi = &c[4 * size_t(nodes)];
+	hi[0] = y[size_t(nodes - 1)];
+	hi[1] = y[size_t(nodes - 1)] - y[size_t(nodes - 2)];
+	return c;
+}
+
 }  // namespace armab

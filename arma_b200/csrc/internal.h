@@ -73,20 +73,34 @@ struct Ctx {
 };
 
 // The NIT table map shared by the standalone NIT kernel and the fused
-// renormalisation: u = (z - x0) / dx, cubic Lagrange interpolation through
-// nodes i-1 .. i+2 inside, linear extrapolation beyond the end nodes.
+// renormalisation.  With u = (z - x0) / dx the table holds, for each interval
+// u in [j, j + 1) (j = 0 .. nodes-2), the power-basis coefficients in
+// t = u - j of the cubic Lagrange interpolant through nodes i-1 .. i+2
+// (i = clamp(j, 1, nodes-3)), and at j = nodes-1 and j = nodes the linear
+// extrapolations beyond the first and the last node (value and node step).
+// One vector load and three FMAs per value.
+template <class T> struct NitCoef;
+template <> struct NitCoef<float> { using type = float4; };
+template <> struct NitCoef<double> { using type = double4; };
+
 template <class T>
-__device__ __forceinline__ T nit_lut_map(T z, const T* __restrict__ y, int nodes, T x0, T inv_dx) {
+__device__ __forceinline__ T nit_lut_map(T z, const typename NitCoef<T>::type* __restrict__ coef,
+                                         int nodes, T x0, T inv_dx) {
 	const T u = (z - x0) * inv_dx;
-	if (u <= T(0)) return y[0] + (y[1] - y[0]) * u;
-	if (u >= T(nodes - 1)) return y[nodes - 1] + (y[nodes - 1] - y[nodes - 2]) * (u - T(nodes - 1));
-	int i = int(u);
-	i = min(max(i, 1), nodes - 3);
-	const T s = u - T(i);  // in [-1, 2) relative to node i
-	const T y0 = y[i - 1], y1 = y[i], y2 = y[i + 1], y3 = y[i + 2];
-	const T sm1 = s + T(1), s1 = s - T(1), s2 = s - T(2);
-	return -y0 * s * s1 * s2 * T(1.0 / 6.0) + y1 * sm1 * s1 * s2 * T(0.5) -
-	       y2 * sm1 * s * s2 * T(0.5) + y3 * sm1 * s * s1 * T(1.0 / 6.0);
+	int j;
+	T t;
+	if (u <= T(0)) {
+		j = nodes - 1;
+		t = u;
+	} else if (u >= T(nodes - 1)) {
+		j = nodes;
+		t = u - T(nodes - 1);
+	} else {
+		j = min(int(u), nodes - 2);
+		t = u - T(j);
+	}
+	const typename NitCoef<T>::type k = coef[j];
+	return fma(fma(fma(k.w, t, k.z), t, k.y), t, k.x);
 }
 
 // cudaMemcpyAsync that counts the bytes a context moves between host and
@@ -232,7 +246,9 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 void launch_nit_bisection(Ctx* c, int dist, const double params[3], double stdev,
                           double a, double b, double eps, int max_iter,
                           uint64_t n, int precision, void* d_zeta);
-void launch_nit_lut(Ctx* c, const double* d_lut_y, int nodes, double x0,
+// d_coef: the table of nit_lut_coefficients in the call's precision
+// (4 (nodes + 1) values).
+void launch_nit_lut(Ctx* c, const void* d_coef, int nodes, double x0,
                     double dx, uint64_t n, int precision, void* d_zeta);
 
 // Velocity.
@@ -295,6 +311,10 @@ const double* driver_velocity_data(const Driver* d);
 // Inverse-CDF table for the NIT LUT path.
 void nit_build_lut(int dist, const double params[3], double stdev, int nodes,
                    double range, double* x0, double* dx, std::vector<double>& y);
+// The device form of a table of y.size() >= 4 nodes: 4 (nodes + 1) values,
+// the per-interval cubic coefficients and the two end extrapolations that
+// nit_lut_map reads.
+std::vector<double> nit_lut_coefficients(const std::vector<double>& y);
 
 // The empirical ACF of a plain-wave group (acf_gen.cc): func 0 sin, 1 cos,
 // 2 stokes, 3 standing wave; wavenum = (kx, ky); shape = ACF shape (a zero

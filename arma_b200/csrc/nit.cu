@@ -10,8 +10,9 @@
 //              the bracket is no wider than eps or |f(c)| <= eps.  FP64.
 //   LUT        a pointwise map through an FP64-built inverse-CDF table with
 //              cubic Lagrange interpolation between nodes and linear
-//              extrapolation beyond the end nodes.  HBM-bound: one read and
-//              one write per value.
+//              extrapolation beyond the end nodes, stored per interval as
+//              power-basis coefficients (one vector load and three FMAs per
+//              value).  HBM-bound: one read and one write per value.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -51,20 +52,28 @@ nit_bisection_kernel(T* __restrict__ z, unsigned long long n, int d, double p0, 
 
 // The table map over n values: groups of kLutPer 16-byte vectors per thread,
 // all loaded before any is mapped (the loads in flight together); the ragged
-// head and tail before / after the vectors scalar.
+// head and tail before / after the vectors scalar.  The coefficient table is
+// staged in shared memory when it fits (smem = true), else read through L1.
 template <class T> struct LutVec;
 template <> struct LutVec<float> { using type = float4; static constexpr int n = 4; };
 template <> struct LutVec<double> { using type = double2; static constexpr int n = 2; };
 constexpr int kLutPer = 4;
+constexpr size_t kLutSmemMax = 48 * 1024;
 
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-nit_lut_kernel(T* __restrict__ z, unsigned long long n, const T* __restrict__ lut, int nodes,
-               T x0, T inv_dx) {
-	extern __shared__ unsigned char smem_raw[];
-	T* y = reinterpret_cast<T*>(smem_raw);
-	for (int i = threadIdx.x; i < nodes; i += kThreads) y[i] = lut[i];
-	__syncthreads();
+nit_lut_kernel(T* __restrict__ z, unsigned long long n,
+               const typename NitCoef<T>::type* __restrict__ table, int nodes, T x0, T inv_dx,
+               int smem) {
+	using C = typename NitCoef<T>::type;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const C* coef = table;
+	if (smem) {
+		C* s = reinterpret_cast<C*>(smem_raw);
+		for (int i = threadIdx.x; i <= nodes; i += kThreads) s[i] = table[i];
+		__syncthreads();
+		coef = s;
+	}
 	using V = typename LutVec<T>::type;
 	constexpr int W = LutVec<T>::n;
 	// head: values before the first 16-byte boundary
@@ -72,7 +81,7 @@ nit_lut_kernel(T* __restrict__ z, unsigned long long n, const T* __restrict__ lu
 	    min(n, (unsigned long long)((16 - (reinterpret_cast<uintptr_t>(z) & 15)) & 15) / sizeof(T));
 	const unsigned long long gtid = blockIdx.x * (unsigned long long)kThreads + threadIdx.x;
 	const unsigned long long nthr = (unsigned long long)gridDim.x * kThreads;
-	if (gtid < head) z[gtid] = nit_lut_map(z[gtid], y, nodes, x0, inv_dx);
+	if (gtid < head) z[gtid] = nit_lut_map(z[gtid], coef, nodes, x0, inv_dx);
 	V* zv = reinterpret_cast<V*>(z + head);
 	const unsigned long long nv = (n - head) / W;
 	for (unsigned long long base = gtid; base < nv; base += nthr * kLutPer) {
@@ -88,13 +97,13 @@ nit_lut_kernel(T* __restrict__ z, unsigned long long n, const T* __restrict__ lu
 			if (i < nv) {
 				T* e = reinterpret_cast<T*>(&v[r]);
 #pragma unroll
-				for (int k = 0; k < W; ++k) e[k] = nit_lut_map(e[k], y, nodes, x0, inv_dx);
+				for (int k = 0; k < W; ++k) e[k] = nit_lut_map(e[k], coef, nodes, x0, inv_dx);
 				zv[i] = v[r];
 			}
 		}
 	}
 	for (unsigned long long i = head + nv * W + gtid; i < n; i += nthr)
-		z[i] = nit_lut_map(z[i], y, nodes, x0, inv_dx);
+		z[i] = nit_lut_map(z[i], coef, nodes, x0, inv_dx);
 }
 
 void upload_gl20(Ctx* c) {
@@ -139,19 +148,23 @@ void launch_nit_bisection(Ctx* c, int d, const double params[3], double stdev, d
 	c->launches += 1;
 }
 
-void launch_nit_lut(Ctx* c, const double* d_lut_y, int nodes, double x0, double dx,
+void launch_nit_lut(Ctx* c, const void* d_coef, int nodes, double x0, double dx,
                     uint64_t n, int precision, void* d_zeta) {
 	ProfScope prof_(c, "nit");
 	ARMA_REQUIRE(nodes >= 4, ARMA_EINVAL, "NIT table needs at least 4 nodes");
 	const int grid = grid_for(n, c->num_sms);
 	if (precision == ARMA_FP64) {
-		nit_lut_kernel<double><<<grid, kThreads, sizeof(double) * nodes, c->stream>>>(
-		    static_cast<double*>(d_zeta), n, d_lut_y, nodes, x0, 1.0 / dx);
+		const size_t bytes = sizeof(double4) * (size_t(nodes) + 1);
+		const bool smem = bytes <= kLutSmemMax;
+		nit_lut_kernel<double><<<grid, kThreads, smem ? bytes : 0, c->stream>>>(
+		    static_cast<double*>(d_zeta), n, static_cast<const double4*>(d_coef), nodes, x0,
+		    1.0 / dx, smem);
 	} else {
-		// the float table follows the double one in the same scratch block
-		const float* lf = reinterpret_cast<const float*>(d_lut_y + nodes);
-		nit_lut_kernel<float><<<grid, kThreads, sizeof(float) * nodes, c->stream>>>(
-		    static_cast<float*>(d_zeta), n, lf, nodes, float(x0), float(1.0 / dx));
+		const size_t bytes = sizeof(float4) * (size_t(nodes) + 1);
+		const bool smem = bytes <= kLutSmemMax;
+		nit_lut_kernel<float><<<grid, kThreads, smem ? bytes : 0, c->stream>>>(
+		    static_cast<float*>(d_zeta), n, static_cast<const float4*>(d_coef), nodes,
+		    float(x0), float(1.0 / dx), smem);
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;

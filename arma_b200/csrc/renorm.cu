@@ -8,6 +8,8 @@
 // unbiased variance is computed here in FP64 by a deterministic two-pass
 // reduction (mean, then sum of squared deviations), and the scale stays on
 // the device so the multiply needs no host round trip.
+#include <algorithm>
+
 #include "internal.h"
 
 namespace armab {
@@ -114,7 +116,7 @@ struct RenormJob {
 	unsigned long long off, cnt, n;
 	double acf0;
 	double* scale;
-	const void* lut;  // NIT table after the scale, or null
+	const void* lut;  // NIT coefficient table (nit_lut_coefficients) after the scale, or null
 	int lut_nodes;
 	int vec;          // z is 16-byte aligned: 16-byte accesses
 	double lut_x0, lut_inv_dx;
@@ -130,14 +132,26 @@ partial_batch_kernel(const RenormJob* __restrict__ jobs, const double* __restric
 	const T* x = static_cast<const T*>(jb.z) + jb.off;
 	const double m = means ? means[s] : 0.0;
 	double acc = 0.0;
-	for (unsigned long long i = (unsigned long long)b * kThreads + threadIdx.x; i < jb.cnt;
-	     i += (unsigned long long)kBatchBlocks * kThreads) {
-		const double v = double(x[i]);
-		if (means) {
-			const double d = v - m;
-			acc = fma(d, d, acc);
-		} else {
-			acc += v;
+	// the thread's values in index order, kUnroll loads in flight at a time
+	constexpr int kUnroll = 8;
+	const unsigned long long stride = (unsigned long long)kBatchBlocks * kThreads;
+	for (unsigned long long i0 = (unsigned long long)b * kThreads + threadIdx.x; i0 < jb.cnt;
+	     i0 += stride * kUnroll) {
+		T v[kUnroll];
+#pragma unroll
+		for (int r = 0; r < kUnroll; ++r) {
+			const unsigned long long i = i0 + r * stride;
+			v[r] = i < jb.cnt ? x[i] : T(0);
+		}
+#pragma unroll
+		for (int r = 0; r < kUnroll; ++r) {
+			if (i0 + r * stride >= jb.cnt) break;
+			if (means) {
+				const double d = double(v[r]) - m;
+				acc = fma(d, d, acc);
+			} else {
+				acc += double(v[r]);
+			}
 		}
 	}
 	for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -162,20 +176,27 @@ __global__ void finish_batch_kernel(const RenormJob* __restrict__ jobs,
 }
 
 // Blocks in proportion to each surface's points (kScaleChunk elements per
-// block), so that the largest surfaces do not trail; block b belongs to the
-// last job whose first block is <= b.
+// block, kLutChunks times that for a surface with a NIT table, whose block
+// first stages the table in shared memory), so that the largest surfaces do
+// not trail; block b belongs to the last job whose first block is <= b.
 constexpr int kScaleChunk = kThreads * 16;
+constexpr int kLutChunks = 16;
+constexpr size_t kLutSmemMax = 48 * 1024;
 
 template <class T> struct Vec16;
 template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
 template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
 
 // zeta *= scale, then (when the job has one) the NIT table: one read and one
-// write per value, 16-byte accesses where the surface is aligned.
+// write per value, 16-byte accesses where the surface is aligned.  lut_smem:
+// the launch's dynamic shared memory holds a job's table (else it is read
+// through L1).
 template <class T>
 __global__ void __launch_bounds__(kThreads)
 scale_batch_kernel(const RenormJob* __restrict__ jobs, const int* __restrict__ first_block,
-                   int njobs) {
+                   int njobs, int lut_smem) {
+	using Coef = typename NitCoef<T>::type;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
 	int lo = 0, hi = njobs - 1;
 	while (lo < hi) {
 		const int mid = (lo + hi + 1) / 2;
@@ -184,42 +205,54 @@ scale_batch_kernel(const RenormJob* __restrict__ jobs, const int* __restrict__ f
 	const RenormJob& jb = jobs[lo];
 	T* x = static_cast<T*>(jb.z);
 	const double sc = *jb.scale;
-	const T* lut = static_cast<const T*>(jb.lut);
+	const Coef* lut = static_cast<const Coef*>(jb.lut);
 	const int nodes = jb.lut_nodes;
 	const T x0 = T(jb.lut_x0), inv_dx = T(jb.lut_inv_dx);
+	if (lut && lut_smem) {
+		Coef* st = reinterpret_cast<Coef*>(smem_raw);
+		for (int i = threadIdx.x; i <= nodes; i += kThreads) st[i] = lut[i];
+		__syncthreads();
+		lut = st;
+	}
 	auto map = [&](T v) {
 		v = T(double(v) * sc);
 		return lut ? nit_lut_map(v, lut, nodes, x0, inv_dx) : v;
 	};
-	const unsigned long long i0 = (unsigned long long)(blockIdx.x - first_block[lo]) * kScaleChunk;
-	const unsigned long long i1 = min(jb.n, i0 + kScaleChunk);
-	if (jb.vec) {
-		// every thread's kPer vectors of the chunk are loaded before any is
-		// mapped, so that they are all in flight at once
-		using V = typename Vec16<T>::type;
-		constexpr int W = Vec16<T>::n;
-		constexpr int kPer = kScaleChunk / (W * kThreads);
-		const unsigned long long nv = (i1 - i0) / W;  // i0 is a multiple of kScaleChunk
-		V* xv = reinterpret_cast<V*>(x + i0);
-		V v[kPer];
+	const int chunks = lut ? kLutChunks : 1;
+	for (int ch = 0; ch < chunks; ++ch) {
+		const unsigned long long i0 =
+		    ((unsigned long long)(blockIdx.x - first_block[lo]) * chunks + ch) * kScaleChunk;
+		if (i0 >= jb.n) break;
+		const unsigned long long i1 = min(jb.n, i0 + kScaleChunk);
+		if (jb.vec) {
+			// every thread's kPer vectors of the chunk are loaded before any is
+			// mapped, so that they are all in flight at once
+			using V = typename Vec16<T>::type;
+			constexpr int W = Vec16<T>::n;
+			constexpr int kPer = kScaleChunk / (W * kThreads);
+			const unsigned long long nv = (i1 - i0) / W;  // i0 is a multiple of kScaleChunk
+			V* xv = reinterpret_cast<V*>(x + i0);
+			V v[kPer];
 #pragma unroll
-		for (int r = 0; r < kPer; ++r) {
-			const unsigned long long i = threadIdx.x + (unsigned long long)r * kThreads;
-			if (i < nv) v[r] = xv[i];
-		}
-#pragma unroll
-		for (int r = 0; r < kPer; ++r) {
-			const unsigned long long i = threadIdx.x + (unsigned long long)r * kThreads;
-			if (i < nv) {
-				T* e = reinterpret_cast<T*>(&v[r]);
-#pragma unroll
-				for (int k = 0; k < W; ++k) e[k] = map(e[k]);
-				xv[i] = v[r];
+			for (int r = 0; r < kPer; ++r) {
+				const unsigned long long i = threadIdx.x + (unsigned long long)r * kThreads;
+				if (i < nv) v[r] = xv[i];
 			}
+#pragma unroll
+			for (int r = 0; r < kPer; ++r) {
+				const unsigned long long i = threadIdx.x + (unsigned long long)r * kThreads;
+				if (i < nv) {
+					T* e = reinterpret_cast<T*>(&v[r]);
+#pragma unroll
+					for (int k = 0; k < W; ++k) e[k] = map(e[k]);
+					xv[i] = v[r];
+				}
+			}
+			for (unsigned long long i = i0 + nv * W + threadIdx.x; i < i1; i += kThreads)
+				x[i] = map(x[i]);
+		} else {
+			for (unsigned long long i = i0 + threadIdx.x; i < i1; i += kThreads) x[i] = map(x[i]);
 		}
-		for (unsigned long long i = i0 + nv * W + threadIdx.x; i < i1; i += kThreads) x[i] = map(x[i]);
-	} else {
-		for (unsigned long long i = i0 + threadIdx.x; i < i1; i += kThreads) x[i] = map(x[i]);
 	}
 }
 
@@ -249,11 +282,18 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 	}
 	const int ns = int(jobs.size());
 	std::vector<int> first(ns);
-	int sblocks = 0;
+	int sblocks = 0, max_nodes = 0;
 	for (int k = 0; k < ns; ++k) {
 		first[k] = sblocks;
-		sblocks += int((jobs[k].n + kScaleChunk - 1) / kScaleChunk);
+		const unsigned long long chunk =
+		    (unsigned long long)kScaleChunk * (jobs[k].lut ? kLutChunks : 1);
+		sblocks += int((jobs[k].n + chunk - 1) / chunk);
+		if (jobs[k].lut) max_nodes = std::max(max_nodes, jobs[k].lut_nodes);
 	}
+	// the largest table of the launch in shared memory when it fits
+	const size_t coef_bytes = precision == ARMA_FP64 ? sizeof(double4) : sizeof(float4);
+	size_t lut_smem = max_nodes ? coef_bytes * (size_t(max_nodes) + 1) : 0;
+	if (lut_smem > kLutSmemMax) lut_smem = 0;
 	int* d_first = static_cast<int*>(scratch_take(c, sizeof(int) * ns));
 	ARMA_CUDA_TRY(copy_async(c, d_first, first.data(), sizeof(int) * ns, cudaMemcpyHostToDevice,
 	                              c->stream));
@@ -269,14 +309,16 @@ void launch_renorm_batch(Ctx* c, const std::vector<RenormSpec>& specs, int preci
 		partial_batch_kernel<double><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
 		if (apply)
-			scale_batch_kernel<double><<<sblocks, kThreads, 0, c->stream>>>(d_jobs, d_first, ns);
+			scale_batch_kernel<double><<<sblocks, kThreads, lut_smem, c->stream>>>(d_jobs, d_first,
+			                                                                        ns, lut_smem > 0);
 	} else {
 		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, nullptr, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 0, means);
 		partial_batch_kernel<float><<<g, kThreads, 0, c->stream>>>(d_jobs, means, partial);
 		finish_batch_kernel<<<ns, 32, 0, c->stream>>>(d_jobs, partial, 1, means);
 		if (apply)
-			scale_batch_kernel<float><<<sblocks, kThreads, 0, c->stream>>>(d_jobs, d_first, ns);
+			scale_batch_kernel<float><<<sblocks, kThreads, lut_smem, c->stream>>>(d_jobs, d_first, ns,
+			                                                                       lut_smem > 0);
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += apply ? 5 : 4;

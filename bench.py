@@ -781,8 +781,14 @@ def run_stage(args):
     elif args.stage == "full":
         batch = fit_batch(make_batch(0)[:args.surfaces or N_SURFACES])
         r = full_path(A, capi, ctx, batch, mt_sets(), 2, stream)
+        ctx.set_profiling(True)
+        ctx.profile_reset()
+        full_path(A, capi, ctx, batch, mt_sets(), 1, stream)
+        kern = {k: round(ctx.profile(k)[0] / 2, 3) for k in ("mt", "noise", "ar32c", "renorm")}
+        ctx.set_profiling(False)
         print(f"full {len(batch)} surfaces ({points(batch)} points): {r['ms_per_step']:.2f} ms/step "
-              f"{json.dumps(r['stage_ms'])}")
+              f"{json.dumps(r['stage_ms'])} kernels (ms per step, profiled) {json.dumps(kern)} "
+              f"velocity roofline {json.dumps(r['velocity_roofline'])}")
     elif args.stage == "nit":
         z = torch.randn(shape, dtype=torch.float32, device="cuda")
         method = A.NIT_BISECTION if args.bisection else A.NIT_LUT
