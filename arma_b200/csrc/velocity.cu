@@ -181,27 +181,37 @@ __device__ __forceinline__ double k_of(double d) {
 	return w * w / kG;
 }
 
-// One event of a thread's own segment, in loop order.
-__device__ __forceinline__ void seg_event(SegWalk& st, double e, double p) {
+// The next position of a thread's own segment, in loop order, when `ev` (it
+// is an extremum) with elevation e and period p: the first event opens run 0;
+// an event of the open run's sign replaces its representative only when its
+// |elevation| is larger (the first maximum stays); an event of the other sign
+// closes the open run (run 0 and run 1 keep their representatives for a later
+// join, every later run adds its pair with the run before) and opens the next.
+// Written as selects rather than branches, so that the lanes of a warp, each
+// walking its own line, do not diverge on the event's kind.
+__device__ __forceinline__ void seg_event_if(SegWalk& st, bool ev, double e, double p) {
 	const int s = e > 0.0 ? 1 : 0;
 	const double ae = fabs(e);
-	if (st.m == 0) {
-		st.open = Run{s, ae, p};
-		st.m = 1;
-	} else if (s == st.open.sign) {
-		if (st.open.best_e < ae) {  // the first maximum stays
-			st.open.best_e = ae;
-			st.open.best_p = p;
-		}
-	} else {
-		const int r = st.m - 1;  // the open run closes
-		if (r == 0) st.r0 = st.open;
-		else if (r == 1) st.r1_p = st.open.best_p;
-		else pair_k(st.prev_p, st.open.best_p, st.dmin, st.dmax);
-		st.prev_p = st.open.best_p;
-		st.open = Run{s, ae, p};
-		++st.m;
-	}
+	const bool first = ev && st.m == 0;
+	const bool same = ev && st.m != 0 && s == st.open.sign;
+	const bool close = ev && st.m != 0 && s != st.open.sign;
+	const bool better = same && st.open.best_e < ae;
+	const int r = st.m - 1;
+	const bool c0 = close && r == 0, c1 = close && r == 1, pk = close && r >= 2;
+	st.r0.sign = c0 ? st.open.sign : st.r0.sign;
+	st.r0.best_e = c0 ? st.open.best_e : st.r0.best_e;
+	st.r0.best_p = c0 ? st.open.best_p : st.r0.best_p;
+	st.r1_p = c1 ? st.open.best_p : st.r1_p;
+	// pair_k: comparisons with a NaN difference are false and change nothing
+	const double d = fabs(st.open.best_p - st.prev_p);
+	st.dmin = pk && d < st.dmin ? d : st.dmin;
+	st.dmax = pk && d > st.dmax ? d : st.dmax;
+	st.prev_p = close ? st.open.best_p : st.prev_p;
+	const bool take = first || close || better;
+	st.open.best_e = take ? ae : st.open.best_e;
+	st.open.best_p = take ? p : st.open.best_p;
+	st.open.sign = (first || close) ? s : st.open.sign;
+	st.m += (first || close) ? 1 : 0;
 }
 
 // The summary of segment A followed by segment B.  B's first run continues
@@ -339,23 +349,32 @@ __device__ __forceinline__ void fw_vertex(T z0, T z1, T z2, double dt, int t, do
 }
 
 // n (<= kFwBatch) consecutive positions after (z1, z0), fed to the walk in
-// order; leaves (z1, z0) at the last two values.
+// order; leaves (z1, z0) at the last two values.  The vertices of kFwIlp
+// positions are computed before any is fed to the walk, extremum or not, so
+// that their FP64 chains (a division each) run side by side: a warp takes the
+// vertex path whenever any of its lanes has an extremum, which is nearly
+// always, so computing it for every position costs the warp nothing more.
 constexpr int kFwBatch = 8;
+constexpr int kFwIlp = 4;
 template <class T>
 __device__ __forceinline__ void fw_batch(SegWalk& st, T& z1, T& z0, const T* zn, int n, double dt,
                                          int t) {
 #pragma unroll
-	for (int k = 0; k < kFwBatch; ++k) {
-		if (k < n) {
-			const T z2 = zn[k];
-			if (fw_extremum(z0, z1, z2)) {
-				double e, p;
-				fw_vertex(z0, z1, z2, dt, t, e, p);
-				seg_event(st, e, p);
+	for (int k0 = 0; k0 < kFwBatch; k0 += kFwIlp) {
+		double e[kFwIlp], p[kFwIlp];
+		bool ev[kFwIlp];
+#pragma unroll
+		for (int k = 0; k < kFwIlp; ++k) {
+			const T z2 = k0 + k < n ? zn[k0 + k] : z0;
+			ev[k] = k0 + k < n && fw_extremum(z0, z1, z2);
+			fw_vertex(z0, z1, z2, dt, t, e[k], p[k]);
+			if (k0 + k < n) {
+				z1 = z0;
+				z0 = z2;
 			}
-			z1 = z0;
-			z0 = z2;
 		}
+#pragma unroll
+		for (int k = 0; k < kFwIlp; ++k) seg_event_if(st, ev[k], e[k], p[k]);
 	}
 }
 
