@@ -8,7 +8,8 @@
 // with x[0..n-1] the seeded state (sgenrand_mt), output word w is
 // temper(x[n+w]).  Every word of a chunk [j0, j0+n-m) depends only on words
 // before j0, so one CTA produces n-m words per barrier step with all
-// arithmetic in 32-bit integers.
+// arithmetic in 32-bit integers; sets with nn = 2 mm run one warp per segment
+// with no barrier (mt_generate_half_kernel).
 //
 // Long streams are cut into segments of J = 2^20 words generated by separate
 // CTAs.  The window of nn raw words at the start of segment k is obtained by
@@ -135,6 +136,106 @@ mt_generate_kernel(const SegJob* __restrict__ jobs) {
 			}
 		}
 		__syncthreads();
+	}
+}
+
+// Sets with nn = 2 mm (every committed set of period 2^19937 - 1): with the
+// chunk n - m = m, output word w = m s + t (step s, slot t < m) is
+//     x[n + w] = x[n + w - m] ^ f(x[w], x[w + 1]),
+// where x[n + w - m] is slot t of step s-1, x[w] slot t of step s-2 and
+// x[w + 1] slot t+1 of step s-2 (slot 0 of step s-1 when t = m-1): every
+// word needs only its own slot's last two values and the next slot's.  One
+// warp runs one segment with no barrier: lane l holds slots t = 32 q + l
+// (q < kHalfQ) of the last two steps in registers, takes the next slot's
+// values by shuffles, and stores each q's 32 words coalesced.  The state
+// window (raw words 0 .. n-1) is steps -2 and -1.
+constexpr int kHalfQ = 10;     // slots per lane: mm <= 320
+constexpr int kHalfWarps = 4;  // warps (segments) per CTA
+constexpr int kHalfMaxN = 2 * 32 * kHalfQ;
+
+__host__ __device__ inline bool half_set(const arma_mt_params& p) {
+	return p.nn == 2 * p.mm && p.mm <= 32 * kHalfQ;
+}
+
+// One step of the warp generator: slots of step s from those of steps s-2 (a)
+// and s-1 (b); b0 = slot 0 of step s-1.  M > 0: the compile-time mm (slot
+// checks resolved at compile time); M = 0: mm = m at run time.
+template <int M>
+__device__ __forceinline__ void half_step(const uint32_t* a, const uint32_t* b, uint32_t* nb,
+                                          uint32_t b0, int m, int lane, const arma_mt_params& p) {
+	const int mm = M > 0 ? M : m;
+#pragma unroll
+	for (int q = 0; q < kHalfQ; ++q) {
+		if (M > 0 && 32 * q >= M) break;
+		const int t = 32 * q + lane;
+		const uint32_t down = __shfl_down_sync(0xffffffffu, a[q], 1);
+		const uint32_t wrap = __shfl_sync(0xffffffffu, q + 1 < kHalfQ ? a[q + 1] : 0u, 0);
+		uint32_t a1 = lane < 31 ? down : wrap;
+		if ((M == 0 || 32 * q + 31 >= M - 1) && t == mm - 1) a1 = b0;
+		const uint32_t y = (a[q] & p.umask) | (a1 & p.lmask);
+		nb[q] = b[q] ^ (y >> 1) ^ ((y & 1u) ? p.aaa : 0u);
+	}
+}
+
+template <int M>
+__global__ void __launch_bounds__(32 * kHalfWarps)
+mt_generate_half_kernel(const SegJob* __restrict__ jobs, int njobs) {
+	__shared__ uint32_t seeded[kHalfWarps][kHalfMaxN];
+	const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+	const int g = blockIdx.x * kHalfWarps + wl;
+	if (g >= njobs) return;
+	const SegJob& jb = jobs[g];
+	const arma_mt_params p = jb.p;
+	const int m = M > 0 ? M : p.mm;
+	const uint32_t* st = jb.state;
+	if (!st) {
+		if (lane == 0) seed_state(seeded[wl], jb.seed, p);
+		__syncwarp();
+		st = seeded[wl];
+	}
+	uint32_t a[kHalfQ], b[kHalfQ];  // slots of steps s-2 and s-1
+#pragma unroll
+	for (int q = 0; q < kHalfQ; ++q) {
+		const int t = 32 * q + lane;
+		a[q] = t < m ? st[t] : 0u;
+		b[q] = t < m ? st[m + t] : 0u;
+	}
+	// segment words w < count (<= 2^30) go to out[first - offset + w] when that
+	// index is >= 0: base = out + max(first - offset, 0), index w - wmin
+	const int count = int(jb.count);
+	const long long shift = (long long)jb.first - (long long)jb.offset;
+	const int wmin = shift < 0 ? int(-shift) : 0;
+	uint32_t* const base = jb.out + (shift > 0 ? shift : 0);
+	int w0 = 0;
+	if (wmin == 0) {
+		// whole steps: every slot < m is stored
+		for (; w0 + m <= count; w0 += m) {
+			const uint32_t b0 = __shfl_sync(0xffffffffu, b[0], 0);
+			uint32_t nb[kHalfQ];
+			half_step<M>(a, b, nb, b0, m, lane, p);
+			uint32_t* dst = base + w0 + lane;
+#pragma unroll
+			for (int q = 0; q < kHalfQ; ++q) {
+				if (M > 0 && 32 * q >= M) break;
+				if ((M > 0 && 32 * q + 32 <= M) || 32 * q + lane < m) dst[32 * q] = temper(nb[q], p);
+				a[q] = b[q];
+				b[q] = nb[q];
+			}
+		}
+	}
+	// the rest: skipped words before the offset, the last partial step
+	for (; w0 < count; w0 += m) {
+		const uint32_t b0 = __shfl_sync(0xffffffffu, b[0], 0);
+		uint32_t nb[kHalfQ];
+		half_step<M>(a, b, nb, b0, m, lane, p);
+#pragma unroll
+		for (int q = 0; q < kHalfQ; ++q) {
+			const int t = 32 * q + lane;
+			const int w = w0 + t;
+			if (t < m && w < count && w >= wmin) base[w - wmin] = temper(nb[q], p);
+			a[q] = b[q];
+			b[q] = nb[q];
+		}
 	}
 }
 
@@ -409,22 +510,46 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 			seg.push_back(s);
 		}
 	}
+	// segments of nn = 2 mm sets: one warp each (32-bit word indices); the
+	// rest: one CTA each
+	auto by_warp = [](const SegJob& j) {
+		return half_set(j.p) && j.count < (1ull << 30) && j.offset < (1ull << 30) &&
+		       j.first < (1ull << 40);
+	};
+	std::stable_partition(seg.begin(), seg.end(), by_warp);
+	const int nhalf = int(std::count_if(seg.begin(), seg.end(), by_warp));
 	auto* d_seg = static_cast<SegJob*>(scratch_take(c, sizeof(SegJob) * seg.size()));
 	ARMA_CUDA_TRY(copy_async(c, d_seg, seg.data(), sizeof(SegJob) * seg.size(),
 	                              cudaMemcpyHostToDevice, c->stream));
-	int chunk = 1;  // the largest chunk of the batch
-	for (const MtJob& j : jobs) chunk = std::max(chunk, j.p.nn - j.p.mm);
-	const int threads = std::min(kGenMaxThreads, (chunk + 31) / 32 * 32);
-	const int own = (chunk + threads - 1) / threads;
-	const int grid = int(seg.size());
-	switch (own) {
-		case 1: mt_generate_kernel<1><<<grid, threads, 0, c->stream>>>(d_seg); break;
-		case 2: mt_generate_kernel<2><<<grid, threads, 0, c->stream>>>(d_seg); break;
-		case 3: mt_generate_kernel<3><<<grid, threads, 0, c->stream>>>(d_seg); break;
-		default: mt_generate_kernel<4><<<grid, threads, 0, c->stream>>>(d_seg); break;
+	if (nhalf > 0) {
+		// mm = 312 (the sets of period 2^19937 - 1) compiled in; others at run time
+		bool all312 = true;
+		for (int k = 0; k < nhalf; ++k) all312 = all312 && seg[k].p.mm == 312;
+		const int hgrid = (nhalf + kHalfWarps - 1) / kHalfWarps;
+		if (all312)
+			mt_generate_half_kernel<312><<<hgrid, 32 * kHalfWarps, 0, c->stream>>>(d_seg, nhalf);
+		else
+			mt_generate_half_kernel<0><<<hgrid, 32 * kHalfWarps, 0, c->stream>>>(d_seg, nhalf);
+		ARMA_CUDA_TRY(cudaGetLastError());
+		c->launches += 1;
 	}
-	ARMA_CUDA_TRY(cudaGetLastError());
-	c->launches += 1;
+	const int grid = int(seg.size()) - nhalf;
+	if (grid > 0) {
+		int chunk = 1;  // the largest chunk of the rest
+		for (size_t k = size_t(nhalf); k < seg.size(); ++k)
+			chunk = std::max(chunk, seg[k].p.nn - seg[k].p.mm);
+		const int threads = std::min(kGenMaxThreads, (chunk + 31) / 32 * 32);
+		const int own = (chunk + threads - 1) / threads;
+		const SegJob* rest = d_seg + nhalf;
+		switch (own) {
+			case 1: mt_generate_kernel<1><<<grid, threads, 0, c->stream>>>(rest); break;
+			case 2: mt_generate_kernel<2><<<grid, threads, 0, c->stream>>>(rest); break;
+			case 3: mt_generate_kernel<3><<<grid, threads, 0, c->stream>>>(rest); break;
+			default: mt_generate_kernel<4><<<grid, threads, 0, c->stream>>>(rest); break;
+		}
+		ARMA_CUDA_TRY(cudaGetLastError());
+		c->launches += 1;
+	}
 }
 
 void launch_mt_window_update(Ctx* c, const std::vector<MtWindowSpec>& specs) {
