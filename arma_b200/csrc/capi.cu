@@ -77,31 +77,54 @@ void white_noise(Ctx* c, const arma_mt_params& p, uint32_t seed, double stddev, 
 	throw Error{ARMA_ECUDA, "white noise: rejection sampling did not converge"};
 }
 
-// White noise for many surfaces: all MT streams in one launch (one CTA per
-// stream), the polar transforms enqueued back to back, one host check.
-// Enqueue the white noise of n surfaces (MT words, then the polar method);
-// returns the device array of accepted pairs per surface.
-long long* white_noise_batch_enqueue(Ctx* c, const arma_surface* s, int n, int precision,
-                                     const std::vector<void*>& dz) {
-	std::vector<MtJob> jobs(n);
-	std::vector<uint64_t> att(n);
+// White noise for many surfaces: all MT streams in a few launches, the polar
+// transforms in one.  The plan holds every surface's MT job (its words in
+// scratch); noise_enqueue generates the words and the normal values of the
+// surfaces idx and returns the device array of their accepted pairs (in idx
+// order).
+struct NoisePlan {
+	std::vector<MtJob> jobs;
+	std::vector<uint64_t> att;
+};
+
+NoisePlan noise_plan(Ctx* c, const arma_surface* s, int n) {
+	NoisePlan plan;
+	plan.jobs.resize(n);
+	plan.att.resize(n);
 	for (int k = 0; k < n; ++k) {
 		ARMA_REQUIRE(s[k].var_wn >= 0.0 && std::isfinite(s[k].var_wn), ARMA_EINVAL,
 		             "variance is less than zero");
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
-		att[k] = noise_attempts(np, c->noise_margin);
-		jobs[k] = MtJob{s[k].mt, s[k].seed, 0, 4 * att[k],
-		                static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * 4 * att[k]))};
+		plan.att[k] = noise_attempts(np, c->noise_margin);
+		plan.jobs[k] = MtJob{s[k].mt, s[k].seed, 0, 4 * plan.att[k],
+		                     static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * 4 * plan.att[k]))};
 	}
+	return plan;
+}
+
+long long* noise_enqueue(Ctx* c, const arma_surface* s, const NoisePlan& plan,
+                         const std::vector<int>& idx, int precision, const std::vector<void*>& dz) {
+	const int n = int(idx.size());
 	long long* d_pairs = static_cast<long long*>(scratch_take(c, sizeof(long long) * n));
+	std::vector<MtJob> jobs(n);
+	for (int q = 0; q < n; ++q) jobs[q] = plan.jobs[idx[q]];
 	launch_mt_generate_batch(c, jobs, c->tuning.mt_log2_segment);
 	std::vector<NoiseSpec> specs(n);
-	for (int k = 0; k < n; ++k) {
+	for (int q = 0; q < n; ++q) {
+		const int k = idx[q];
 		const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
-		specs[k] = NoiseSpec{jobs[k].out, 4 * att[k], np, std::sqrt(s[k].var_wn), dz[k]};
+		specs[q] = NoiseSpec{plan.jobs[k].out, 4 * plan.att[k], np, std::sqrt(s[k].var_wn), dz[k]};
 	}
 	enqueue_white_noise_batch(c, specs, precision, d_pairs);
 	return d_pairs;
+}
+
+long long* white_noise_batch_enqueue(Ctx* c, const arma_surface* s, int n, int precision,
+                                     const std::vector<void*>& dz) {
+	const NoisePlan plan = noise_plan(c, s, n);
+	std::vector<int> idx(n);
+	for (int k = 0; k < n; ++k) idx[k] = k;
+	return noise_enqueue(c, s, plan, idx, precision, dz);
 }
 
 // True when surface k's accepted pairs do not cover its points (rare: the
@@ -309,6 +332,10 @@ int arma_ctx_destroy(arma_ctx* ctx) {
 		for (auto& kv : ctx->c.nit_tables) cudaFree(kv.second);
 		for (auto& ch : ctx->chunks) pool_free(&ctx->c, ch.first);
 		cudaStreamSynchronize(ctx->c.stream);
+		if (ctx->c.side_stream) {
+			cudaStreamSynchronize(ctx->c.side_stream);
+			cudaStreamDestroy(ctx->c.side_stream);
+		}
 		if (ctx->c.copy_stream) {
 			cudaStreamSynchronize(ctx->c.copy_stream);
 			cudaStreamDestroy(ctx->c.copy_stream);
@@ -944,13 +971,16 @@ void batch(Ctx* c, arma_surface* s, int n, int precision, bool host, bool redo =
 }
 
 // FP32 surfaces into host buffers with the device->host copies overlapped with
-// the computation.  The batch is split into groups of decreasing work (35, 30,
-// 20, 15 % of the total points x taps); each group's white noise, filter and
-// renormalisation run on the context's stream and its device->host copies on
-// a copy stream, overlapping the next group's computation.  Per % of the bench
-// batch the copies take about 0.76 ms and the computation about 0.9 ms (noise
-// and filter, with the tail of each group's persistent launch), so the copies
-// keep up and only the last, smallest group's are exposed.
+// the computation.  The surfaces are ordered by the length of their filter's
+// dependency chain (slices + tile rows + tile columns) and cut, in that order,
+// into groups holding shares of the total points x taps (a first share, then
+// equal ones), so that each group's persistent filter launch ends without a
+// long tail and the first group, of the shortest chains, is ready early.  The
+// groups' white noise, filter and renormalisation alternate between two
+// compute streams, so that one group's launches fill the SMs that the other's
+// tail leaves idle; each group's device->host copies run on a copy stream as
+// soon as its renormalisation is done.  The copies bound the call: the
+// computation outpaces the PCIe link after the first group.
 void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<void*>& dz,
                            const SurfaceLut* luts) {
 	const int G = std::min(std::max(c->tuning.host_groups, 1), std::max(n, 1));
@@ -964,18 +994,24 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 		          s[k].order[1] * s[k].order[2];
 		total += work[k];
 	}
-	// largest surfaces first, each to the group furthest below its share
+	// shortest dependency chains first, cut into consecutive groups by share
+	auto chain = [&](int k) {
+		return s[k].shape[0] + (s[k].shape[1] + tx - 1) / tx + (s[k].shape[2] + ty - 1) / ty;
+	};
 	std::vector<int> order(n);
 	for (int k = 0; k < n; ++k) order[k] = k;
-	std::sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+	std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+		return chain(a) != chain(b) ? chain(a) < chain(b) : work[a] < work[b];
+	});
 	std::vector<std::vector<int>> members(G);
-	std::vector<double> assigned(G, 0.0);
-	for (int k : order) {
-		int best = 0;
-		for (int g = 1; g < G; ++g)
-			if (frac[g] * total - assigned[g] > frac[best] * total - assigned[best]) best = g;
-		members[best].push_back(k);
-		assigned[best] += work[k];
+	{
+		int g = 0;
+		double bound = frac[0] * total, acc = 0.0;
+		for (int k : order) {
+			while (g + 1 < G && acc >= bound) bound += frac[++g] * total;
+			members[g].push_back(k);
+			acc += work[k];
+		}
 	}
 	// the filter's coefficient tables of every surface (host work, one
 	// upload), built while the device generates the first group's noise
@@ -993,27 +1029,45 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 	// back (a device->host read on the context's stream would queue behind the
 	// previous groups' copies); the counts are checked at the end.
 	std::vector<long long*> d_pairs(G, nullptr);
+	// every surface's MT jump-ahead windows once, in wide launches (per group
+	// they would be narrow, latency-bound trees), before the groups' words
+	NoisePlan plan = noise_plan(c, s, n);
 	auto noise = [&](int g) {
-		std::vector<arma_surface> sub;
-		std::vector<void*> dsub;
-		for (int k : members[g]) {
-			sub.push_back(s[k]);
-			dsub.push_back(dz[k]);
-		}
-		d_pairs[g] = white_noise_batch_enqueue(c, sub.data(), int(sub.size()), ARMA_FP32C, dsub);
+		d_pairs[g] = noise_enqueue(c, s, plan, members[g], ARMA_FP32C, dz);
 	};
 	if (!c->copy_stream)
 		ARMA_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+	if (!c->side_stream)
+		ARMA_CUDA_TRY(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
 	double* d_scale = static_cast<double*>(scratch_take(c, sizeof(double) * n));
 	std::vector<cudaEvent_t> ev;
+	auto event = [&](cudaStream_t st) {
+		cudaEvent_t e;
+		ARMA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+		ev.push_back(e);
+		ARMA_CUDA_TRY(cudaEventRecord(e, st));
+		return e;
+	};
+	const cudaStream_t main_stream = c->stream;
 	auto release = [&] {
+		c->stream = main_stream;
 		for (cudaEvent_t e : ev) cudaEventDestroy(e);
 	};
 	try {
+		launch_mt_prepare(c, plan.jobs, c->tuning.mt_log2_segment);
+		// the side stream starts after the caller's earlier work and the windows
+		ARMA_CUDA_TRY(cudaStreamWaitEvent(c->side_stream, event(main_stream), 0));
 		for (int g = 0; g < G; ++g) {
 			if (members[g].empty()) continue;
+			// the context's launch helpers enqueue on c->stream
+			c->stream = (g % 2 == 0) ? main_stream : c->side_stream;
 			noise(g);
-			if (as.empty()) as = ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
+			if (as.empty()) {
+				as = ar32_surfaces(c, n, phis.data(), ords.data(), shps.data(), zs.data());
+				// the coefficient tables' upload precedes the other stream's filters
+				const cudaStream_t other = c->stream == main_stream ? c->side_stream : main_stream;
+				ARMA_CUDA_TRY(cudaStreamWaitEvent(other, event(c->stream), 0));
+			}
 			std::vector<Ar32Surface> ga;
 			std::vector<RenormSpec> rs;
 			for (int k : members[g]) {
@@ -1023,17 +1077,15 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 			}
 			launch_ar32c(c, ga, tx, ty, 1);
 			launch_renorm_batch(c, rs, ARMA_FP32C);
-			cudaEvent_t e;
-			ARMA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-			ev.push_back(e);
-			ARMA_CUDA_TRY(cudaEventRecord(e, c->stream));
-			ARMA_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, e, 0));
+			ARMA_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, event(c->stream), 0));
 			for (int k : members[g]) {
 				const size_t np = size_t(s[k].shape[0]) * s[k].shape[1] * s[k].shape[2];
 				ARMA_CUDA_TRY(copy_async(c, s[k].d_zeta, dz[k], np * sizeof(float),
 				                              cudaMemcpyDeviceToHost, c->copy_stream));
 			}
 		}
+		c->stream = main_stream;
+		ARMA_CUDA_TRY(cudaStreamWaitEvent(main_stream, event(c->side_stream), 0));
 		std::vector<double> sc(n, 1.0);
 		ARMA_CUDA_TRY(copy_async(c, sc.data(), d_scale, sizeof(double) * n, cudaMemcpyDeviceToHost,
 		                              c->stream));
@@ -1053,6 +1105,7 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 					      luts ? luts + members[g][q] : nullptr);
 		}
 	} catch (...) {
+		cudaStreamSynchronize(c->side_stream);
 		cudaStreamSynchronize(c->copy_stream);
 		release();
 		throw;
@@ -1216,8 +1269,8 @@ int arma_autotune(arma_ctx* ctx, arma_surface* surfaces, int n, int precision, i
 				consider(t);
 			}
 			if (host && n >= 4) {
-				const std::pair<int, double> splits[] = {{4, 0.10}, {6, 0.06}, {8, 0.05},
-				                                         {12, 0.04}, {16, 0.03}};
+				const std::pair<int, double> splits[] = {{4, 0.35}, {8, 0.05}, {12, 0.04},
+				                                         {12, 0.12}, {16, 0.03}};
 				for (const auto& sp : splits) {
 					arma_tuning t = cur;
 					t.host_groups = sp.first;

@@ -51,8 +51,9 @@ struct Ctx {
 	bool own_stream = false;
 	int* d_err = nullptr;            // device error word
 	cudaStream_t copy_stream = nullptr;  // device->host copies overlapped with compute (lazy)
+	cudaStream_t side_stream = nullptr;  // second compute stream of the host-output pipeline (lazy)
 	double noise_margin = 1.0;           // polar-attempt estimate multiplier of the batched calls
-	arma_tuning tuning{20, 0, 4, 0.35};  // result-invariant speed settings (arma_ctx_set_tuning)
+	arma_tuning tuning{20, 0, 16, 0.06};  // result-invariant speed settings (arma_ctx_set_tuning)
 	uint64_t launches = 0;           // kernel launches issued
 	uint64_t h2d_bytes = 0;          // bytes copied host -> device through copy_async
 	uint64_t d2h_bytes = 0;          // bytes copied device -> host through copy_async
@@ -157,6 +158,9 @@ struct MtJob {
 	unsigned long long offset, count;
 	uint32_t* out;
 	const uint32_t* state = nullptr;
+	// the windows at every segment start (launch_mt_prepare with the same
+	// segment length), or null: jump ahead here
+	const uint32_t* seg_states = nullptr;
 };
 void launch_mt_generate(Ctx* c, const arma_mt_params& p, uint32_t seed,
                         uint64_t offset, uint64_t n, uint32_t* d_out);
@@ -165,6 +169,10 @@ void launch_mt_generate(Ctx* c, const arma_mt_params& p, uint32_t seed,
 constexpr int kMtLog2Seg = 20;
 void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs,
                               int log2_seg = kMtLog2Seg);
+// Only the jump-ahead windows of the jobs longer than one segment, into
+// jobs[q].seg_states (scratch), for later launch_mt_generate_batch calls on
+// subsets of the jobs with the same segment length.
+void launch_mt_prepare(Ctx* c, std::vector<MtJob>& jobs, int log2_seg = kMtLog2Seg);
 // After a chunk consumed 4 * *attempts words of `words` (n_words long): the
 // raw window in front of the next word (untempered copies of the nn words
 // before it), and *position += 4 * *attempts.  All on the device; an attempt

@@ -396,7 +396,12 @@ const MtTable& jump_table(Ctx* c, const arma_mt_params& p, int log2_seg) {
 
 }  // namespace
 
-void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_seg) {
+namespace {
+// The jump-ahead windows and the generation of a batch of jobs.  prepare:
+// only the windows (at every segment start of every job longer than one
+// segment), handed back in prepare[q].seg_states; a job that already carries
+// seg_states is not jumped again.
+void mt_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_seg, std::vector<MtJob>* prepare) {
 	ProfScope prof_(c, "mt");
 	ARMA_REQUIRE(log2_seg >= 12 && log2_seg <= 24, ARMA_EINVAL, "bad MT segment length");
 	for (const MtJob& j : jobs) {
@@ -415,10 +420,18 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 	std::vector<const MtTable*> tab(jobs.size(), nullptr);
 	int Kmax = 1;
 	size_t nstates = 0;
+	std::vector<char> ready(jobs.size(), 0);  // windows precomputed: no jumps here
+	std::vector<const uint32_t*> state0(jobs.size(), nullptr);  // per job: K windows of nn words
 	for (size_t q = 0; q < jobs.size(); ++q) {
 		const unsigned long long total = jobs[q].offset + jobs[q].count;
 		ARMA_REQUIRE((total + J - 1) / J <= (1ull << kLevels), ARMA_EINVAL, "MT stream too long");
 		K[q] = int(std::max(1ull, (total + J - 1) / J));
+		if (jobs[q].seg_states) {
+			ARMA_REQUIRE(K[q] > 1, ARMA_EINVAL, "MT job with windows but one segment");
+			ready[q] = 1;
+			state0[q] = jobs[q].seg_states;
+			continue;
+		}
 		if (K[q] > 1) {
 			tab[q] = &jump_table(c, jobs[q].p, log2_seg);
 			if (!tab[q]->ok) K[q] = 1;  // not a full-period set: one sequential segment
@@ -426,7 +439,6 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		if (K[q] > 1) nstates += size_t(K[q]) * jobs[q].p.nn;
 		Kmax = std::max(Kmax, K[q]);
 	}
-	std::vector<uint32_t*> state0(jobs.size(), nullptr);  // per job: K windows of nn words
 	if (nstates) {
 		uint32_t* states = static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * nstates));
 		size_t off = 0;
@@ -435,13 +447,13 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		std::vector<const uint32_t*> src;
 		std::vector<uint32_t*> dst;
 		for (size_t q = 0; q < jobs.size(); ++q) {
-			if (K[q] <= 1) continue;
+			if (K[q] <= 1 || ready[q]) continue;
 			state0[q] = states + off;
 			off += size_t(K[q]) * jobs[q].p.nn;
 			ps.push_back(jobs[q].p);
 			seeds.push_back(jobs[q].seed);
 			src.push_back(jobs[q].state);
-			dst.push_back(state0[q]);
+			dst.push_back(states + (state0[q] - states));
 		}
 		auto* d_ps = static_cast<arma_mt_params*>(scratch_take(c, sizeof(arma_mt_params) * ps.size()));
 		auto* d_seeds = static_cast<uint32_t*>(scratch_take(c, sizeof(uint32_t) * seeds.size()));
@@ -462,7 +474,7 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		while ((1 << levels) < Kmax) ++levels;
 		size_t smem = 0;
 		for (size_t q = 0; q < jobs.size(); ++q)
-			if (K[q] > 1)
+			if (K[q] > 1 && !ready[q])
 				smem = std::max(smem, sizeof(uint32_t) * size_t(32 * jobs[q].p.nn - jobs[q].p.rr +
 				                                                jobs[q].p.nn + kJumpThreads));
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(mt_jump_kernel,
@@ -471,12 +483,12 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 			std::vector<JumpJob> jj;
 			const int step = 1 << lv;
 			for (size_t q = 0; q < jobs.size(); ++q) {
-				if (K[q] <= 1) continue;
+				if (K[q] <= 1 || ready[q]) continue;
 				const int nn = jobs[q].p.nn;
+				uint32_t* w = states + (state0[q] - states);
 				for (int base = 0; base + step < K[q]; base += 2 * step)
-					jj.push_back(JumpJob{jobs[q].p, state0[q] + size_t(base) * nn,
-					                     state0[q] + size_t(base + step) * nn, tab[q]->bits[lv],
-					                     tab[q]->nbits[lv]});
+					jj.push_back(JumpJob{jobs[q].p, w + size_t(base) * nn, w + size_t(base + step) * nn,
+					                     tab[q]->bits[lv], tab[q]->nbits[lv]});
 			}
 			if (jj.empty()) continue;
 			auto* d_jj = static_cast<JumpJob*>(scratch_take(c, sizeof(JumpJob) * jj.size()));
@@ -491,6 +503,11 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 			ARMA_CUDA_TRY(cudaGetLastError());
 			c->launches += 1;
 		}
+	}
+	if (prepare) {
+		for (size_t q = 0; q < jobs.size(); ++q)
+			if (K[q] > 1) (*prepare)[q].seg_states = state0[q];
+		return;
 	}
 	// generation: one CTA per segment
 	std::vector<SegJob> seg;
@@ -550,6 +567,16 @@ void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_s
 		ARMA_CUDA_TRY(cudaGetLastError());
 		c->launches += 1;
 	}
+}
+
+}  // namespace
+
+void launch_mt_generate_batch(Ctx* c, const std::vector<MtJob>& jobs, int log2_seg) {
+	mt_batch(c, jobs, log2_seg, nullptr);
+}
+
+void launch_mt_prepare(Ctx* c, std::vector<MtJob>& jobs, int log2_seg) {
+	mt_batch(c, jobs, log2_seg, &jobs);
 }
 
 void launch_mt_window_update(Ctx* c, const std::vector<MtWindowSpec>& specs) {

@@ -96,11 +96,13 @@ int arma_ctx_profile_reset(arma_ctx* ctx);
  *                    jump-ahead work;
  *   ar_ctas_per_sm   CTAs of the persistent FP32 filter launch per SM, 0 =
  *                    as many as fit (default);
- *   host_groups      arma_batch_generate_host (FP32) splits the batch into
- *                    this many groups, 1..16 (default 4), whose device->host
- *                    copies overlap the next groups' computation;
+ *   host_groups      arma_batch_generate_host (FP32) splits the batch, in
+ *                    order of the filter's dependency chain, into this many
+ *                    groups, 1..16 (default 16), computed on two alternating
+ *                    streams, whose device->host copies overlap the later
+ *                    groups' computation;
  *   host_first       share of the work in the first group, (0, 1) (default
- *                    0.35); the other groups share the rest equally.
+ *                    0.06); the other groups share the rest equally.
  * arma_autotune (after the batch calls below) picks them for a batch by
  * timing. */
 typedef struct {
