@@ -33,6 +33,7 @@ def main(argv=None) -> int:
         with A.Context(0) as ctx, A.Driver.open(argv[0]) as drv:
             info = drv.info()
             sys.stderr.write(f"Input file = {argv[0]}\nOutput grid = {info['shape']}\n")
+            drv.set_output_dir(outdir)
             drv.generate_wavy_surface(ctx)
             drv.compute_velocity_potentials(ctx)
             drv.write_all(outdir)

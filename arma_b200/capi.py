@@ -35,11 +35,12 @@ EXPORTS = (
     "arma_ctx_set_profiling", "arma_ctx_profile", "arma_ctx_profile_reset",
     "arma_mt_file_count", "arma_mt_file_read", "arma_mt_file_write",
     "arma_mt19937_params", "arma_mt_genrand", "arma_acf_eval", "arma_auto_covariance",
+    "arma_auto_covariance_device",
     "arma_ar_fit",
     "arma_ar_fit_analytic", "arma_white_noise", "arma_ar_filter",
     "arma_variance_renorm", "arma_nit_apply", "arma_velocity_linear",
     "arma_batch_generate", "arma_batch_generate_host", "arma_ar_filter_fp32c_noalloc",
-    "arma_driver_open", "arma_driver_close", "arma_driver_generate",
+    "arma_driver_open", "arma_driver_close", "arma_driver_generate", "arma_driver_set_output_dir",
     "arma_driver_compute_velocity", "arma_driver_write_all", "arma_driver_info",
     "arma_driver_copy", "arma_server_config_default", "arma_server_create",
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
@@ -204,6 +205,7 @@ def lib():
             "arma_mt_genrand": (i, [vp, mp, C.c_uint32, C.c_uint64, sz, vp]),
             "arma_acf_eval": (i, [i, d, d, dp, dp, dp, ip, dp]),
             "arma_auto_covariance": (i, [dp, ip, dp]),
+            "arma_auto_covariance_device": (i, [vp, vp, ip, i, vp]),
             "arma_ar_fit": (i, [dp, ip, ip, i, dp, dp]),
             "arma_ar_fit_analytic": (i, [i, d, d, dp, dp, dp, ip, dp, dp]),
             "arma_white_noise": (i, [vp, mp, C.c_uint32, d, sz, i, vp]),
@@ -221,6 +223,7 @@ def lib():
             "arma_driver_open": (i, [C.c_char_p, i, C.POINTER(vp)]),
             "arma_driver_close": (i, [vp]),
             "arma_driver_generate": (i, [vp, vp]),
+            "arma_driver_set_output_dir": (i, [vp, C.c_char_p]),
             "arma_driver_compute_velocity": (i, [vp, vp]),
             "arma_driver_write_all": (i, [vp, C.c_char_p]),
             "arma_driver_info": (i, [vp, ip, dp, ip, dp, ip, C.POINTER(C.c_uint)]),
@@ -521,6 +524,11 @@ class Context:
         _check(lib().arma_velocity_linear_batch(self._h, arr, len(jobs), nx, ny, precision, depth,
                                                 zsp, len(zs)))
 
+    def auto_covariance(self, d_in: int, shape, precision: int, d_out: int):
+        """Circular auto-covariance of a device array into FP64 device memory."""
+        _check(lib().arma_auto_covariance_device(self._h, C.c_void_p(d_in), _i3(shape), precision,
+                                                 C.c_void_p(d_out)))
+
     def ma_filter(self, theta, shape, precision: int, d_eps: int, d_zeta: int):
         """zeta = eps - sum_{m != 0} theta(m) eps(n - m) on device buffers."""
         theta = np.ascontiguousarray(theta, np.float64)
@@ -636,6 +644,10 @@ class Driver:
         return {"shape": tuple(shape), "delta": tuple(delta), "order": tuple(order),
                 "var_wn": var.value, "velocity_shape": tuple(vs),
                 "output": [n for k, n in enumerate(OUTPUT_FLAGS) if fl.value >> k & 1]}
+
+    def set_output_dir(self, directory: str):
+        """Where zeta.bin goes when it is streamed during generation."""
+        _check(lib().arma_driver_set_output_dir(self._h, directory.encode()))
 
     def generate_wavy_surface(self, ctx: Context):
         _check(lib().arma_driver_generate(ctx.handle, self._h))

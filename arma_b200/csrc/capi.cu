@@ -588,6 +588,18 @@ int arma_auto_covariance(const double* in, const int shape[3], double* out) {
 	});
 }
 
+int arma_auto_covariance_device(arma_ctx* ctx, const void* d_in, const int shape[3],
+                                int precision, double* d_out) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && d_in && shape && d_out, ARMA_EINVAL, "null argument");
+		require_shape(shape, "array");
+		elem_size(precision);
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		launch_auto_covariance(&ctx->c, d_in, shape, precision, d_out);
+	});
+}
+
 int arma_acf_eval(int kind, double amplitude, double velocity, const double alpha[3],
                   const double beta[2], const double delta[3], const int shape[3],
                   double* acf) {
@@ -1488,6 +1500,13 @@ int arma_driver_compute_velocity(arma_ctx* ctx, arma_driver* drv) {
 		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
 		scratch_begin(&ctx->c, 0);
 		driver_velocity(&ctx->c, drv->d);
+	});
+}
+
+int arma_driver_set_output_dir(arma_driver* drv, const char* dir) {
+	return guard([&] {
+		ARMA_REQUIRE(drv, ARMA_EINVAL, "null argument");
+		driver_set_output_dir(drv->d, dir ? dir : "");
 	});
 }
 

@@ -24,6 +24,7 @@
 #include <memory>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -446,6 +447,10 @@ struct Driver {
 	std::vector<double> zeta;
 	std::vector<double> vel;  // (ntd, nz, nx, ny)
 	std::vector<double> vel_t, vel_z;
+	// where files written while generating go (the reference: the working
+	// directory); zeta.bin of an AR model is written then, not by write_all
+	std::string out_dir;
+	bool bin_written = false;
 };
 
 namespace {
@@ -522,6 +527,106 @@ void finalise(Driver* d) {
 }
 
 }  // namespace
+
+namespace {
+// The reference's writer thread (src/generator/ar_model_parallel.cc:112-145):
+// with the `binary` flag, an AR model's surface goes to zeta.bin in t-slabs,
+// network byte order, as the generation completes them.  The reference joins
+// the writer before it renormalises the surface and applies the NIT
+// (src/generator/ar_model_parallel.cc:196-198, src/generator/basic_arma_model.cc:
+// 100-110), so the file holds the surface as generated, and write_all does not
+// write it again (src/arma_driver.cc:41-46, src/generator/ar_model.hh:59-62).
+// Here the device->host copies of the slabs run on the context's copy stream
+// into page-locked memory and a host thread converts and writes each slab as
+// its copy completes, while the device goes on with the renormalisation.
+class SlabWriter {
+public:
+	SlabWriter(Ctx* c, const void* d_src, const int shape[3], size_t es, const std::string& path)
+	    : es_(es), path_(path) {
+		const size_t slice = size_t(shape[1]) * shape[2];
+		n_ = size_t(shape[0]) * slice;
+		const size_t per = std::max<size_t>(1, (size_t(4) << 20) / std::max<size_t>(slice, 1));
+		if (!c->copy_stream)
+			ARMA_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+		ARMA_CUDA_TRY(cudaHostAlloc(&stage_, std::max<size_t>(n_ * es_, 1), cudaHostAllocDefault));
+		cudaEvent_t ready;
+		ARMA_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+		events_.push_back(ready);
+		ARMA_CUDA_TRY(cudaEventRecord(ready, c->stream));
+		ARMA_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, ready, 0));
+		for (size_t t0 = 0; t0 < size_t(shape[0]); t0 += per) {
+			const size_t off = t0 * slice, cnt = std::min(per, size_t(shape[0]) - t0) * slice;
+			ARMA_CUDA_TRY(copy_async(c, static_cast<char*>(stage_) + off * es_,
+			                         static_cast<const char*>(d_src) + off * es_, cnt * es_,
+			                         cudaMemcpyDeviceToHost, c->copy_stream));
+			cudaEvent_t e;
+			ARMA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+			events_.push_back(e);
+			ARMA_CUDA_TRY(cudaEventRecord(e, c->copy_stream));
+			slabs_.push_back({off, cnt});
+		}
+		thread_ = std::thread([this] { run(); });
+	}
+	~SlabWriter() {
+		if (thread_.joinable()) thread_.join();
+		for (cudaEvent_t e : events_) cudaEventDestroy(e);
+		if (stage_) cudaFreeHost(stage_);
+	}
+	// waits for the writer; throws what it met
+	void finish() {
+		if (thread_.joinable()) thread_.join();
+		if (!error_.empty()) throw Error{error_code_, error_};
+	}
+
+private:
+	void run() {
+		std::ofstream out(path_, std::ios::binary);
+		if (!out) {
+			error_code_ = ARMA_EIO;
+			error_ = "cannot write " + path_;
+		}
+		std::vector<unsigned char> buf;
+		for (size_t k = 0; k < slabs_.size(); ++k) {
+			if (cudaEventSynchronize(events_[k + 1]) != cudaSuccess) {
+				error_code_ = ARMA_ECUDA;
+				error_ = "zeta.bin: device->host copy failed";
+				return;
+			}
+			if (!error_.empty()) continue;  // drain the copies, write nothing
+			const size_t off = slabs_[k].first, cnt = slabs_[k].second;
+			buf.resize(cnt * 8);
+			for (size_t i = 0; i < cnt; ++i) {
+				double v;
+				if (es_ == 8) std::memcpy(&v, static_cast<char*>(stage_) + (off + i) * 8, 8);
+				else {
+					float f;
+					std::memcpy(&f, static_cast<char*>(stage_) + (off + i) * 4, 4);
+					v = f;
+				}
+				unsigned char b[8];
+				std::memcpy(b, &v, 8);
+				for (int q = 0; q < 8; ++q) buf[i * 8 + q] = b[7 - q];  // network byte order
+			}
+			out.write(reinterpret_cast<const char*>(buf.data()), std::streamsize(buf.size()));
+			if (!out) {
+				error_code_ = ARMA_EIO;
+				error_ = "cannot write " + path_;
+			}
+		}
+	}
+
+	size_t es_, n_ = 0;
+	std::string path_;
+	void* stage_ = nullptr;
+	std::vector<cudaEvent_t> events_;
+	std::vector<std::pair<size_t, size_t>> slabs_;
+	std::thread thread_;
+	int error_code_ = ARMA_OK;
+	std::string error_;
+};
+}  // namespace
+
+void driver_set_output_dir(Driver* d, const std::string& dir) { d->out_dir = dir; }
 
 // generate: ACF -> order -> grid rescale -> fit (AR: Yule-Walker, MA: fixed
 // point) -> noise -> AR or MA filter -> renorm -> NIT
@@ -613,8 +718,27 @@ void driver_generate(Ctx* c, Driver* d) {
 	s.mt = mt;
 	s.seed = seed;
 	s.d_zeta = dz;
-	if (a.ma) ma_generate_device(c, &s, 1, a.precision);
-	else batch_generate_device(c, &s, 1, a.precision);
+	d->bin_written = false;
+	const bool stream_bin = !a.ma && (a.output & (1u << F_BINARY));
+	if (a.ma) {
+		ma_generate_device(c, &s, 1, a.precision);
+	} else if (!stream_bin) {
+		batch_generate_device(c, &s, 1, a.precision);
+	} else {
+		// the surface as generated, then its renormalisation on a copy while
+		// the writer streams the generated one to zeta.bin
+		s.acf0 = 0.0;
+		batch_generate_device(c, &s, 1, a.precision);
+		SlabWriter w(c, dz, d->shape, es, (d->out_dir.empty() ? "" : d->out_dir + "/") + "zeta.bin");
+		void* dz2 = scratch_take(c, n * es);
+		ARMA_CUDA_TRY(cudaMemcpyAsync(dz2, dz, n * es, cudaMemcpyDeviceToDevice, c->stream));
+		dz = dz2;
+		auto* d_scale = static_cast<double*>(scratch_take(c, sizeof(double)));
+		RenormSpec r{dz, {d->shape[0], d->shape[1], d->shape[2]}, d->acf[0], d_scale};
+		launch_renorm_batch(c, {r}, a.precision);
+		w.finish();
+		d->bin_written = true;
+	}
 	if (a.nit) {
 		launch_nit_bisection(c, a.nit_dist, a.nit_params, std::sqrt(d->acf[0]), a.cdf_interval[0],
 		                     a.cdf_interval[1], a.cdf_eps, a.cdf_iter, n, a.precision, dz);
@@ -706,7 +830,7 @@ void driver_write(Driver* d, const std::string& dir) {
 					out << i << ',' << d->delta[1] * j << ',' << d->delta[2] * k << ','
 					    << d->zeta[(size_t(i) * nx + j) * ny + k] << '\n';
 	}
-	if (f & (1u << F_BINARY)) {
+	if ((f & (1u << F_BINARY)) && !d->bin_written) {
 		std::ofstream out(pre + "zeta.bin", std::ios::binary);
 		if (!out) throw Error{ARMA_EIO, "cannot write " + pre + "zeta.bin"};
 		for (double v : d->zeta) {  // network byte order

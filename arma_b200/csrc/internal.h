@@ -309,6 +309,7 @@ void driver_close(Driver* d);
 void driver_generate(Ctx* c, Driver* d);
 void driver_velocity(Ctx* c, Driver* d);
 void driver_write(Driver* d, const std::string& dir);
+void driver_set_output_dir(Driver* d, const std::string& dir);
 void driver_info(const Driver* d, int shape[3], double delta[3], int order[3], double* var_wn,
                  int vshape[4], unsigned* oflags);
 const double* driver_zeta(const Driver* d);
@@ -338,6 +339,10 @@ struct EmpiricalAcf {
 };
 std::vector<double> empirical_acf(const EmpiricalAcf& p, int shape[3], double delta[3]);
 std::vector<double> auto_covariance(const std::vector<double>& w, const int n[3]);
+// The same on the device: d_in (FP32 or FP64, precision) -> d_out (FP64);
+// sides <= 1024.
+void launch_auto_covariance(Ctx* c, const void* d_in, const int shape[3], int precision,
+                            double* d_out);
 
 // Choi's order-recursive Yule-Walker solver (choi.cc) on a cubic n^3 ACF:
 // 0 with phi (order[0] x order[1] x order[2]) and the solver's variance, 1 bad

@@ -161,6 +161,12 @@ int arma_mt_genrand(arma_ctx* ctx, const arma_mt_params* p, uint32_t seed,
  * generator calls (src/generator/acf_generator.cc:147).  in and out may
  * alias. */
 int arma_auto_covariance(const double* in, const int shape[3], double* out);
+/* The same on the device for a surface in device memory (FP32 or FP64 per
+ * `precision`; ARMA_FP32C reads FP32), the result in FP64 device memory: the
+ * ACF of a realisation, as the reference checks generated surfaces.  Every
+ * side <= 1024 (ARMA_ENOTSUP beyond); asynchronous on the context's stream. */
+int arma_auto_covariance_device(arma_ctx* ctx, const void* d_in, const int shape[3],
+                                int precision, double* d_out);
 /* Analytic ACF on the non-negative lag grid (src/acf.hh:18-62). */
 int arma_acf_eval(int kind, double amplitude, double velocity,
                   const double alpha[3], const double beta[2],
@@ -396,6 +402,14 @@ int arma_ma_generate(arma_ctx* ctx, arma_surface* surfaces, int n, int precision
 typedef struct arma_driver arma_driver;
 int arma_driver_open(const char* config, int is_path, arma_driver** out);
 int arma_driver_close(arma_driver* drv);
+/* Directory of the files written while generating (default: the working
+ * directory, as the reference): with the `binary` flag an AR model's zeta.bin
+ * is streamed there in t-slabs during arma_driver_generate, holding the
+ * surface before the variance renormalisation and the NIT, as the
+ * reference's writer thread writes it (src/generator/ar_model_parallel.cc:
+ * 112-145, joined at :196-198 before src/generator/basic_arma_model.cc:106);
+ * arma_driver_write_all then does not write it again. */
+int arma_driver_set_output_dir(arma_driver* drv, const char* dir);
 int arma_driver_generate(arma_ctx* ctx, arma_driver* drv);
 int arma_driver_compute_velocity(arma_ctx* ctx, arma_driver* drv);
 int arma_driver_write_all(arma_driver* drv, const char* dir);

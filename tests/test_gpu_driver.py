@@ -54,6 +54,30 @@ velocity_potential_solver = linear {{
 """
 
 
+MA_BINARY = """model = MA {{
+	out_grid = (40,24,24)
+	acf = {{
+		func = propagating_wave
+		grid = (20,10,10) : (10,5,5)
+		amplitude = 1
+		velocity = 0.6
+		alpha = (1,1,1)
+		beta = (0.4,0.4)
+	}}
+	order = (20,10,10)
+	algorithm = fixed_point_iteration
+	output = surface,binary
+	validate = 0
+	seed = 321
+	mt_file = {mt}
+}}
+velocity_potential_solver = linear {{
+	depth = 12
+	domain = from (10,-6) to (30,0) npoints (3,4)
+}}
+"""
+
+
 def oracle_fit():
     delta = [L / 9 for L in ACF_LEN]
     acf = O.acf("standing_wave", (10, 10, 10), 1.5, 0.5, [0.06] * 3, [0.8, 0.8], delta)
@@ -74,7 +98,14 @@ def oracle_surface(phi, var, acf0, seed=1234):
 def test_driver_generate_velocity_write(ctx, tmp_path):
     mt = write_mt(tmp_path / "mt.dat")
     d = A.Driver(config(mt))
+    out = tmp_path / "out"
+    out.mkdir()
+    d.set_output_dir(str(out))
     d.generate_wavy_surface(ctx)
+    # zeta.bin is streamed while generating: the surface before the variance
+    # renormalisation, as the reference's writer thread writes it
+    assert sorted(os.listdir(out)) == ["zeta.bin"]
+    raw = (out / "zeta.bin").read_bytes()
     acf, phi_ref, var_ref = oracle_fit()
     # the fit is a host LL^T; its rounding differs from the oracle's in the
     # last bits, amplified by the Yule-Walker matrix's condition number
@@ -83,6 +114,13 @@ def test_driver_generate_velocity_write(ctx, tmp_path):
     zeta_ref = oracle_surface(d.phi(), d.info()["var_wn"], acf[0, 0, 0])
     zeta = d.zeta()
     assert np.abs(zeta - zeta_ref).max() <= 1e-12 * np.abs(zeta_ref).max()
+    shape = (40, 24, 24)
+    eps = O.white_noise(O.mt19937_params(), 1234, math.sqrt(d.info()["var_wn"]),
+                        int(np.prod(shape))).reshape(shape)
+    gen = O.ar_filter(eps, d.phi())
+    got = np.frombuffer(raw, dtype=">f8").reshape(shape)
+    assert np.abs(got - gen).max() <= 1e-12 * np.abs(gen).max()
+    assert not np.array_equal(got, zeta)
 
     d.compute_velocity_potentials(ctx)
     info = d.info()
@@ -93,12 +131,19 @@ def test_driver_generate_velocity_write(ctx, tmp_path):
     ref = O.velocity_linear(zeta, info["delta"], 12.0, z, t_idx)
     assert np.abs(vel - ref).max() <= 1e-9 * np.abs(ref).max()
 
-    out = tmp_path / "out"
-    out.mkdir()
     d.write_all(str(out))
     assert sorted(os.listdir(out)) == ["phi", "phi.csv", "zeta", "zeta.bin", "zeta.csv"]
-    O.write_zeta_bin(str(tmp_path / "ref.bin"), zeta)
-    assert (out / "zeta.bin").read_bytes() == (tmp_path / "ref.bin").read_bytes()
+    assert (out / "zeta.bin").read_bytes() == raw  # not written again
+    # an MA model has no writer thread: write_all writes the final surface
+    ma = A.Driver(MA_BINARY.format(mt=mt))
+    out_ma = tmp_path / "out_ma"
+    out_ma.mkdir()
+    ma.set_output_dir(str(out_ma))
+    ma.generate_wavy_surface(ctx)
+    assert os.listdir(out_ma) == []
+    ma.write_all(str(out_ma))
+    O.write_zeta_bin(str(tmp_path / "ref_ma.bin"), ma.zeta())
+    assert (out_ma / "zeta.bin").read_bytes() == (tmp_path / "ref_ma.bin").read_bytes()
     O.write_zeta_csv(str(tmp_path / "ref.csv"), zeta, info["delta"])
     assert (out / "zeta.csv").read_text() == (tmp_path / "ref.csv").read_text()
     head = (out / "zeta").read_text().split("\n", 1)[0]

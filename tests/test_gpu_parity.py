@@ -558,3 +558,26 @@ def test_velocity_high_amplitude_vs_oracle(ctx, shape, depth, zs, amp):
                             high_amplitude=True)
         got = out.cpu().numpy().astype(np.float64)
         assert np.abs(got - ref).max() <= tol * scale, (prec, np.abs(got - ref).max() / scale)
+
+
+@pytest.mark.gpu
+def test_auto_covariance_device(ctx):
+    """arma_auto_covariance_device against the host FP64 form (which
+    tests/test_acf_gen.py pins to the reference's CosineNoDecay case and to
+    numpy) on odd, prime and the generator's 2 n + 1 sides, from FP64 and FP32
+    input."""
+    rng = np.random.default_rng(11)
+    for shape in [(7, 11, 13), (21, 21, 21), (65, 33, 17), (1, 64, 2), (40, 40, 40), (5, 129, 3)]:
+        w = rng.standard_normal(shape)
+        host = A.auto_covariance(w)
+        for prec, dt in [(A.FP64, torch.float64), (A.FP32C, torch.float32)]:
+            src = torch.tensor(w, dtype=dt, device="cuda")
+            out = torch.empty(shape, dtype=torch.float64, device="cuda")
+            ctx.auto_covariance(src.data_ptr(), shape, prec, out.data_ptr())
+            ctx.synchronize()
+            ref = host if prec == A.FP64 else A.auto_covariance(src.cpu().double().numpy())
+            assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-12 * np.max(np.abs(ref)), shape
+    with pytest.raises(capi.ArmaError) as e:
+        big = torch.zeros((2, 2, 1025), dtype=torch.float64, device="cuda")
+        ctx.auto_covariance(big.data_ptr(), big.shape, A.FP64, big.data_ptr())
+    assert e.value.code == -8
