@@ -41,6 +41,7 @@ EXPORTS = (
     "arma_variance_renorm", "arma_nit_apply", "arma_velocity_linear",
     "arma_batch_generate", "arma_batch_generate_host", "arma_ar_filter_fp32c_noalloc",
     "arma_driver_open", "arma_driver_close", "arma_driver_generate", "arma_driver_set_output_dir",
+    "arma_selftest_wait",
     "arma_driver_compute_velocity", "arma_driver_write_all", "arma_driver_info",
     "arma_driver_copy", "arma_server_config_default", "arma_server_create",
     "arma_server_destroy", "arma_stream_open", "arma_stream_close", "arma_stream_submit",
@@ -224,6 +225,7 @@ def lib():
             "arma_driver_close": (i, [vp]),
             "arma_driver_generate": (i, [vp, vp]),
             "arma_driver_set_output_dir": (i, [vp, C.c_char_p]),
+            "arma_selftest_wait": (i, [vp]),
             "arma_driver_compute_velocity": (i, [vp, vp]),
             "arma_driver_write_all": (i, [vp, C.c_char_p]),
             "arma_driver_info": (i, [vp, ip, dp, ip, dp, ip, C.POINTER(C.c_uint)]),
@@ -523,6 +525,11 @@ class Context:
         zs, zsp = _d(z_levels)
         _check(lib().arma_velocity_linear_batch(self._h, arr, len(jobs), nx, ny, precision, depth,
                                                 zsp, len(zs)))
+
+    def selftest_wait(self):
+        """The filter's bounded wait on a flag nothing sets: raises ArmaError
+        (ARMA_ETIMEDOUT) after about a second; the context stays usable."""
+        _check(lib().arma_selftest_wait(self._h))
 
     def auto_covariance(self, d_in: int, shape, precision: int, d_out: int):
         """Circular auto-covariance of a device array into FP64 device memory."""

@@ -540,7 +540,22 @@ size_t smem_bytes(int pt, int px, int py) {
 	                        std::max(GROUP * R, HUNITS * PS));
 }
 
+// The filter's neighbour wait on a tile flag that nothing publishes: it runs
+// out after kSpinLimit polls and sets the error word (the failure path of
+// every bounded wait, exercised on purpose).
+__global__ void wait_selftest_kernel(const int* flag, int* err) {
+	if (threadIdx.x == 0) wait_flags(flag, nullptr, nullptr, 1, err);
+}
+
 }  // namespace
+
+void launch_wait_selftest(Ctx* c) {
+	int* flag = static_cast<int*>(scratch_take(c, sizeof(int)));
+	ARMA_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), c->stream));
+	wait_selftest_kernel<<<1, 32, 0, c->stream>>>(flag, c->d_err);
+	ARMA_CUDA_TRY(cudaGetLastError());
+	c->launches += 1;
+}
 
 int ar32c_tile_x() { return TX; }
 int ar32c_tile_y() { return TY; }

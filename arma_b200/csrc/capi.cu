@@ -1503,6 +1503,16 @@ int arma_driver_compute_velocity(arma_ctx* ctx, arma_driver* drv) {
 	});
 }
 
+int arma_selftest_wait(arma_ctx* ctx) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx, ARMA_EINVAL, "null argument");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		launch_wait_selftest(&ctx->c);
+		check_device_error(&ctx->c);  // ARMA_ETIMEDOUT, error word cleared
+	});
+}
+
 int arma_driver_set_output_dir(arma_driver* drv, const char* dir) {
 	return guard([&] {
 		ARMA_REQUIRE(drv, ARMA_EINVAL, "null argument");

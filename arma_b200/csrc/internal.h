@@ -228,6 +228,9 @@ struct Ar32Surface {
 };
 void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx,
                   int ty, int tt);
+// One bounded neighbour wait of the FP32 filter on a flag nothing sets
+// (arma_selftest_wait); leaves DEV_TIMEOUT in the context's error word.
+void launch_wait_selftest(Ctx* c);
 int ar32c_tile_x();
 int ar32c_tile_y();
 int ar32c_max_tap_rows();  // largest pt * px of the FP32 tile kernel

@@ -402,6 +402,11 @@ int arma_ma_generate(arma_ctx* ctx, arma_surface* surfaces, int n, int precision
 typedef struct arma_driver arma_driver;
 int arma_driver_open(const char* config, int is_path, arma_driver** out);
 int arma_driver_close(arma_driver* drv);
+/* Failure-path self-test: runs the FP32 filter's bounded neighbour wait on a
+ * tile flag that nothing publishes; the wait gives up after its poll limit
+ * (about a second), the call returns ARMA_ETIMEDOUT, and the context stays
+ * usable (its error word is cleared). */
+int arma_selftest_wait(arma_ctx* ctx);
 /* Directory of the files written while generating (default: the working
  * directory, as the reference): with the `binary` flag an AR model's zeta.bin
  * is streamed there in t-slabs during arma_driver_generate, holding the

@@ -581,3 +581,21 @@ def test_auto_covariance_device(ctx):
         big = torch.zeros((2, 2, 1025), dtype=torch.float64, device="cuda")
         ctx.auto_covariance(big.data_ptr(), big.shape, A.FP64, big.data_ptr())
     assert e.value.code == -8
+
+
+@pytest.mark.gpu
+def test_bounded_wait_times_out_and_context_survives(ctx):
+    """A device wait that runs out (a tile flag nothing publishes) comes back
+    as ARMA_ETIMEDOUT after its poll limit, and the context keeps working."""
+    import time
+    t0 = time.perf_counter()
+    with pytest.raises(capi.ArmaError) as e:
+        ctx.selftest_wait()
+    assert e.value.code == -4
+    assert time.perf_counter() - t0 < 30.0
+    phi, var = A.ar_fit_analytic(A.ACF_STANDING, (3, 3, 3), 1.5, 0.8, [0.05] * 3, [0.5, 0.5])
+    z = torch.empty((20, 16, 24), dtype=torch.float32, device="cuda")
+    ctx.batch_generate([capi.make_surface(z.shape, phi, var, 1.5, A.mt19937_params(), 7,
+                                          z.data_ptr())], A.FP32C)
+    ctx.synchronize()
+    assert torch.isfinite(z).all()
