@@ -295,7 +295,8 @@ __global__ void __launch_bounds__(kThreads)
 noise_batch_kernel(const NoiseJob* __restrict__ jobs, int njobs,
                    unsigned long long* __restrict__ status, unsigned int* __restrict__ ticket,
                    long long* __restrict__ pairs, int* __restrict__ err) {
-	__shared__ int s_g;
+	extern __shared__ __align__(16) unsigned char noise_smem[];  // 2 kTile values of T
+	__shared__ int s_g, s_total;
 	__shared__ long long s_excl;
 	__shared__ int s_cnt[kRounds * kWarps];  // per (round, warp); then their exclusive scan
 	if (threadIdx.x == 0) s_g = int(atomicAdd(ticket, 1u));
@@ -341,11 +342,37 @@ noise_batch_kernel(const NoiseJob* __restrict__ jobs, int njobs,
 			run += c[j];
 		}
 		const int total = __shfl_sync(0xffffffffu, incl, 31);
-		const bool first = g == jb.block_base;
-		if (lane == 0)
-			st_status(status + g, ((unsigned long long)total << 2) | (first ? 2ull : 1ull));
+		// the tile's own count goes out at once: successors look past it
+		if (lane == 0) {
+			s_total = total;
+			st_status(status + g, ((unsigned long long)total << 2) |
+			                          (g == jb.block_base ? 2ull : 1ull));
+		}
+	}
+	__syncthreads();
+
+	// pass 2: the accepted attempts' pairs, in tile order, into shared memory
+	// (before the tile's first output slot is known, so that the FP64
+	// arithmetic runs while the predecessors publish theirs)
+	T* buf = reinterpret_cast<T*>(noise_smem);
+	const unsigned below = (1u << lane) - 1u;
+#pragma unroll 2
+	for (int k = 0; k < kRounds; ++k) {
+		const bool ok = (okbits >> k) & 1u;
+		const unsigned bal = __ballot_sync(0xffffffffu, ok);
+		if (!ok) continue;
+		const unsigned long long a = tile0 + (unsigned long long)k * kThreads + threadIdx.x;
+		const Attempt at = attempt(words[a]);
+		const int lr = s_cnt[k * kWarps + warp] + __popc(bal & below);
+		const double m = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, log(at.r2)), at.r2));
+		buf[2 * lr] = T(__dadd_rn(__dmul_rn(__dmul_rn(at.y, m), jb.stddev), 0.0));
+		buf[2 * lr + 1] = T(__dadd_rn(__dmul_rn(__dmul_rn(at.x, m), jb.stddev), 0.0));
+	}
+	// the first output slot: the surface's pairs before this tile
+	if (warp == 0) {
+		const int total = s_total;
 		long long excl = 0;
-		if (!first) {
+		if (g != jb.block_base) {
 			excl = look_back(status, g, jb.block_base, err);
 			if (lane == 0) st_status(status + g, ((unsigned long long)(excl + total) << 2) | 2ull);
 		}
@@ -356,25 +383,23 @@ noise_batch_kernel(const NoiseJob* __restrict__ jobs, int njobs,
 	}
 	__syncthreads();
 
-	// pass 2: the accepted attempts' pairs at their ranks
+	// the tile's values to their slots (coalesced), up to the surface's n
 	T* out = static_cast<T*>(jb.out);
 	const long long excl = s_excl;
-	const unsigned below = (1u << lane) - 1u;
+	const unsigned long long o0 = 2ull * (unsigned long long)excl;
+	const int nv = 2 * s_total;
+	for (int q = threadIdx.x; q < nv; q += kThreads)
+		if (o0 + q < jb.n) out[o0 + q] = buf[q];
+	// a chunk that continues a stream: the attempts consumed up to the pair
+	// that ends at value n
+	if (jb.attempts && jb.n >= o0 + 2 && jb.n <= o0 + nv) {
+		const long long want = (long long)(jb.n - o0) / 2 - 1;  // local rank of that pair
 #pragma unroll 2
-	for (int k = 0; k < kRounds; ++k) {
-		const bool ok = (okbits >> k) & 1u;
-		const unsigned bal = __ballot_sync(0xffffffffu, ok);
-		if (!ok) continue;
-		const unsigned long long a = tile0 + (unsigned long long)k * kThreads + threadIdx.x;
-		const Attempt at = attempt(words[a]);
-		const long long rank = excl + s_cnt[k * kWarps + warp] + __popc(bal & below);
-		const unsigned long long i0 = 2ull * (unsigned long long)rank;
-		if (i0 < jb.n) {
-			const double m = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, log(at.r2)), at.r2));
-			out[i0] = T(__dadd_rn(__dmul_rn(__dmul_rn(at.y, m), jb.stddev), 0.0));
-			if (i0 + 1 < jb.n)
-				out[i0 + 1] = T(__dadd_rn(__dmul_rn(__dmul_rn(at.x, m), jb.stddev), 0.0));
-			if (jb.attempts && i0 + 2 == jb.n) *jb.attempts = a + 1;
+		for (int k = 0; k < kRounds; ++k) {
+			const bool ok = (okbits >> k) & 1u;
+			const unsigned bal = __ballot_sync(0xffffffffu, ok);
+			if (ok && s_cnt[k * kWarps + warp] + __popc(bal & below) == want)
+				*jb.attempts = tile0 + (unsigned long long)k * kThreads + threadIdx.x + 1;
 		}
 	}
 }
@@ -407,12 +432,16 @@ void enqueue_white_noise_batch(Ctx* c, const std::vector<NoiseSpec>& specs, int 
 	                              cudaMemcpyHostToDevice, c->stream));
 	const int nj = int(jobs.size());
 	auto* ticket = reinterpret_cast<unsigned int*>(sync);
-	if (precision == ARMA_FP64)
-		noise_batch_kernel<double><<<int(total_tiles), kThreads, 0, c->stream>>>(
+	if (precision == ARMA_FP64) {
+		const size_t smem = 2 * sizeof(double) * kTile;
+		ARMA_CUDA_TRY(cudaFuncSetAttribute(noise_batch_kernel<double>,
+		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		noise_batch_kernel<double><<<int(total_tiles), kThreads, smem, c->stream>>>(
 		    d_jobs, nj, sync + 1, ticket, d_pairs, c->d_err);
-	else
-		noise_batch_kernel<float><<<int(total_tiles), kThreads, 0, c->stream>>>(
-		    d_jobs, nj, sync + 1, ticket, d_pairs, c->d_err);
+	} else {
+		noise_batch_kernel<float><<<int(total_tiles), kThreads, 2 * sizeof(float) * kTile,
+		                            c->stream>>>(d_jobs, nj, sync + 1, ticket, d_pairs, c->d_err);
+	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
 }
