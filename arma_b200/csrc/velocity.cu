@@ -1074,6 +1074,21 @@ __device__ __noinline__ double window_even(int kx, int ky, int nx, int ny, doubl
 	return 0.5 * (w1 + w2);
 }
 
+// True when every entry of the fixed window is the same 4 pi: z = 0 at
+// infinite depth with s2 = (dkx i)^2 + (dky j)^2 positive and finite at every
+// (i, j) != (0, 0) of the nx x ny grid.  Rounding keeps s2 monotone in i and
+// j, so (1, 0), (0, 1) and (nx-1, ny-1) decide it; window_raw then returns its
+// z = 0 shortcut everywhere, (0, 0) copies (1, 1) and no edge fix applies, so
+// the even part is that constant and its odd part 0.
+__device__ __forceinline__ bool window_flat(int nx, int ny, double dkx, double dky, double z,
+                                            double depth) {
+	if (!(z == 0.0 && depth == INFINITY)) return false;
+	const double ex = dkx * (nx - 1), ey = dky * (ny - 1);
+	return dkx * dkx > 0.0 && dky * dky > 0.0 && ex * ex + ey * ey <= DBL_MAX;
+}
+// the value of that window, as window_raw forms it
+__device__ __forceinline__ double window_flat_value() { return k2Pi * 2.0 * 1.0 / 1.0; }
+
 template <int M, int NY, int NT>
 __global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1)
 velocity_real_kernel(const VelSlice<float>* __restrict__ sl, const double* __restrict__ kinfo,
@@ -1124,6 +1139,8 @@ velocity_real_kernel(const VelSlice<float>* __restrict__ sl, const double* __res
 		auto We = [&](int kx, int ky) {
 			return window_even(kx, ky, NX, NY, dkx, dky, z, depth);
 		};
+		const bool flat = window_flat(NX, NY, dkx, dky, z, depth);
+		const float flat_w = float(window_flat_value());
 		// one thread per pair {(a, b), (-a, -b)}: b in [0, NY/2], a in [0, M),
 		// with b in {0, NY/2} only a <= M/2 (the others are partners);
 		// consecutive threads on consecutive b (one row of A)
@@ -1135,12 +1152,18 @@ velocity_real_kernel(const VelSlice<float>* __restrict__ sl, const double* __res
 			// E = (z1 + conj z2) / 2, O = (z1 - conj z2) / 2i
 			const float2 E = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
 			const float2 O = make_float2(0.5f * (z1.y + z2.y), -0.5f * (z1.x - z2.x));
-			const double wa = We(a, b), wb = We(a + M, b);
-			const float Sv = float(0.5 * (wa + wb)), Dv = float(0.5 * (wa - wb));
-			const float2 w = tw[a * (L / NX)];  // W_nx^a
-			const float2 wO = cmul_tw<false>(O, w), wE = cmul_tw<true>(E, w);
-			const float2 E2 = make_float2(Sv * E.x + Dv * wO.x, Sv * E.y + Dv * wO.y);
-			const float2 O2 = make_float2(Sv * O.x + Dv * wE.x, Sv * O.y + Dv * wE.y);
+			float2 E2, O2;
+			if (flat) {  // S = the constant, D = 0: the same values without the window calls
+				E2 = make_float2(flat_w * E.x, flat_w * E.y);
+				O2 = make_float2(flat_w * O.x, flat_w * O.y);
+			} else {
+				const double wa = We(a, b), wb = We(a + M, b);
+				const float Sv = float(0.5 * (wa + wb)), Dv = float(0.5 * (wa - wb));
+				const float2 w = tw[a * (L / NX)];  // W_nx^a
+				const float2 wO = cmul_tw<false>(O, w), wE = cmul_tw<true>(E, w);
+				E2 = make_float2(Sv * E.x + Dv * wO.x, Sv * E.y + Dv * wO.y);
+				O2 = make_float2(Sv * O.x + Dv * wE.x, Sv * O.y + Dv * wE.y);
+			}
 			A[a * LD + b] = make_float2(E2.x - O2.y, E2.y + O2.x);     // E' + i O'
 			A[am * LD + bm] = make_float2(E2.x + O2.y, -E2.y + O2.x);  // conj E' + i conj O'
 		}
@@ -1270,6 +1293,8 @@ velocity_real2_kernel(const VelSlice<float>* __restrict__ sl, const double* __re
 			__syncthreads();
 		}
 		const double z = zs[iz];
+		const bool flat = window_flat(NX, NY, dkx, dky, z, depth);
+		const float flat_w = float(window_flat_value());
 		// pairs {(a, b), (-a, -b)} with a = 2j + rank (local row j)
 		for (int q = threadIdx.x; q < H * (NY / 2 + 1); q += NT) {
 			const int j = q / (NY / 2 + 1), b = q % (NY / 2 + 1), a = 2 * j + rank;
@@ -1279,13 +1304,19 @@ velocity_real2_kernel(const VelSlice<float>* __restrict__ sl, const double* __re
 			const float2 z1 = A[j * LD + b], z2 = A[jm * LD + bm];
 			const float2 E = make_float2(0.5f * (z1.x + z2.x), 0.5f * (z1.y - z2.y));
 			const float2 O = make_float2(0.5f * (z1.y + z2.y), -0.5f * (z1.x - z2.x));
-			const double wa = window_even(a, b, NX, NY, dkx, dky, z, depth);
-			const double wb = window_even(a + M, b, NX, NY, dkx, dky, z, depth);
-			const float Sv = float(0.5 * (wa + wb)), Dv = float(0.5 * (wa - wb));
-			const float2 w = tw[a * (L / NX)];  // W_nx^a
-			const float2 wO = cmul_tw<false>(O, w), wE = cmul_tw<true>(E, w);
-			const float2 E2 = make_float2(Sv * E.x + Dv * wO.x, Sv * E.y + Dv * wO.y);
-			const float2 O2 = make_float2(Sv * O.x + Dv * wE.x, Sv * O.y + Dv * wE.y);
+			float2 E2, O2;
+			if (flat) {  // S = the constant, D = 0: the same values without the window calls
+				E2 = make_float2(flat_w * E.x, flat_w * E.y);
+				O2 = make_float2(flat_w * O.x, flat_w * O.y);
+			} else {
+				const double wa = window_even(a, b, NX, NY, dkx, dky, z, depth);
+				const double wb = window_even(a + M, b, NX, NY, dkx, dky, z, depth);
+				const float Sv = float(0.5 * (wa + wb)), Dv = float(0.5 * (wa - wb));
+				const float2 w = tw[a * (L / NX)];  // W_nx^a
+				const float2 wO = cmul_tw<false>(O, w), wE = cmul_tw<true>(E, w);
+				E2 = make_float2(Sv * E.x + Dv * wO.x, Sv * E.y + Dv * wO.y);
+				O2 = make_float2(Sv * O.x + Dv * wE.x, Sv * O.y + Dv * wE.y);
+			}
 			A[j * LD + b] = make_float2(E2.x - O2.y, E2.y + O2.x);
 			A[jm * LD + bm] = make_float2(E2.x + O2.y, -E2.y + O2.x);
 		}
