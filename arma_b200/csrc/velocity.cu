@@ -144,6 +144,28 @@ __device__ __forceinline__ void solver_input(const VelSlice<T>& s, int nx, int n
 // at the end.
 constexpr int kFwThreads = 256;
 constexpr int kFwTile = 35;  // row pitch of the y pass's transposing tile (odd)
+// y pass tiles per warp: two in FP32 (the next 32 columns stage while the
+// current ones are walked), one in FP64 (two would halve the CTAs per SM)
+template <class T>
+constexpr int fw_tiles() { return sizeof(T) == 4 ? 2 : 1; }
+
+// One element from global into shared memory, asynchronously (L1-allocating
+// cp.async of 4 or 8 bytes); cp_async_commit closes a group of them and
+// cp_async_wait<N> waits until at most N of this thread's groups are pending.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* dst_smem, const T* src) {
+	static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+	const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst_smem));
+	asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(sizeof(T))
+	             : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+	asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+	asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 struct Run {
 	int sign;       // elevation > 0
@@ -418,44 +440,77 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 	const int nseg = outer * P, blocks = (outer + 31) / 32;
 	const int nstore = max(nseg, nwarps);  // segments, then the warps' results
 	const SegStore seg(fw_smem, nstore);
-	T* tile = reinterpret_cast<T*>(fw_smem + seg_region_bytes(nstore)) + warp * 32 * kFwTile;
+	T* tile = reinterpret_cast<T*>(fw_smem + seg_region_bytes(nstore)) +
+	          warp * fw_tiles<T>() * 32 * kFwTile;
 	for (int u = warp; u < blocks * P; u += nwarps) {
 		const int piece = u / blocks, b0 = (u % blocks) * 32, b = b0 + lane;
 		const int a_lo = 1 + piece * per, a_hi = 1 + min(npos, (piece + 1) * per);  // [a_lo, a_hi)
 		SegWalk st;
 		if (axis == 0) {
 			if (b < outer && a_lo < a_hi) {
-				// positions in batches of kFwBatch independent loads, so a lane
-				// has a batch in flight instead of one load per position
+				// positions in batches of kFwBatch independent loads; in FP32
+				// the next batch is loaded before the current one is walked, so
+				// its latency hides behind the walk (in FP64 the second batch's
+				// registers would spill)
+				constexpr bool ahead = sizeof(T) == 4;
 				T z1 = z[(long long)(a_lo - 1) * ny + b];
 				T z0 = z[(long long)a_lo * ny + b];
-				for (int a0 = a_lo; a0 < a_hi; a0 += kFwBatch) {
-					const int n = min(kFwBatch, a_hi - a0);
-					T buf[kFwBatch];
+				T buf[kFwBatch], nxt[kFwBatch];
+				if (ahead) {
 #pragma unroll
 					for (int k = 0; k < kFwBatch; ++k)
-						if (k < n) buf[k] = z[(long long)(a0 + 1 + k) * ny + b];
+						if (a_lo + k < a_hi) buf[k] = z[(long long)(a_lo + 1 + k) * ny + b];
+				}
+				for (int a0 = a_lo; a0 < a_hi; a0 += kFwBatch) {
+					const int n = min(kFwBatch, a_hi - a0);
+					const int a1 = ahead ? a0 + kFwBatch : a0;
+#pragma unroll
+					for (int k = 0; k < kFwBatch; ++k)
+						if (a1 + k < a_hi) (ahead ? nxt : buf)[k] = z[(long long)(a1 + 1 + k) * ny + b];
 					fw_batch(st, z1, z0, buf, n, dt, t);
+					if (ahead) {
+#pragma unroll
+						for (int k = 0; k < kFwBatch; ++k) buf[k] = nxt[k];
+					}
 				}
 			}
 		} else {
 			const int rows = min(32, outer - b0);
-			for (int c0 = a_lo; c0 < a_hi; c0 += 32) {
-				// columns c0-1 .. c0+32 of rows b0 .. b0+rows-1 (those < ny)
-				__syncwarp();
+			// columns c0-1 .. c0+32 of rows b0 .. b0+rows-1 (those < ny) into
+			// tile tb, as one group of asynchronous copies
+			auto stage = [&](int c0, T* tb) {
 				for (int r = 0; r < rows; ++r) {
 					const T* zr = z + (long long)(b0 + r) * ny;
-					if (c0 - 1 + lane < ny) tile[r * kFwTile + lane] = zr[c0 - 1 + lane];
-					if (lane < 2 && c0 + 31 + lane < ny) tile[r * kFwTile + 32 + lane] = zr[c0 + 31 + lane];
+					if (c0 - 1 + lane < ny) cp_async_elem(tb + r * kFwTile + lane, zr + c0 - 1 + lane);
+					if (lane < 2 && c0 + 31 + lane < ny)
+						cp_async_elem(tb + r * kFwTile + 32 + lane, zr + c0 + 31 + lane);
+				}
+				cp_async_commit();
+			};
+			constexpr int NB = fw_tiles<T>();
+			int cur = 0;
+			if (NB == 2 && a_lo < a_hi) stage(a_lo, tile);
+			for (int c0 = a_lo; c0 < a_hi; c0 += 32) {
+				T* tb = tile + cur * 32 * kFwTile;
+				if (NB == 2 && c0 + 32 < a_hi) {
+					// the other tile was last read in the previous step, which
+					// ended with a warp barrier
+					stage(c0 + 32, tile + (cur ^ 1) * 32 * kFwTile);
+					cp_async_wait<1>();
+				} else {
+					if (NB == 1) stage(c0, tb);
+					cp_async_wait<0>();
 				}
 				__syncwarp();
 				if (b < outer) {
-					const T* row = tile + lane * kFwTile;  // row[k] = z(b, c0 - 1 + k)
+					const T* row = tb + lane * kFwTile;  // row[k] = z(b, c0 - 1 + k)
 					T z1 = row[0], z0 = row[1];
 					const int n = min(32, a_hi - c0);
 					for (int k0 = 0; k0 < n; k0 += kFwBatch)
 						fw_batch(st, z1, z0, row + 2 + k0, min(kFwBatch, n - k0), dt, t);
 				}
+				__syncwarp();  // tile tb read by every lane before it is staged again
+				cur ^= NB - 1;
 			}
 		}
 		if (b < outer) seg.put(b * P + piece, st);  // loop order: line, then piece
@@ -1554,7 +1609,7 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 		const int fwarps = fw_warps(nx, ny);
 		const int nseg = std::max(nx * fw_pieces(nx, ny - 2, fwarps), ny * fw_pieces(ny, nx - 2, fwarps));
 		const size_t fw_smem = seg_region_bytes(std::max(nseg, fwarps)) +
-		                       sizeof(T) * size_t(fwarps) * 32 * kFwTile;
+		                       sizeof(T) * size_t(fwarps) * fw_tiles<T>() * 32 * kFwTile;
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(factor_waves_kernel<T>,
 		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(fw_smem)));
 		factor_waves_kernel<T><<<2 * ns, 32 * fwarps, fw_smem, c->stream>>>(d_sl, nx, ny, d_k);
