@@ -144,8 +144,9 @@ __device__ __forceinline__ void solver_input(const VelSlice<T>& s, int nx, int n
 // at the end.
 constexpr int kFwThreads = 256;
 constexpr int kFwTile = 35;  // row pitch of the y pass's transposing tile (odd)
-// y pass tiles per warp: two in FP32 (the next 32 columns stage while the
-// current ones are walked), one in FP64 (two would halve the CTAs per SM)
+// staging tiles of 32 x kFwTile elements per warp: two in FP32 (the next 32
+// positions stage while the current ones are walked), one in FP64 (two would
+// halve the CTAs per SM)
 template <class T>
 constexpr int fw_tiles() { return sizeof(T) == 4 ? 2 : 1; }
 
@@ -370,8 +371,8 @@ __device__ __forceinline__ void fw_vertex(T z0, T z1, T z2, double dt, int t, do
 	elev = cc + tex * (bb + aa * tex);
 }
 
-// n (<= kFwBatch) consecutive positions after (z1, z0), fed to the walk in
-// order; leaves (z1, z0) at the last two values.  The vertices of kFwIlp
+// n (<= kFwBatch) consecutive positions after (z1, z0), es elements apart
+// from zn on, fed to the walk in order; leaves (z1, z0) at the last two values.  The vertices of kFwIlp
 // positions are computed before any is fed to the walk, extremum or not, so
 // that their FP64 chains (a division each) run side by side: a warp takes the
 // vertex path whenever any of its lanes has an extremum, which is nearly
@@ -379,15 +380,15 @@ __device__ __forceinline__ void fw_vertex(T z0, T z1, T z2, double dt, int t, do
 constexpr int kFwBatch = 8;
 constexpr int kFwIlp = 4;
 template <class T>
-__device__ __forceinline__ void fw_batch(SegWalk& st, T& z1, T& z0, const T* zn, int n, double dt,
-                                         int t) {
+__device__ __forceinline__ void fw_batch(SegWalk& st, T& z1, T& z0, const T* zn, int es, int n,
+                                         double dt, int t) {
 #pragma unroll
 	for (int k0 = 0; k0 < kFwBatch; k0 += kFwIlp) {
 		double e[kFwIlp], p[kFwIlp];
 		bool ev[kFwIlp];
 #pragma unroll
 		for (int k = 0; k < kFwIlp; ++k) {
-			const T z2 = k0 + k < n ? zn[k0 + k] : z0;
+			const T z2 = k0 + k < n ? zn[(k0 + k) * es] : z0;
 			ev[k] = k0 + k < n && fw_extremum(z0, z1, z2);
 			fw_vertex(z0, z1, z2, dt, t, e[k], p[k]);
 			if (k0 + k < n) {
@@ -419,10 +420,12 @@ inline int fw_warps(int nx, int ny) {
 }
 
 // One CTA per (slice, axis).  axis 0 loops y outer, x inner over z(x,y): lane
-// b walks column y = b down x (loads coalesced across the warp); axis 1 (the
-// reference's transposed call) x outer, y inner: lane b walks row x = b, each
-// warp staging 32 rows x 34 columns at a time through shared memory.  Writes
-// min_k, max_k of the axis.
+// b walks column y = b down x; axis 1 (the reference's transposed call) x
+// outer, y inner: lane b walks row x = b.  Each warp stages 34 positions of
+// its 32 lines at a time into shared memory with asynchronous copies (rows of
+// the slice, coalesced), in FP32 into two tiles so that the next positions
+// arrive while the current ones are walked; both passes then run the same
+// walk.  Writes min_k, max_k of the axis.
 template <class T>
 __global__ void __launch_bounds__(kFwThreads, 2)
 factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* __restrict__ kout) {
@@ -446,72 +449,53 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 		const int piece = u / blocks, b0 = (u % blocks) * 32, b = b0 + lane;
 		const int a_lo = 1 + piece * per, a_hi = 1 + min(npos, (piece + 1) * per);  // [a_lo, a_hi)
 		SegWalk st;
-		if (axis == 0) {
-			if (b < outer && a_lo < a_hi) {
-				// positions in batches of kFwBatch independent loads; in FP32
-				// the next batch is loaded before the current one is walked, so
-				// its latency hides behind the walk (in FP64 the second batch's
-				// registers would spill)
-				constexpr bool ahead = sizeof(T) == 4;
-				T z1 = z[(long long)(a_lo - 1) * ny + b];
-				T z0 = z[(long long)a_lo * ny + b];
-				T buf[kFwBatch], nxt[kFwBatch];
-				if (ahead) {
-#pragma unroll
-					for (int k = 0; k < kFwBatch; ++k)
-						if (a_lo + k < a_hi) buf[k] = z[(long long)(a_lo + 1 + k) * ny + b];
-				}
-				for (int a0 = a_lo; a0 < a_hi; a0 += kFwBatch) {
-					const int n = min(kFwBatch, a_hi - a0);
-					const int a1 = ahead ? a0 + kFwBatch : a0;
-#pragma unroll
-					for (int k = 0; k < kFwBatch; ++k)
-						if (a1 + k < a_hi) (ahead ? nxt : buf)[k] = z[(long long)(a1 + 1 + k) * ny + b];
-					fw_batch(st, z1, z0, buf, n, dt, t);
-					if (ahead) {
-#pragma unroll
-						for (int k = 0; k < kFwBatch; ++k) buf[k] = nxt[k];
-					}
-				}
-			}
-		} else {
-			const int rows = min(32, outer - b0);
-			// columns c0-1 .. c0+32 of rows b0 .. b0+rows-1 (those < ny) into
-			// tile tb, as one group of asynchronous copies
-			auto stage = [&](int c0, T* tb) {
-				for (int r = 0; r < rows; ++r) {
+		const int lines = min(32, outer - b0);
+		// positions c0-1 .. c0+32 of the unit's lines (those inside the
+		// slice) into tile tb, as one group of asynchronous copies: for the x
+		// pass (lines are columns) 34 rows of 32 lines, coalesced along the
+		// rows; for the y pass (lines are rows) 32 lines of 34 positions at a
+		// row pitch of kFwTile
+		auto stage = [&](int c0, T* tb) {
+			if (axis == 0) {
+				if (lane < lines)
+					for (int r = 0; r < 34 && c0 - 1 + r < nx; ++r)
+						cp_async_elem(tb + r * 32 + lane, z + (long long)(c0 - 1 + r) * ny + b0 + lane);
+			} else {
+				for (int r = 0; r < lines; ++r) {
 					const T* zr = z + (long long)(b0 + r) * ny;
 					if (c0 - 1 + lane < ny) cp_async_elem(tb + r * kFwTile + lane, zr + c0 - 1 + lane);
 					if (lane < 2 && c0 + 31 + lane < ny)
 						cp_async_elem(tb + r * kFwTile + 32 + lane, zr + c0 + 31 + lane);
 				}
-				cp_async_commit();
-			};
-			constexpr int NB = fw_tiles<T>();
-			int cur = 0;
-			if (NB == 2 && a_lo < a_hi) stage(a_lo, tile);
-			for (int c0 = a_lo; c0 < a_hi; c0 += 32) {
-				T* tb = tile + cur * 32 * kFwTile;
-				if (NB == 2 && c0 + 32 < a_hi) {
-					// the other tile was last read in the previous step, which
-					// ended with a warp barrier
-					stage(c0 + 32, tile + (cur ^ 1) * 32 * kFwTile);
-					cp_async_wait<1>();
-				} else {
-					if (NB == 1) stage(c0, tb);
-					cp_async_wait<0>();
-				}
-				__syncwarp();
-				if (b < outer) {
-					const T* row = tb + lane * kFwTile;  // row[k] = z(b, c0 - 1 + k)
-					T z1 = row[0], z0 = row[1];
-					const int n = min(32, a_hi - c0);
-					for (int k0 = 0; k0 < n; k0 += kFwBatch)
-						fw_batch(st, z1, z0, row + 2 + k0, min(kFwBatch, n - k0), dt, t);
-				}
-				__syncwarp();  // tile tb read by every lane before it is staged again
-				cur ^= NB - 1;
 			}
+			cp_async_commit();
+		};
+		// the lane's line in a tile: position c0 - 1 + k at line[k * es]
+		const int loff = axis == 0 ? lane : lane * kFwTile, es = axis == 0 ? 32 : 1;
+		constexpr int NB = fw_tiles<T>();
+		int cur = 0;
+		if (NB == 2 && a_lo < a_hi) stage(a_lo, tile);
+		for (int c0 = a_lo; c0 < a_hi; c0 += 32) {
+			T* tb = tile + cur * 32 * kFwTile;
+			if (NB == 2 && c0 + 32 < a_hi) {
+				// the other tile was last read in the previous step, which ended
+				// with a warp barrier
+				stage(c0 + 32, tile + (cur ^ 1) * 32 * kFwTile);
+				cp_async_wait<1>();
+			} else {
+				if (NB == 1) stage(c0, tb);
+				cp_async_wait<0>();
+			}
+			__syncwarp();
+			if (b < outer) {
+				const T* line = tb + loff;
+				T z1 = line[0], z0 = line[es];
+				const int n = min(32, a_hi - c0);
+				for (int k0 = 0; k0 < n; k0 += kFwBatch)
+					fw_batch(st, z1, z0, line + (2 + k0) * es, es, min(kFwBatch, n - k0), dt, t);
+			}
+			__syncwarp();  // tile tb read by every lane before it is staged again
+			cur ^= NB - 1;
 		}
 		if (b < outer) seg.put(b * P + piece, st);  // loop order: line, then piece
 	}
