@@ -66,25 +66,42 @@ struct VelSlice {
 // -d zeta/dt at point p of slice s (src/derivative.hh:8-73): central
 // differences inside, second-order one-sided differences at both ends, the
 // slice itself when the surface has fewer than three slices.
+// Which slices the derivative reads (offsets from the point in units of
+// elements, all uniform over a slice) and which of the four forms applies.
+struct ZtTaps {
+	int form;  // 0: the slice itself, 1: first slice, 2: last slice, 3: central
+	int n;     // slices read
+	long long o[3];
+};
+
+template <class T>
+__device__ __forceinline__ ZtTaps zt_taps(const VelSlice<T>& s, long long n2) {
+	const long long d = s.d;
+	const int nt = s.nt;
+	if (nt - 1 < 2) return ZtTaps{0, 1, {d * n2, 0, 0}};
+	if (d == 0) return ZtTaps{1, 3, {2 * n2, n2, 0}};
+	if (d == nt - 1) return ZtTaps{2, 3, {d * n2, (d - 1) * n2, (d - 2) * n2}};
+	return ZtTaps{3, 2, {(d + 1) * n2, (d - 1) * n2, 0}};
+}
+
+// -d zeta/dt from the values v[k] at the offsets o[k]
+__device__ __forceinline__ double zt_value(const ZtTaps& k, const double* v, double dt) {
+	double r;
+	if (k.form == 0) return -v[0];
+	if (k.form == 1) r = 0.5 * (-v[0] + 4.0 * v[1] - 3.0 * v[2]);
+	else if (k.form == 2) r = 0.5 * (3.0 * v[0] - 4.0 * v[1] + v[2]);
+	else r = 0.5 * (v[0] - v[1]);
+	if (dt != 1.0) r /= dt;  // a division by 1 is exact: skipped
+	return -r;
+}
+
 template <class T>
 __device__ __forceinline__ double zeta_t(const VelSlice<T>& s, long long n2, long long p) {
 	const T* f = s.zeta + p;
-	const int d = s.d, nt = s.nt;
-	double r;
-	if (nt - 1 < 2) {
-		r = double(f[d * n2]);
-	} else {
-		if (d == 0) {
-			r = 0.5 * (-double(f[2 * n2]) + 4.0 * double(f[n2]) - 3.0 * double(f[0]));
-		} else if (d == nt - 1) {
-			r = 0.5 * (3.0 * double(f[d * n2]) - 4.0 * double(f[(d - 1) * n2]) +
-			           double(f[(d - 2) * n2]));
-		} else {
-			r = 0.5 * (double(f[(d + 1) * n2]) - double(f[(d - 1) * n2]));
-		}
-		if (s.dt != 1.0) r /= s.dt;  // a division by 1 is exact: skipped
-	}
-	return -r;
+	const ZtTaps k = zt_taps(s, n2);
+	double v[3] = {0.0, 0.0, 0.0};
+	for (int q = 0; q < k.n; ++q) v[q] = double(f[k.o[q]]);
+	return zt_value(k, v, s.dt);
 }
 
 // d zeta / dx (axis 1) or d zeta / dy (axis 2) at point p of slice s, with
@@ -1128,6 +1145,61 @@ __device__ __forceinline__ bool window_flat(int nx, int ny, double dkx, double d
 // the value of that window, as window_raw forms it
 __device__ __forceinline__ double window_flat_value() { return k2Pi * 2.0 * 1.0 / 1.0; }
 
+// The solver's input of rows 2p and 2p + 1 (p = p0 + i, i < rows) into
+// A[i * LD + y] as (row 2p, row 2p + 1).  The linear solver's -zeta_t loads
+// the slices of kRealBatch points of each thread before forming any of them,
+// so that a thread has that many loads in flight; the high-amplitude input
+// goes point by point.
+constexpr int kRealBatch = 4;
+template <int NY, int NT, int LD>
+__device__ __forceinline__ void real_input_rows(const VelSlice<float>& S, int NX, int p0, int rows,
+                                                float2* A) {
+	const long long n2 = (long long)NX * NY;
+	const int total = rows * NY;
+	if (S.mode != 0) {
+		for (int q = threadIdx.x; q < total; q += NT) {
+			const int i = q / NY, y = q % NY, p = p0 + i;
+			double re, im;
+			solver_input(S, NX, NY, (long long)(2 * p) * NY + y, re, im);
+			const double r0 = re;
+			solver_input(S, NX, NY, (long long)(2 * p + 1) * NY + y, re, im);
+			A[i * LD + y] = make_float2(float(r0), float(re));
+		}
+		return;
+	}
+	const ZtTaps k = zt_taps(S, n2);
+	for (int q0 = threadIdx.x; q0 < total; q0 += kRealBatch * NT) {
+		float v[kRealBatch][2][3];
+#pragma unroll
+		for (int u = 0; u < kRealBatch; ++u) {
+			const int q = q0 + u * NT;
+			if (q < total) {
+				const int i = q / NY, y = q % NY;
+				const float* f = S.zeta + (long long)(2 * (p0 + i)) * NY + y;
+#pragma unroll
+				for (int h = 0; h < 2; ++h)
+#pragma unroll
+					for (int j = 0; j < 3; ++j)
+						if (j < k.n) v[u][h][j] = f[h * NY + k.o[j]];
+			}
+		}
+#pragma unroll
+		for (int u = 0; u < kRealBatch; ++u) {
+			const int q = q0 + u * NT;
+			if (q < total) {
+				const int i = q / NY, y = q % NY;
+				double a[3], b[3];
+#pragma unroll
+				for (int j = 0; j < 3; ++j) {
+					a[j] = j < k.n ? double(v[u][0][j]) : 0.0;
+					b[j] = j < k.n ? double(v[u][1][j]) : 0.0;
+				}
+				A[i * LD + y] = make_float2(float(zt_value(k, a, S.dt)), float(zt_value(k, b, S.dt)));
+			}
+		}
+	}
+}
+
 template <int M, int NY, int NT>
 __global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1)
 velocity_real_kernel(const VelSlice<float>* __restrict__ sl, const double* __restrict__ kinfo,
@@ -1147,14 +1219,7 @@ velocity_real_kernel(const VelSlice<float>* __restrict__ sl, const double* __res
 		tw[j] = make_float2(float(cs), float(-sn));
 	}
 	// zeta_t of rows 2p and 2p + 1 into z(p, y)
-	for (int q = threadIdx.x; q < M * NY; q += NT) {
-		const int p = q / NY, y = q % NY;
-		double re, im;
-		solver_input(S, NX, NY, (long long)(2 * p) * NY + y, re, im);
-		const double r0 = re;
-		solver_input(S, NX, NY, (long long)(2 * p + 1) * NY + y, re, im);
-		A[p * LD + y] = make_float2(float(r0), float(re));
-	}
+	real_input_rows<NY, NT, LD>(S, NX, 0, M, A);
 	__syncthreads();
 	lines_fft<NY, false, NT, false>(A, M, LD, 1, tw, L / NY);  // rows
 	__syncthreads();
@@ -1297,14 +1362,7 @@ velocity_real2_kernel(const VelSlice<float>* __restrict__ sl, const double* __re
 		sincospi(2.0 * j / L, &sn, &cs);
 		tw[j] = make_float2(float(cs), float(-sn));
 	}
-	for (int q = threadIdx.x; q < H * NY; q += NT) {
-		const int i = q / NY, y = q % NY, p = rank * H + i;
-		double re, im;
-		solver_input(S, NX, NY, (long long)(2 * p) * NY + y, re, im);
-		const double r0 = re;
-		solver_input(S, NX, NY, (long long)(2 * p + 1) * NY + y, re, im);
-		A[i * LD + y] = make_float2(float(r0), float(re));
-	}
+	real_input_rows<NY, NT, LD>(S, NX, rank * H, H, A);
 	__syncthreads();
 	lines_fft<NY, false, NT, false>(A, H, LD, 1, tw, L / NY);  // rows
 	cl.sync();
