@@ -418,22 +418,22 @@ __device__ __forceinline__ void fw_batch(SegWalk& st, T& z1, T& z0, const T* zn,
 	}
 }
 
-// Pieces per line: enough (line blocks of 32) x pieces for two units per
-// warp of the CTA, at least 8 positions each.
-__host__ __device__ inline int fw_pieces(int outer, int npos, int nwarps) {
+// Pieces per line for a launch of ns slices: a work unit is one piece of 32
+// neighbouring lines, walked by one warp.  As few pieces as keep two waves of
+// units (16 warps per SM) in the launch, at least 8 positions each and no
+// more than two units per warp of a full CTA (which bounds the segments'
+// shared memory): long units keep the next positions staging while a warp
+// walks (a unit of one chunk waits for its loads) and leave fewer segments
+// to join.
+inline int fw_piece_cap(int outer, int npos) {
 	const int blocks = (outer + 31) / 32;
-	const int want = (2 * nwarps + blocks - 1) / blocks;
-	return npos < 16 ? 1 : (want < npos / 8 ? want : npos / 8);
+	return npos < 16 ? 1 : std::min(npos / 8, (2 * (kFwThreads / 32) + blocks - 1) / blocks);
 }
-
-// Warps per CTA for slices of nx x ny: up to kFwThreads / 32, no more than
-// the larger axis has work units (line blocks of 32 x pieces of >= 8
-// positions), so that small slices do not hold idle warps and their tiles.
-inline int fw_warps(int nx, int ny) {
-	auto units = [](int outer, int npos) {
-		return ((outer + 31) / 32) * (npos < 16 ? 1 : npos / 8);
-	};
-	return std::max(1, std::min(kFwThreads / 32, std::max(units(ny, nx - 2), units(nx, ny - 2))));
+inline int fw_pieces(int outer, int npos, int ns, int num_sms) {
+	const long long units1 = 2ll * ns * ((outer + 31) / 32);  // both axes' CTAs, one piece each
+	const long long want = 2ll * 16 * num_sms;
+	const long long p = (want + units1 - 1) / units1;
+	return int(std::max(1ll, std::min<long long>(p, fw_piece_cap(outer, npos))));
 }
 
 // One CTA per (slice, axis).  axis 0 loops y outer, x inner over z(x,y): lane
@@ -445,7 +445,8 @@ inline int fw_warps(int nx, int ny) {
 // walk.  Writes min_k, max_k of the axis.
 template <class T>
 __global__ void __launch_bounds__(kFwThreads, 2)
-factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* __restrict__ kout) {
+factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, int pieces0, int pieces1,
+                    double* __restrict__ kout) {
 	extern __shared__ __align__(16) unsigned char fw_smem[];
 	const int slice = blockIdx.x >> 1, axis = blockIdx.x & 1;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -456,9 +457,10 @@ factor_waves_kernel(const VelSlice<T>* __restrict__ sl, int nx, int ny, double* 
 	const int t = int(dt * S.d);  // factor_waves(slice, int t, dt): the truncated coordinate
 	const int outer = axis == 0 ? ny : nx;
 	const int npos = (axis == 0 ? nx : ny) - 2;  // positions 1 .. npos of each line
-	const int P = fw_pieces(outer, npos, nwarps), per = (npos + P - 1) / P;
+	const int P = axis == 0 ? pieces0 : pieces1, per = (npos + P - 1) / P;
 	const int nseg = outer * P, blocks = (outer + 31) / 32;
-	const int nstore = max(nseg, nwarps);  // segments, then the warps' results
+	// segments, then the warps' results: the larger axis's count for both
+	const int nstore = max(max(ny * pieces0, nx * pieces1), nwarps);
 	const SegStore seg(fw_smem, nstore);
 	T* tile = reinterpret_cast<T*>(fw_smem + seg_region_bytes(nstore)) +
 	          warp * fw_tiles<T>() * 32 * kFwTile;
@@ -1302,7 +1304,10 @@ bool launch_real_shape(Ctx* c, const VelSlice<float>* d_sl, int ns, int nx, int 
 	if constexpr (M * NY > kRealMaxPoints / 2) {
 		return false;
 	} else {
-		constexpr int NT = M * NY >= 8192 ? 512 : 256;
+		// 512 threads where the array takes one CTA per SM (16384 points);
+		// 256 below, two CTAs per SM (up to ~70 KB each), so that one CTA's
+		// barrier phases overlap the other's work
+		constexpr int NT = M * NY >= 16384 ? 512 : 256;
 		constexpr int L = 2 * M > NY ? 2 * M : NY;
 		const size_t smem = sizeof(float2) * (size_t(M) * RealLd<M, NY>::v + L);
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(velocity_real_kernel<M, NY, NT>,
@@ -1648,13 +1653,21 @@ void velocity_slices(Ctx* c, const std::vector<VelSlice<T>>& slices, int nx, int
 	                              cudaMemcpyHostToDevice, c->stream));
 	ARMA_CUDA_TRY(copy_async(c, d_z, z, sizeof(double) * nz, cudaMemcpyHostToDevice, c->stream));
 	{
-		const int fwarps = fw_warps(nx, ny);
-		const int nseg = std::max(nx * fw_pieces(nx, ny - 2, fwarps), ny * fw_pieces(ny, nx - 2, fwarps));
+		// pieces per line of the x pass (lines are the ny columns) and the y
+		// pass (the nx rows); warps per CTA: the larger axis's units, <= 8;
+		// then the other axis's lines are cut further so that its CTAs have a
+		// unit for every warp too, where the lines are long enough
+		const int b0 = (ny + 31) / 32, b1 = (nx + 31) / 32;
+		int p0 = fw_pieces(ny, nx - 2, ns, c->num_sms), p1 = fw_pieces(nx, ny - 2, ns, c->num_sms);
+		const int fwarps = std::max(1, std::min(kFwThreads / 32, std::max(b0 * p0, b1 * p1)));
+		p0 = std::max(p0, std::min(fw_piece_cap(ny, nx - 2), (fwarps + b0 - 1) / b0));
+		p1 = std::max(p1, std::min(fw_piece_cap(nx, ny - 2), (fwarps + b1 - 1) / b1));
+		const int nseg = std::max(ny * p0, nx * p1);
 		const size_t fw_smem = seg_region_bytes(std::max(nseg, fwarps)) +
 		                       sizeof(T) * size_t(fwarps) * fw_tiles<T>() * 32 * kFwTile;
 		ARMA_CUDA_TRY(cudaFuncSetAttribute(factor_waves_kernel<T>,
 		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(fw_smem)));
-		factor_waves_kernel<T><<<2 * ns, 32 * fwarps, fw_smem, c->stream>>>(d_sl, nx, ny, d_k);
+		factor_waves_kernel<T><<<2 * ns, 32 * fwarps, fw_smem, c->stream>>>(d_sl, nx, ny, p0, p1, d_k);
 	}
 	ARMA_CUDA_TRY(cudaGetLastError());
 	c->launches += 1;
