@@ -1152,7 +1152,7 @@ __device__ __forceinline__ double window_flat_value() { return k2Pi * 2.0 * 1.0 
 // the slices of kRealBatch points of each thread before forming any of them,
 // so that a thread has that many loads in flight; the high-amplitude input
 // goes point by point.
-constexpr int kRealBatch = 4;
+constexpr int kRealBatch = 8;
 template <int NY, int NT, int LD>
 __device__ __forceinline__ void real_input_rows(const VelSlice<float>& S, int NX, int p0, int rows,
                                                 float2* A) {
