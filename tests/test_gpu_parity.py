@@ -508,6 +508,28 @@ def test_velocity_batch_equals_single_calls(ctx):
             assert torch.equal(o, ref)
 
 
+@pytest.mark.parametrize("prec,dt", [(A.FP32C, torch.float32), (A.FP64, torch.float64)])
+def test_velocity_independent_of_line_pieces(ctx, prec, dt):
+    """factor_waves cuts each slice's lines into fewer pieces the more slices a
+    launch holds (here 3 and 7 pieces per line on the two axes for 3 slices,
+    1 and 2 for 1600, with 148 SMs), and joins the pieces' walks afterwards:
+    the potentials of every slice are the same bits whichever cut was taken."""
+    shape = (1600, 32, 64)
+    phi, var = A.ar_fit_analytic(A.ACF_PROPAGATING, (2, 2, 2), 1.0, 0.6, [0.04] * 3, [0.3, 0.2])
+    eps = O.white_noise(O.mt19937_params(), 11, np.sqrt(var), int(np.prod(shape))).reshape(shape)
+    z = dev(O.ar_filter(eps, phi), dt)
+    every = list(range(shape[0]))
+    whole = torch.zeros((shape[0], 1) + shape[1:], dtype=dt, device="cuda")
+    ctx.velocity_linear(z.data_ptr(), shape, prec, (1.0, 1.0, 1.0), np.inf, [0.0], every,
+                        whole.data_ptr())
+    for t0 in (0, 1, 797, 1597):
+        part = torch.zeros((3, 1) + shape[1:], dtype=dt, device="cuda")
+        ctx.velocity_linear(z.data_ptr(), shape, prec, (1.0, 1.0, 1.0), np.inf, [0.0],
+                            [t0, t0 + 1, t0 + 2], part.data_ptr())
+        ctx.synchronize()
+        assert torch.equal(part, whole[t0:t0 + 3]), t0
+
+
 @pytest.mark.parametrize("shape,depth,zs", [
     ((8, 40, 24), 12.0, [0.0, -3.0]),     # 40 = 4.2.5, 24 = 4.2.3
     ((6, 20, 30), np.inf, [0.0]),         # 30 = 2.3.5
