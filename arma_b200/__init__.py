@@ -7,7 +7,8 @@ to a CPU implementation -- if the library is missing, importing
 :mod:`arma_b200.capi` raises.
 """
 from .capi import (  # noqa: F401
-    ArmaError, Context, Driver, MtParams, NitTable, Server, server_config, Surface, Tuning, lib,
+    ArmaError, Context, Driver, MtParams, NitTable, Router, Server, server_config, Surface, Tuning,
+    lib,
     library_path, nit_table,
     FP64, FP32C, ACF_STANDING, ACF_PROPAGATING,
     NIT_GRAM_CHARLIER, NIT_SKEW_NORMAL, NIT_BISECTION, NIT_LUT,

@@ -51,6 +51,9 @@ EXPORTS = (
     "arma_ma_fit", "arma_ma_filter", "arma_ma_generate", "arma_ctx_set_noise_margin",
     "arma_mt_create", "arma_mt_is_primitive", "arma_mt_equidistribution",
     "arma_batch_generate_nit", "arma_ctx_get_tuning", "arma_ctx_set_tuning", "arma_autotune",
+    "arma_router_create", "arma_router_destroy", "arma_router_replicas", "arma_router_stream_open",
+    "arma_router_stream_close", "arma_router_stream_submit", "arma_router_poll",
+    "arma_router_placement", "arma_router_stats_get",
 )
 
 
@@ -240,6 +243,15 @@ def lib():
             "arma_server_stats_get": (i, [vp, C.POINTER(ServerStats)]),
             "arma_server_last_failure": (i, [vp, C.c_char_p, sz]),
             "arma_server_profile": (i, [vp, C.c_char_p, dp, C.POINTER(C.c_uint64)]),
+            "arma_router_create": (i, [ip, i, C.POINTER(ServerConfig), C.POINTER(vp)]),
+            "arma_router_destroy": (i, [vp]),
+            "arma_router_replicas": (i, [vp, ip]),
+            "arma_router_stream_open": (i, [vp, C.POINTER(StreamSpec), C.POINTER(C.c_uint64)]),
+            "arma_router_stream_close": (i, [vp, C.c_uint64]),
+            "arma_router_stream_submit": (i, [vp, C.c_uint64, vp, vp, C.POINTER(C.c_uint64)]),
+            "arma_router_poll": (i, [vp, C.POINTER(Completion), i, i, ip]),
+            "arma_router_placement": (i, [vp, C.c_uint64, ip, ip]),
+            "arma_router_stats_get": (i, [vp, i, C.POINTER(ServerStats)]),
             "arma_velocity_linear_batch": (i, [vp, C.POINTER(VelocityJob), i, i, i, i, d, dp, i]),
             "arma_validate_process": (i, [dp, ip, ip]),
             "arma_poly_roots": (i, [dp, i, dp, dp]),
@@ -703,7 +715,62 @@ def server_config(**kw) -> ServerConfig:
     return cfg
 
 
-class Server:
+def _stream_spec(nx, ny, phi, var_wn, acf0, mt, seed, delta) -> StreamSpec:
+    """``arma_stream_spec`` over `phi` (a float64 C-contiguous array the caller
+    keeps alive for the call)."""
+    spec = StreamSpec()
+    spec.nx, spec.ny = int(nx), int(ny)
+    spec.order = (C.c_int * 3)(*phi.shape)
+    spec.phi = _dp(phi)
+    spec.var_wn = var_wn
+    spec.acf0 = acf0
+    spec.mt = mt
+    spec.seed = seed
+    spec.delta = (C.c_double * 3)(*delta)
+    return spec
+
+
+def _completions(buf, n, keep) -> list:
+    out = []
+    for k in range(n):
+        c = buf[k]
+        keep.pop(c.request, None)
+        out.append({"request": c.request, "stream": c.stream, "chunk": c.chunk,
+                    "status": c.status, "batch_size": c.batch_size,
+                    "latency_ms": c.latency_ms, "queue_ms": c.queue_ms,
+                    "device_ms": c.device_ms})
+    return out
+
+
+class _Requests:
+    """Handle life cycle and waiting shared by ``Server`` and ``Router``."""
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def wait(self, count: int, timeout_ms: int = 60000):
+        """Poll until `count` completions arrived (raises on timeout)."""
+        import time
+        got = []
+        deadline = time.monotonic() + timeout_ms / 1000.0
+        while len(got) < count:
+            left = int((deadline - time.monotonic()) * 1000)
+            if left <= 0:
+                raise TimeoutError(f"{len(got)} of {count} completions")
+            got += self.poll(256, min(left, 1000))
+        return got
+
+
+class Server(_Requests):
     """An ``arma_server``: device-resident surface streams served in chunks
     with continuous batching."""
 
@@ -720,30 +787,10 @@ class Server:
             self._h = None
             self._keep.clear()
 
-    def __enter__(self):
-        return self
-
-    def __exit__(self, *exc):
-        self.close()
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
-
     def open_stream(self, nx, ny, phi, var_wn, acf0, mt: MtParams, seed: int,
                     delta=(1.0, 1.0, 1.0)) -> int:
         phi = np.ascontiguousarray(phi, np.float64)
-        spec = StreamSpec()
-        spec.nx, spec.ny = int(nx), int(ny)
-        spec.order = (C.c_int * 3)(*phi.shape)
-        spec.phi = _dp(phi)
-        spec.var_wn = var_wn
-        spec.acf0 = acf0
-        spec.mt = mt
-        spec.seed = seed
-        spec.delta = (C.c_double * 3)(*delta)
+        spec = _stream_spec(nx, ny, phi, var_wn, acf0, mt, seed, delta)
         sid = C.c_uint64()
         _check(lib().arma_stream_open(self._h, C.byref(spec), C.byref(sid)))
         return sid.value
@@ -765,27 +812,7 @@ class Server:
         buf = (Completion * max_n)()
         n = C.c_int()
         _check(lib().arma_server_poll(self._h, buf, max_n, timeout_ms, C.byref(n)))
-        out = []
-        for k in range(n.value):
-            c = buf[k]
-            self._keep.pop(c.request, None)
-            out.append({"request": c.request, "stream": c.stream, "chunk": c.chunk,
-                        "status": c.status, "batch_size": c.batch_size,
-                        "latency_ms": c.latency_ms, "queue_ms": c.queue_ms,
-                        "device_ms": c.device_ms})
-        return out
-
-    def wait(self, count: int, timeout_ms: int = 60000):
-        """Poll until `count` completions arrived (raises on timeout)."""
-        import time
-        got = []
-        deadline = time.monotonic() + timeout_ms / 1000.0
-        while len(got) < count:
-            left = int((deadline - time.monotonic()) * 1000)
-            if left <= 0:
-                raise TimeoutError(f"{len(got)} of {count} completions")
-            got += self.poll(256, min(left, 1000))
-        return got
+        return _completions(buf, n.value, self._keep)
 
     def stats(self) -> dict:
         st = ServerStats()
@@ -803,3 +830,66 @@ class Server:
         buf = C.create_string_buffer(1024)
         lib().arma_server_last_failure(self._h, buf, len(buf))
         return buf.value.decode(errors="replace")
+
+
+class Router(_Requests):
+    """An ``arma_router``: one serving replica per listed device (a device may
+    be listed more than once).  A stream is placed on the replica with the
+    least stream state and stays there; its ids carry the replica index in
+    their top 8 bits.  Outputs of a stream must be memory of its replica's
+    device or page-locked host memory."""
+
+    def __init__(self, devices=(0,), config: ServerConfig | None = None, **kw):
+        self.config = config if config is not None else server_config(**kw)
+        devs = (C.c_int * len(devices))(*devices)
+        h = C.c_void_p()
+        _check(lib().arma_router_create(devs, len(devices), C.byref(self.config), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def close(self):
+        if self._h:
+            _check(lib().arma_router_destroy(self._h))
+            self._h = None
+            self._keep.clear()
+
+    def replicas(self) -> int:
+        n = C.c_int()
+        _check(lib().arma_router_replicas(self._h, C.byref(n)))
+        return n.value
+
+    def open_stream(self, nx, ny, phi, var_wn, acf0, mt: MtParams, seed: int,
+                    delta=(1.0, 1.0, 1.0)) -> int:
+        phi = np.ascontiguousarray(phi, np.float64)
+        spec = _stream_spec(nx, ny, phi, var_wn, acf0, mt, seed, delta)
+        sid = C.c_uint64()
+        _check(lib().arma_router_stream_open(self._h, C.byref(spec), C.byref(sid)))
+        return sid.value
+
+    def close_stream(self, sid: int):
+        _check(lib().arma_router_stream_close(self._h, sid))
+
+    def submit(self, sid: int, zeta_ptr: int, velocity_ptr: int = 0, keep=None) -> int:
+        rid = C.c_uint64()
+        _check(lib().arma_router_stream_submit(self._h, sid, C.c_void_p(zeta_ptr),
+                                               C.c_void_p(velocity_ptr or None), C.byref(rid)))
+        if keep is not None:
+            self._keep[rid.value] = keep
+        return rid.value
+
+    def poll(self, max_n: int = 256, timeout_ms: int = 0):
+        buf = (Completion * max_n)()
+        n = C.c_int()
+        _check(lib().arma_router_poll(self._h, buf, max_n, timeout_ms, C.byref(n)))
+        return _completions(buf, n.value, self._keep)
+
+    def placement(self, sid: int):
+        """(replica index, device) of a stream."""
+        rep, dev = C.c_int(), C.c_int()
+        _check(lib().arma_router_placement(self._h, sid, C.byref(rep), C.byref(dev)))
+        return rep.value, dev.value
+
+    def stats(self, replica: int = 0) -> dict:
+        st = ServerStats()
+        _check(lib().arma_router_stats_get(self._h, replica, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in st._fields_}

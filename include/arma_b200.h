@@ -506,6 +506,35 @@ int arma_server_profile(arma_server* srv, const char* name, double* ms, uint64_t
 /* The last failure the serving thread saw (empty if none). */
 int arma_server_last_failure(arma_server* srv, char* buf, size_t len);
 
+/* ------------------------------------------------ replica router */
+/* No counterpart in the reference.  One server per listed device (a replica;
+ * a device may be listed more than once) behind one handle, for serving on
+ * several GPUs of a node: a stream opens on the replica with the least
+ * stream state placed on it (nx * ny * (pt - 1 + 2 chunk_slices) points,
+ * ties to fewer streams, then to the lower index) and stays there; its
+ * requests go to that replica, and one poll returns the completions of all
+ * replicas.  Stream and request ids are the replica's own ids with the
+ * replica index in the top 8 bits, so ids of different replicas never
+ * collide.  Replicas share nothing: no collective, no peer memory. */
+typedef struct arma_router arma_router;
+int arma_router_create(const int* devices, int n, const arma_server_config* cfg,
+                       arma_router** out);
+/* Destroys every replica (each finishes its queued requests first). */
+int arma_router_destroy(arma_router* r);
+int arma_router_replicas(arma_router* r, int* n);
+int arma_router_stream_open(arma_router* r, const arma_stream_spec* spec, uint64_t* stream_id);
+int arma_router_stream_close(arma_router* r, uint64_t stream_id);
+/* As arma_stream_submit; the outputs must be memory of the stream's replica's
+ * device (or page-locked host memory). */
+int arma_router_stream_submit(arma_router* r, uint64_t stream_id, float* zeta_out,
+                              float* velocity_out, uint64_t* request_id);
+/* Up to max completions of any replica; waits up to timeout_ms (-1: forever)
+ * for the first. */
+int arma_router_poll(arma_router* r, arma_completion* out, int max, int timeout_ms, int* n);
+/* The replica index and device a stream was placed on. */
+int arma_router_placement(arma_router* r, uint64_t stream_id, int* replica, int* device);
+int arma_router_stats_get(arma_router* r, int replica, arma_server_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

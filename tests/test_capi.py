@@ -132,3 +132,10 @@ def test_malformed_mt_parameter_set_rejected(tmp_path, field, value):
     with pytest.raises(capi.ArmaError) as e:
         A.mt_file_write(str(tmp_path / "mt.dat"), [p])
     assert e.value.code == -1 and "bad MT parameter set" in str(e.value)
+
+
+def test_router_rejects_bad_arguments_without_a_device():
+    for devices in ([], list(range(257))):
+        with pytest.raises(A.ArmaError) as e:
+            A.Router(devices=devices)
+        assert e.value.code == -1

@@ -214,3 +214,37 @@ def test_open_rejects_bad_streams():
         with pytest.raises(A.ArmaError) as e:
             srv.open_stream(64, 64, big, bv, 0.0, mt(), 1)     # history > chunk
         assert e.value.code == -1
+
+
+def test_router_places_by_stream_state_and_serves_exactly(ctx):
+    """Two replicas on one device: streams go to the replica with the least
+    stream state (nx * ny * (pt - 1 + 2 T) points), ids carry the replica in
+    their top 8 bits, one poll merges both replicas' completions, and every
+    stream's chunks equal the one-shot surface of the same seed."""
+    phi, var = model()                      # pt = 5
+    T = 16
+    sizes = [(128, 128), (64, 64), (64, 64), (64, 64), (64, 96)]
+    with A.Router(devices=[0, 0], chunk_slices=T, velocity=0, max_inflight=2) as r:
+        assert r.replicas() == 2
+        sids = [r.open_stream(*n2, phi, var, 0.0, mt(), 40 + k) for k, n2 in enumerate(sizes[:4])]
+        # 128^2 x 36 = 589,824 on replica 0; each 64^2 x 36 = 147,456 to replica 1
+        assert [r.placement(s) for s in sids] == [(0, 0), (1, 0), (1, 0), (1, 0)]
+        assert [s >> 56 for s in sids] == [0, 1, 1, 1]
+        r.close_stream(sids[0])             # replica 0 now holds nothing
+        sids[0] = r.open_stream(*sizes[4], phi, var, 0.0, mt(), 44)
+        assert r.placement(sids[0]) == (0, 0)
+        outs = {s: run_stream(r, s, 2, n2, T) for s, n2 in zip(sids, [sizes[4]] + sizes[1:4])}
+        got = r.wait(2 * len(sids))
+        # a closed stream's state is reclaimed by its replica's serving thread
+        assert r.stats(0)["streams"] == 1 and r.stats(1)["streams"] == 3
+        assert all(g["status"] == 0 for g in got)
+        assert sorted(g["stream"] for g in got) == sorted(sids * 2)
+        assert all(g["request"] >> 56 == g["stream"] >> 56 for g in got)
+        torch.cuda.synchronize()
+        chunks = {s: np.concatenate([z.cpu().numpy() for z, _ in o]) for s, o in outs.items()}
+        with pytest.raises(A.ArmaError):
+            r.placement((1 << 56) | 999)       # no such stream on replica 1
+    seeds = [44, 41, 42, 43]
+    for s, n2, seed in zip(sids, [sizes[4]] + sizes[1:4], seeds):
+        ref, _ = one_shot(ctx, (2 * T,) + n2, phi, var, 0.0, seed)
+        assert np.array_equal(chunks[s], ref)
