@@ -38,6 +38,7 @@
 // counter in dependency order, so a CTA only ever waits on tiles that are
 // already owned by running CTAs.
 #include <algorithm>
+#include <climits>
 #include <mutex>
 #include <vector>
 
@@ -118,14 +119,23 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 }
 
 // Wait until every non-null flag is >= need; the three acquire loads of a
-// poll are issued together so one L2 round trip covers them.  Gives up after
+// poll are issued together so one L2 round trip covers them.  seen[] holds the
+// values this thread's earlier acquire loads returned: a neighbour that is
+// already known to be at or past `need` is not polled again (that load's
+// acquire already ordered its slices before this thread's later loads), so a
+// tile whose neighbours run ahead pays no round trip.  Gives up after
 // kSpinLimit polls (or when another CTA already gave up) and reports
 // DEV_TIMEOUT; returns false then.
-__device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need, int* err) {
+__device__ bool wait_flags(const int* f0, const int* f1, const int* f2, int need, int* seen,
+                           int* err) {
+	if (seen[0] >= need && seen[1] >= need && seen[2] >= need) return true;
 	for (long long it = 0; it < kSpinLimit; ++it) {
 		const int a = f0 ? ld_acquire(f0) : need;
 		const int b = f1 ? ld_acquire(f1) : need;
 		const int c = f2 ? ld_acquire(f2) : need;
+		seen[0] = f0 ? a : INT_MAX;
+		seen[1] = f1 ? b : INT_MAX;
+		seen[2] = f2 ? c : INT_MAX;
 		if (a >= need && b >= need && c >= need) return true;
 		if ((it & 63) == 63 && *((volatile int*)err) != DEV_OK) return false;
 		__nanosleep(64);
@@ -302,20 +312,20 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 		const int* fN = (by > 0) ? tk.flags + bx * tk.tiles_y + by - 1 : nullptr;
 		const int* fNW = (bx > 0 && by > 0) ? tk.flags + (bx - 1) * tk.tiles_y + by - 1 : nullptr;
 		int* own_flag = tk.flags + bx * tk.tiles_y + by;
+		int seen[3] = {-1, -1, -1};
 		for (int t = tk.t0; t < tk.nt; ++t) {
+			// the release store orders the compute threads' stores of slice
+			// t-1 (made visible to this thread by the barrier) before the flag
 			if (t > tk.t0) {
 				bar_sync(BAR_DONE, NTHREADS);
-				if (lane == 0) {
-					__threadfence();
-					st_release(own_flag, t);
-				}
+				if (lane == 0) st_release(own_flag, t);
 			}
 			float* cur = ring + (t % pt) * slot_sz;
 			const float* zt = tk.zeta + t * sst;
 			for (int q = lane; q < slot_sz; q += 32) cur[q] = 0.0f;
 			__syncwarp();
 			int ok = 1;
-			if (lane == 0) ok = wait_flags(fW, fN, fNW, t + 1, err) ? 1 : 0;
+			if (lane == 0) ok = wait_flags(fW, fN, fNW, t + 1, seen, err) ? 1 : 0;
 			ok = __shfl_sync(0xffffffffu, ok, 0);
 			if (ok) {
 				// rows above the tile (all columns) and the left columns of the
@@ -351,10 +361,7 @@ __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned c
 		}
 		if (tk.nt > tk.t0) {
 			bar_sync(BAR_DONE, NTHREADS);
-			if (lane == 0) {
-				__threadfence();
-				st_release(own_flag, tk.nt);
-			}
+			if (lane == 0) st_release(own_flag, tk.nt);
 		}
 		return;
 	}
@@ -544,7 +551,8 @@ size_t smem_bytes(int pt, int px, int py) {
 // out after kSpinLimit polls and sets the error word (the failure path of
 // every bounded wait, exercised on purpose).
 __global__ void wait_selftest_kernel(const int* flag, int* err) {
-	if (threadIdx.x == 0) wait_flags(flag, nullptr, nullptr, 1, err);
+	int seen[3] = {-1, -1, -1};
+	if (threadIdx.x == 0) wait_flags(flag, nullptr, nullptr, 1, seen, err);
 }
 
 }  // namespace
