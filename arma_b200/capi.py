@@ -53,7 +53,7 @@ EXPORTS = (
     "arma_batch_generate_nit", "arma_ctx_get_tuning", "arma_ctx_set_tuning", "arma_autotune",
     "arma_router_create", "arma_router_destroy", "arma_router_replicas", "arma_router_stream_open",
     "arma_router_stream_close", "arma_router_stream_submit", "arma_router_poll",
-    "arma_router_placement", "arma_router_stats_get",
+    "arma_router_placement", "arma_router_stats_get", "arma_ar_filter_strip",
 )
 
 
@@ -214,6 +214,7 @@ def lib():
             "arma_ar_fit_analytic": (i, [i, d, d, dp, dp, dp, ip, dp, dp]),
             "arma_white_noise": (i, [vp, mp, C.c_uint32, d, sz, i, vp]),
             "arma_ar_filter": (i, [vp, dp, ip, ip, i, vp]),
+            "arma_ar_filter_strip": (i, [vp, dp, ip, ip, i, i, vp]),
             "arma_variance_renorm": (i, [vp, vp, ip, i, d, dp]),
             "arma_nit_apply": (i, [vp, i, dp, d, i, dp, d, i, i, d, sz, i, vp]),
             "arma_velocity_linear": (i, [vp, vp, ip, i, dp, d, dp, i, ip, i, vp]),
@@ -500,6 +501,13 @@ class Context:
         phi = np.ascontiguousarray(phi, np.float64)
         _check(lib().arma_ar_filter(self._h, _dp(phi), _i3(phi.shape), _i3(shape), precision,
                                     C.c_void_p(d_zeta)))
+
+    def ar_filter_strip(self, phi, shape, t0: int, given_rows: int, d_zeta: int):
+        """FP32 filter of one x-strip: rows [0, given_rows) and slices [0, t0)
+        of the (nt, nx, ny) float32 buffer are given, the rest holds noise."""
+        phi = np.ascontiguousarray(phi, np.float64)
+        _check(lib().arma_ar_filter_strip(self._h, _dp(phi), _i3(phi.shape), _i3(shape), t0,
+                                          given_rows, C.c_void_p(d_zeta)))
 
     def variance_renorm(self, d_zeta: int, shape, precision: int, acf0: float) -> float:
         s = C.c_double()

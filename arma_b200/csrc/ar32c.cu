@@ -75,6 +75,7 @@ constexpr long long kSpinLimit = 1ll << 24;
 struct Task {
 	int nt, nx, ny, pt, px, py;
 	int t0;  // slices [0, t0) are history: read, never written
+	int given_tx;  // tile rows [0, given_tx) are given (an x-strip's upper band): read, never written
 	int tiles_x, tiles_y;
 	int ticket_base;
 	float* zeta;
@@ -249,6 +250,12 @@ template <int PY>
 __device__ void run_tile(const Task& tk, int bx, int by, float* smem, unsigned char* s_lo,
                          int* err) {
 	const int tid = threadIdx.x;
+	if (bx < tk.given_tx) {
+		// a given tile (the band above an x-strip, holding the upper strip's
+		// finished values): published as complete for every slice at once
+		if (tid == 0) st_release(tk.flags + bx * tk.tiles_y + by, tk.nt);
+		return;
+	}
 	const int grp = tid / GROUP;                 // 0 or 1: halves of the tap rows
 	const int lt = tid % GROUP;
 	const int xl = lt / STRIPS;                  // tile-local row
@@ -601,6 +608,7 @@ void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx, int 
 		t.nt = s.nt; t.nx = s.nx; t.ny = s.ny;
 		t.pt = s.pt; t.px = s.px; t.py = s.py;
 		t.t0 = s.t0;
+		t.given_tx = s.given_tx;
 		t.tiles_x = s.tiles_x; t.tiles_y = s.tiles_y;
 		t.ticket_base = total;
 		t.zeta = s.zeta; t.phi = s.phi; t.phi_lo = s.phi_lo; t.h = s.h;
@@ -761,6 +769,7 @@ extern "C" int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, con
 	t.nt = shape[0]; t.nx = shape[1]; t.ny = shape[2];
 	t.pt = order[0]; t.px = order[1]; t.py = order[2];
 	t.t0 = 0;
+	t.given_tx = 0;
 	t.tiles_x = tiles_x; t.tiles_y = tiles_y;
 	t.ticket_base = 0;
 	t.zeta = d_zeta;

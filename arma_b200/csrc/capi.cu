@@ -783,6 +783,27 @@ int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3], const i
 	});
 }
 
+int arma_ar_filter_strip(arma_ctx* ctx, const double* phi, const int order[3], const int shape[3],
+                         int t0, int given_rows, float* d_zeta) {
+	return guard([&] {
+		ARMA_REQUIRE(ctx && phi && d_zeta, ARMA_EINVAL, "null argument");
+		require_shape(shape, "out_grid");
+		require_order(order);
+		const int tx = ar32c_tile_x(), ty = ar32c_tile_y();
+		ARMA_REQUIRE(t0 >= 0 && t0 < shape[0], ARMA_EINVAL, "t0 must be in [0, nt)");
+		ARMA_REQUIRE(given_rows >= 0 && given_rows % tx == 0 && given_rows < shape[1], ARMA_EINVAL,
+		             "given_rows must be a multiple of 16 rows below nx");
+		ARMA_CUDA_TRY(cudaSetDevice(ctx->c.device));
+		scratch_begin(&ctx->c, 0);
+		float* z = d_zeta;
+		std::vector<Ar32Surface> s = ar32_surfaces(&ctx->c, 1, &phi, &order, &shape, &z);
+		s[0].t0 = t0;
+		s[0].given_tx = given_rows / tx;
+		launch_ar32c(&ctx->c, s, tx, ty, 1);
+		check_device_error(&ctx->c);
+	});
+}
+
 int arma_variance_renorm(arma_ctx* ctx, void* d_zeta, const int shape[3], int precision,
                          double acf0, double* scale_out) {
 	return guard([&] {

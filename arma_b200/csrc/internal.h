@@ -225,6 +225,7 @@ struct Ar32Surface {
 	const float* h;        // device, intra-slice impulse response (TX*TY)
 	int tiles_x, tiles_y;  // spatial tile grid
 	int t0 = 0;            // slices [0, t0) hold a finished history (streams)
+	int given_tx = 0;      // tile rows [0, given_tx) hold given values (x-strips)
 };
 void launch_ar32c(Ctx* c, const std::vector<Ar32Surface>& surfaces, int tx,
                   int ty, int tt);

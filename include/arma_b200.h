@@ -225,6 +225,21 @@ int arma_ar_filter(arma_ctx* ctx, const double* phi, const int order[3],
 int arma_ar_filter_fp32c_noalloc(void* stream, const double* phi, const int order[3],
                                  const int shape[3], float* d_zeta);
 
+/* One x-strip of a surface split by rows across devices, for a surface too
+ * large for one device (the reference ships each partition of a surface with
+ * its halo to a remote kernel, src/generator/ar_model_bscheduler.cc:285-353).
+ * d_zeta holds shape = (nt, nx, ny): rows [0, given_rows) of every slice and
+ * slices [0, t0) are given -- finished values (the last rows of the strip
+ * above, zeros above the surface's first row; the previous time chunk) that
+ * are read and never written -- and every other point holds its white noise
+ * on entry and its surface value on return.  given_rows is 0 or a multiple
+ * of the filter's 16 tile rows below nx; FP32C orders only (see
+ * arma_ar_filter).  When the strip's first computed row sits at a multiple of
+ * 16 rows of the whole surface, its rows are bit-identical to
+ * arma_ar_filter(..., ARMA_FP32C, ...) of the whole surface. */
+int arma_ar_filter_strip(arma_ctx* ctx, const double* phi, const int order[3],
+                         const int shape[3], int t0, int given_rows, float* d_zeta);
+
 /* ------------------------------------------ A10: variance renormalisation */
 /* zeta *= sqrt(acf0 / var) with var the unbiased variance of the
  * numElements() contiguous values starting at zeta(nt/2, nx/2, ny/2)
