@@ -102,13 +102,18 @@ NoisePlan noise_plan(Ctx* c, const arma_surface* s, int n) {
 	return plan;
 }
 
+// words_ready: the surfaces' MT words were generated already (one wide launch
+// for a whole batch); only the polar transform is enqueued.
 long long* noise_enqueue(Ctx* c, const arma_surface* s, const NoisePlan& plan,
-                         const std::vector<int>& idx, int precision, const std::vector<void*>& dz) {
+                         const std::vector<int>& idx, int precision, const std::vector<void*>& dz,
+                         bool words_ready = false) {
 	const int n = int(idx.size());
 	long long* d_pairs = static_cast<long long*>(scratch_take(c, sizeof(long long) * n));
-	std::vector<MtJob> jobs(n);
-	for (int q = 0; q < n; ++q) jobs[q] = plan.jobs[idx[q]];
-	launch_mt_generate_batch(c, jobs, c->tuning.mt_log2_segment);
+	if (!words_ready) {
+		std::vector<MtJob> jobs(n);
+		for (int q = 0; q < n; ++q) jobs[q] = plan.jobs[idx[q]];
+		launch_mt_generate_batch(c, jobs, c->tuning.mt_log2_segment);
+	}
 	std::vector<NoiseSpec> specs(n);
 	for (int q = 0; q < n; ++q) {
 		const int k = idx[q];
@@ -1062,11 +1067,12 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 	// back (a device->host read on the context's stream would queue behind the
 	// previous groups' copies); the counts are checked at the end.
 	std::vector<long long*> d_pairs(G, nullptr);
-	// every surface's MT jump-ahead windows once, in wide launches (per group
-	// they would be narrow, latency-bound trees), before the groups' words
+	// every surface's MT jump-ahead windows and then all its words once, in
+	// wide launches (per group they would be narrow, latency-bound trees and
+	// short generation launches); the groups run only the polar transform
 	NoisePlan plan = noise_plan(c, s, n);
 	auto noise = [&](int g) {
-		d_pairs[g] = noise_enqueue(c, s, plan, members[g], ARMA_FP32C, dz);
+		d_pairs[g] = noise_enqueue(c, s, plan, members[g], ARMA_FP32C, dz, true);
 	};
 	if (!c->copy_stream)
 		ARMA_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
@@ -1088,7 +1094,8 @@ void pipelined_host_output(Ctx* c, arma_surface* s, int n, const std::vector<voi
 	};
 	try {
 		launch_mt_prepare(c, plan.jobs, c->tuning.mt_log2_segment);
-		// the side stream starts after the caller's earlier work and the windows
+		launch_mt_generate_batch(c, plan.jobs, c->tuning.mt_log2_segment);
+		// the side stream starts after the caller's earlier work and the words
 		ARMA_CUDA_TRY(cudaStreamWaitEvent(c->side_stream, event(main_stream), 0));
 		for (int g = 0; g < G; ++g) {
 			if (members[g].empty()) continue;
