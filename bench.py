@@ -340,6 +340,27 @@ def gpu_arm(args):
         e2e_d2h = (d2h1 - d2h0) // e2e_steps
         # parity spot check of the host copy against the device result
         assert torch.equal(host[0], bufs32[0].cpu())
+        # the device->host link of this box: plain pinned copies of about
+        # 1 GB of the same surfaces, best of three, CUDA events on one stream
+        pick, nb = [], 0
+        for k in range(len(batch)):
+            pick.append(k)
+            nb += host[k].numel() * 4
+            if nb >= 1 << 30:
+                break
+        link = 0.0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for k in pick:
+                host[k].copy_(bufs32[k], non_blocking=True)
+            e1.record()
+            e1.synchronize()
+            link = max(link, nb / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+        e2e_link = {"d2h_link_gbs": link,
+                    "copy_bound_ms": e2e_d2h / (link * 1e9) * 1e3,
+                    "ms_per_call": e2e_t / e2e_steps * 1e3}
         ctx.set_tuning(tuned_dev)  # the device-resident legs below
     del bufs32
 
@@ -413,7 +434,7 @@ def gpu_arm(args):
                        "l2": "inputs larger than L2 (%.1f GB per rank)" % (npts * 4 / 1e9),
                        "parallelism": f"dp{world} (independent surfaces per rank)"},
             "e2e": {"value": e2e, "unit": "points/s", "h2d_bytes_per_step": e2e_h2d,
-                    "d2h_bytes_per_step": e2e_d2h, "steps": e2e_steps,
+                    "d2h_bytes_per_step": e2e_d2h, "steps": e2e_steps, **e2e_link,
                     "copies": "counted by the library (arma_ctx_transfer_bytes): host->device "
                               "task lists, parameter sets and coefficient tables; device->host "
                               "surfaces, scales and accepted-pair counts"} if e2e else None,
