@@ -117,3 +117,38 @@ def test_strip_bounds_and_windows():
         for t, lo, hi in X.renorm_window(shape, x0, x1):
             seen += part[t, lo:hi].tolist()
     assert sorted(seen) == list(range(s0, s0 + count))
+
+
+def test_strip_arguments_are_checked():
+    import torch
+    from arma_b200 import xstrip as X
+    phi, eps = model()
+    z = torch.from_numpy(np.ascontiguousarray(eps[:, :16]))
+    band = lambda a, b: torch.zeros((b - a, X.BAND, SHAPE[2]))  # noqa: E731
+    with pytest.raises(ValueError):   # strips start on the 16-row tile grid
+        X.filter_strip(StripFilter(), phi, z, 8, 4, band)
+    with pytest.raises(ValueError):   # a strip below the first needs its band
+        X.filter_strip(StripFilter(), phi, z, 16, 4)
+    with pytest.raises(ValueError):   # the first strip has none
+        X.filter_strip(StripFilter(), phi, z, 0, 4, band)
+    short = torch.from_numpy(np.ascontiguousarray(eps[:, :8]))
+    with pytest.raises(ValueError):   # too few rows to feed the strip below
+        X.filter_strip(StripFilter(), phi, short, 0, 4, None, lambda a, b, t: None)
+
+
+def test_one_slice_chunks_equal_the_whole_surface_in_one_process():
+    """The pipeline with the bands handed over in memory, chunks of one slice
+    (every chunk's history from earlier chunks only)."""
+    import torch
+    from arma_b200 import xstrip as X
+    phi, eps = model()
+    whole = eps.copy()
+    StripFilter().ar_filter_strip(phi, SHAPE, 0, 0, whole.ctypes.data)
+    bands, out = {}, []
+    for r, (x0, x1) in enumerate(X.strip_bounds(SHAPE[1], 2)):
+        z = torch.from_numpy(np.ascontiguousarray(eps[:, x0:x1]))
+        recv = (lambda a, b, r=r: bands[(r - 1, a)]) if r else None
+        send = (lambda a, b, t, r=r: bands.__setitem__((r, a), t.clone())) if r == 0 else None
+        X.filter_strip(StripFilter(), phi, z, x0, 1, recv, send)
+        out.append(z.numpy())
+    assert np.array_equal(np.concatenate(out, axis=1), whole)
